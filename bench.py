@@ -1,0 +1,323 @@
+"""Benchmark of the state-vector hot path: 30-qubit random-layer circuit, HBM GB/s.
+
+Workload: random-layer circuit on 30 qubits (2^30 amplitudes, complex f32 =
+8 GiB), 20 layers, seed 1; each layer is Rz(theta)+Rx(phi) on every qubit
+and a CNOT brickwork (even pairs on even layers, odd pairs on odd layers).
+A step is one full simulation: |0...0> initialisation plus the 20 layers.
+
+value   -- HBM GB/s of the device work with the prepared gate program
+           resident on the GPU: algorithmic bytes (S for the |0> write, 2S per
+           full sweep over the state) / device time (CUDA events on the
+           state's stream), summed over ranks / max time over ranks.
+e2e     -- the same bytes through the public API with host buffers: reset,
+           apply(host gate list), read <Z_i> for all qubits back to the host;
+           wall-clock per step.
+roofline-- the dominant kernel (the multi-gate sweep): 2S per launch / its
+           average launch time, against the measured HBM copy bandwidth.
+
+N>1 ranks (torchrun) run independent replicas (the state does not shard on
+one node at this size): weak scaling, no collective on the data path.
+`--impl reference` times the CPU restatement of the reference's kernels on
+all host cores (bounded sample of the same circuit) on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "30q HBM GB/s"
+UNIT = "GB/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--qubits", type=int, default=30)
+    ap.add_argument("--layers", type=int, default=20)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
+    ap.add_argument("--mode", choices=["auto", "per_gate", "sweep"], default="auto")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def _peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def _workload_desc(a):
+    return (f"random-layer circuit, {a.qubits} qubits, {a.layers} layers, seed {a.seed}, "
+            f"complex {a.precision} state (Rz+Rx on every qubit, CNOT brickwork)")
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.proc = None
+        self.path = None
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 7:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx = float(p[1])
+            except ValueError:
+                continue
+            for name, v in zip(names, p[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline_sample(a, parallel: bool, gates_in_sample: int = 4):
+    """Time the oracle (restated reference kernels) on the first gates of the same circuit.
+    Returns (GB/s, seconds, cores, sample description)."""
+    import oracle
+    from ruqu_b200 import workloads
+    gates = workloads.random_layer_circuit(a.qubits, a.layers, a.seed)[:gates_in_sample]
+    prec = oracle.RQ_F32 if a.precision == "f32" else oracle.RQ_F64
+    st = oracle.OracleState(a.qubits, prec, 0)
+    elem = 8 if a.precision == "f32" else 16
+    S = (1 << a.qubits) * elem
+    nbytes = sum(S if g[0] == 12 else 2 * S for g in gates)
+    t0 = time.perf_counter()
+    st.apply(gates, parallel=parallel)
+    dt = time.perf_counter() - t0
+    cores = oracle.num_threads() if parallel else 1
+    desc = (f"first {len(gates)} gates of the {a.qubits}-qubit circuit on a {a.precision} state, "
+            f"{'OpenMP restatement of the reference parallel kernels' if parallel else 'scalar reference kernels'}"
+            f", {cores} thread(s)")
+    return nbytes / dt / 1e9, dt, cores, desc
+
+
+def run_reference(a):
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    import oracle
+    from ruqu_b200 import workloads
+    gates = workloads.random_layer_circuit(a.qubits, a.layers, a.seed)
+    prec = oracle.RQ_F32 if a.precision == "f32" else oracle.RQ_F64
+    st = oracle.OracleState(a.qubits, prec, 0)
+    elem = 8 if a.precision == "f32" else 16
+    S = (1 << a.qubits) * elem
+    per_step = 4
+    pos = 0
+    times, nbytes = [], []
+    for it in range(a.warmup + a.steps):
+        chunk = [gates[(pos + k) % len(gates)] for k in range(per_step)]
+        pos += per_step
+        b = sum(S if g[0] == 12 else 2 * S for g in chunk)
+        t0 = time.perf_counter()
+        st.apply(chunk, parallel=True)
+        dt = time.perf_counter() - t0
+        if it >= a.warmup:
+            times.append(dt)
+            nbytes.append(b)
+    value = sum(nbytes) / sum(times) / 1e9
+    cores = oracle.num_threads()
+    sample = (f"{per_step} consecutive gates of the {a.qubits}-qubit circuit per step on a {a.precision} state, "
+              f"one pass over the state per gate (the reference's execution model)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": a.precision, "data": "synthetic",
+        "config": {"workload": _workload_desc(a), "l2": "state larger than L2"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(a):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    import ruqu_b200 as rq
+    from ruqu_b200 import workloads
+    from ruqu_b200.circuit import gates_to_array
+
+    ws, rank, local = _dist()
+    dist = ws > 1
+    if dist:
+        import datetime
+
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    rq.set_device(local)
+    torch.cuda.set_device(local)
+
+    mode = {"auto": rq.RQ_EXEC_AUTO, "per_gate": rq.RQ_EXEC_PER_GATE, "sweep": rq.RQ_EXEC_SWEEP}[a.mode]
+    gates = workloads.random_layer_circuit(a.qubits, a.layers, a.seed)
+    garr = gates_to_array(gates)
+    state = rq.QuantumState(a.qubits, 0, a.precision)
+    plan = rq.Plan(state, garr, mode)
+    stats = plan.stats()
+    elem = 8 if a.precision == "f32" else 16
+    S = (1 << a.qubits) * elem
+    step_bytes = S + stats["hbm_bytes"]
+    _, sptr = state.device_pointer()
+    stream = torch.cuda.ExternalStream(sptr, device=torch.device("cuda", local))
+
+    def step(evs=None):
+        # reset = one init kernel (stream-ordered, no host sync); the plan = the sweeps
+        if evs:
+            evs[0].record(stream)
+        state.reset()
+        if evs:
+            evs[1].record(stream)
+        plan.execute(state)
+        if evs:
+            evs[2].record(stream)
+
+    for _ in range(a.warmup):
+        step()
+    state.synchronize()
+
+    clocks = Clocks(local)
+    if dist:
+        tdist.barrier()
+    torch.cuda.synchronize(local)
+    state.synchronize()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(a.steps)]
+    for k in range(a.steps):
+        step(ev[k])
+    state.synchronize()
+    torch.cuda.synchronize(local)
+    clk = clocks.stop()
+    total_ms = ev[0][0].elapsed_time(ev[-1][2])
+    plan_ms = sum(e[1].elapsed_time(e[2]) for e in ev)
+    init_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = ws * step_bytes * a.steps / (total_ms / 1e3) / 1e9
+    peak, peak_kind = _peak()
+    sweeps = max(1, stats["sweeps"] or stats["launches"])
+    avg_launch_ms = plan_ms / (a.steps * sweeps)
+    per_launch_bytes = (stats["hbm_bytes"] / sweeps)
+    achieved = per_launch_bytes / (avg_launch_ms / 1e3) / 1e9
+
+    # ---- end to end through the public API, host buffers ----
+    e2e = None
+    if not a.no_e2e:
+        zs = [[(q, 3)] for q in range(a.qubits)]
+        state.reset()
+        state.apply_gates(garr, mode)
+        state.expectation_values(zs)
+        t0 = time.perf_counter()
+        ksteps = max(1, min(a.steps, 3))
+        for _ in range(ksteps):
+            state.reset()
+            state.apply_gates(garr, mode)
+            state.expectation_values(zs)
+        dt = (time.perf_counter() - t0) / ksteps
+        e2e = {"value": ws * step_bytes / dt / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": len(gates) * C.sizeof(rq._capi.RqGate),
+               "d2h_bytes_per_step": 8 * a.qubits, "ms_per_step": dt * 1e3,
+               "path": "QuantumState.reset + apply_gates(host list) + expectation_values(<Z_i>) -> host"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        v, secs, cores, desc = cpu_baseline_sample(a, parallel=False)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc, "seconds": secs}
+
+    if rank == 0:
+        ref_layer_bytes = workloads.random_layer_bytes(a.qubits, a.layers, elem) + S
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": total_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": a.precision, "data": "synthetic",
+            "config": {"workload": _workload_desc(a), "mode": a.mode, "parallelism": f"replicas x{ws}",
+                       "l2": "state (%.1f GiB) larger than L2, no flush needed" % (S / 2**30),
+                       "sweeps_per_step": stats["sweeps"], "launches_per_step": 1 + stats["launches"],
+                       "phases_per_step": stats["phases"], "device_ops_per_step": stats["ops"],
+                       "bytes_per_step": step_bytes, "layers_per_s": ws * a.layers * a.steps / (total_ms / 1e3),
+                       "ms_init": init_ms / a.steps, "ms_gates": plan_ms / a.steps,
+                       "unfused_reference_bytes_per_step": ref_layer_bytes},
+            "roofline": {"bound": "hbm", "kernel": "k_sweep (multi-gate sweep)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg_launch_ms,
+                         "traffic": None},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": a.steps * (1 + stats["launches"]),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    del plan
+    del state
+    if dist:
+        tdist.barrier()
+        tdist.destroy_process_group()
+
+
+def main():
+    a = _args()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,277 @@
+/*
+ * ruqu_cuda.h -- C-ABI boundary of the B200 state-vector engine.
+ *
+ * Every entry point here replaces one call of ruqu-core's dense state-vector
+ * path (crate `ruqu-core`, files under crates/ruqu-core/src/) or one batched
+ * loop of ruqu-algorithms' QAOA / VQE drivers.  The reference has no backend
+ * trait for this path, so the boundary mirrors the `QuantumState` methods and
+ * the `Simulator` calls one-for-one.  Plain pointers and sizes only; all
+ * host arrays are owned by the caller and never retained after return.
+ *
+ * Threading: one rq_state owns one device buffer and one CUDA stream.  Calls
+ * on one handle must be serialised by the caller (the reference state is a
+ * single-owner `&mut self` value); distinct handles may be driven from
+ * distinct threads.
+ *
+ * Errors: every function returns an rq_status.  Codes 1..5 mirror the
+ * variants of `QuantumError` (crates/ruqu-core/src/error.rs:8-23);
+ * rq_last_error_message() gives the formatted message of the last failure
+ * on the calling thread.
+ */
+#ifndef RUQU_CUDA_H
+#define RUQU_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RQ_API __attribute__((visibility("default")))
+#else
+#define RQ_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- limits (crates/ruqu-core/src/state.rs:15, mixed_precision.rs:185) ---- */
+#define RQ_MAX_QUBITS_F64 32u
+#define RQ_MAX_QUBITS_F32 33u
+
+/* ---- status codes (crates/ruqu-core/src/error.rs:8-23) ---- */
+typedef enum rq_status {
+    RQ_OK = 0,
+    RQ_ERR_QUBIT_LIMIT_EXCEEDED = 1,    /* QuantumError::QubitLimitExceeded      */
+    RQ_ERR_INVALID_QUBIT_INDEX = 2,     /* QuantumError::InvalidQubitIndex       */
+    RQ_ERR_MEMORY_ALLOCATION = 3,       /* QuantumError::MemoryAllocationFailed  */
+    RQ_ERR_INVALID_STATE_VECTOR = 4,    /* QuantumError::InvalidStateVector      */
+    RQ_ERR_CIRCUIT = 5,                 /* QuantumError::CircuitError            */
+    RQ_ERR_CUDA = 6,                    /* a CUDA runtime call failed            */
+    RQ_ERR_TIMEOUT = 7,                 /* a bounded device-side wait expired    */
+    RQ_ERR_INVALID_ARGUMENT = 8         /* null pointer / bad enum / bad size    */
+} rq_status;
+
+/* ---- amplitude precision ---- */
+typedef enum rq_precision {
+    RQ_F32 = 0,   /* interleaved complex float  (QuantumStateF32, mixed_precision.rs:193) */
+    RQ_F64 = 1    /* interleaved complex double (QuantumState, state.rs:18)               */
+} rq_precision;
+
+/* ---- gate kinds, in the order of `enum Gate` (crates/ruqu-core/src/gate.rs:8-36) ---- */
+typedef enum rq_gate_kind {
+    RQ_GATE_H = 0,
+    RQ_GATE_X = 1,
+    RQ_GATE_Y = 2,
+    RQ_GATE_Z = 3,
+    RQ_GATE_S = 4,
+    RQ_GATE_SDG = 5,
+    RQ_GATE_T = 6,
+    RQ_GATE_TDG = 7,
+    RQ_GATE_RX = 8,
+    RQ_GATE_RY = 9,
+    RQ_GATE_RZ = 10,
+    RQ_GATE_PHASE = 11,
+    RQ_GATE_CNOT = 12,       /* q0 = control, q1 = target */
+    RQ_GATE_CZ = 13,
+    RQ_GATE_SWAP = 14,
+    RQ_GATE_RZZ = 15,
+    RQ_GATE_MEASURE = 16,
+    RQ_GATE_RESET = 17,
+    RQ_GATE_BARRIER = 18,
+    RQ_GATE_UNITARY1Q = 19   /* m[] holds the 2x2 matrix */
+} rq_gate_kind;
+
+/* One gate, plain old data (replaces `Gate`, gate.rs:8-36). */
+typedef struct rq_gate {
+    int32_t  kind;      /* rq_gate_kind                                            */
+    uint32_t q0;        /* the qubit (1q gates) / first qubit (2q gates)           */
+    uint32_t q1;        /* second qubit of 2q gates, ignored otherwise             */
+    uint32_t pad;       /* zero                                                    */
+    double   angle;     /* Rx/Ry/Rz/Phase/Rzz angle in radians                     */
+    double   m[8];      /* UNITARY1Q: m00 m01 m10 m11 as (re,im) pairs, row-major  */
+} rq_gate;
+
+/* One measurement result (replaces `MeasurementOutcome`, types.rs:230-235). */
+typedef struct rq_measurement {
+    uint32_t qubit;
+    int32_t  result;       /* 1 = measured |1> */
+    double   probability;  /* probability of the observed branch */
+} rq_measurement;
+
+/* Pauli factors (replaces `PauliOp`, types.rs:190-197). */
+typedef enum rq_pauli { RQ_PAULI_I = 0, RQ_PAULI_X = 1, RQ_PAULI_Y = 2, RQ_PAULI_Z = 3 } rq_pauli;
+
+typedef struct rq_pauli_op {
+    uint32_t qubit;
+    int32_t  op;           /* rq_pauli */
+} rq_pauli_op;
+
+/* Execution modes for rq_state_apply (the reference always runs one pass per gate). */
+typedef enum rq_exec_mode {
+    RQ_EXEC_AUTO = 0,      /* autotuned choice (default) */
+    RQ_EXEC_PER_GATE = 1,  /* one kernel per gate: the unfused path              */
+    RQ_EXEC_SWEEP = 2      /* register/shared-memory tiled multi-gate sweeps     */
+} rq_exec_mode;
+
+typedef struct rq_state rq_state;   /* opaque: device-resident amplitudes */
+typedef struct rq_plan rq_plan;     /* opaque: a gate list prepared for one state shape */
+
+/* What a prepared plan launches (filled by rq_plan_get_stats). */
+typedef struct rq_plan_stats {
+    uint64_t gates;       /* unitary gates in the plan                          */
+    uint64_t launches;    /* kernel launches per execution                      */
+    uint64_t sweeps;      /* full passes over the state (sweep mode)            */
+    uint64_t phases;      /* register phases summed over all sweeps             */
+    uint64_t ops;         /* device ops after 1-qubit fusion                    */
+    uint64_t hbm_bytes;   /* algorithmic HBM bytes per execution                */
+} rq_plan_stats;
+
+/* ------------------------------------------------------------------------ */
+/* errors / library                                                          */
+/* ------------------------------------------------------------------------ */
+
+/* Message of the last failing call on this thread ("" if none). */
+RQ_API const char* rq_last_error_message(void);
+
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+RQ_API int32_t rq_version(void);
+
+/* One draw of the documented uniform stream (Philox4x32-10, Salmon et al.,
+ * SC'11): u in [0,1) with 53 random bits.  Draw `index` of `stream` under
+ * key `seed`.  Stream 0 feeds measurements; shot s of a run_shots call with
+ * base seed b uses key b+s (wrapping), mirroring simulator.rs:124-130. */
+RQ_API double rq_uniform(uint64_t seed, uint32_t stream, uint64_t index);
+
+/* Select the CUDA device used by states created afterwards on this thread. */
+RQ_API int rq_device_set(int32_t device);
+RQ_API int rq_device_count(int32_t* out);
+
+/* ------------------------------------------------------------------------ */
+/* state lifetime (state.rs:31-96, mixed_precision.rs:214-280)               */
+/* ------------------------------------------------------------------------ */
+
+/* QuantumState::new / new_with_seed (seeded != 0).  |0...0>.  0 qubits is a
+ * CircuitError for both (state.rs:32-36 checks it in `new` only; the seeded
+ * constructor would build a 1-amplitude state -- we reject it in both). */
+RQ_API int rq_state_create(uint32_t num_qubits, int32_t precision, uint64_t seed,
+                    int32_t seeded, rq_state** out);
+
+/* QuantumState::from_amplitudes (state.rs:75-96): `len` complex values given
+ * as 2*len interleaved doubles; len must equal 2^num_qubits. */
+RQ_API int rq_state_from_amplitudes(const double* interleaved, uint64_t len,
+                             uint32_t num_qubits, int32_t precision,
+                             uint64_t seed, rq_state** out);
+
+RQ_API int rq_state_destroy(rq_state* s);
+
+/* Back to |0...0>, measurement stream rewound to draw 0 of the same seed.
+ * Stream-ordered: returns once the init kernel is queued. */
+RQ_API int rq_state_reset(rq_state* s);
+
+RQ_API int rq_state_num_qubits(const rq_state* s, uint32_t* out);
+RQ_API int rq_state_precision(const rq_state* s, int32_t* out);
+
+/* Device pointer of the amplitudes (interleaved complex) and its stream, for
+ * zero-copy interop; valid until rq_state_destroy. */
+RQ_API int rq_state_device_ptr(const rq_state* s, void** out_ptr, void** out_stream);
+
+/* Block the host until all work queued on the state's stream is done. */
+RQ_API int rq_state_synchronize(rq_state* s);
+
+/* ------------------------------------------------------------------------ */
+/* gates (state.rs:158-276)                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* Apply `n` gates in order (QuantumState::apply_gate in a loop, as
+ * Simulator::run_with_config does, simulator.rs:69-79).  Validation happens
+ * for the whole list before anything runs; an invalid gate returns its error
+ * and leaves the state untouched.  Measure/Reset outcomes are written to
+ * `out` (capacity `cap`); their count goes to *nout (out may be NULL when
+ * the list has no Measure/Reset). */
+RQ_API int rq_state_apply(rq_state* s, const rq_gate* gates, uint64_t n,
+                   rq_measurement* out, uint64_t cap, uint64_t* nout);
+
+/* Same, with an explicit execution mode (rq_exec_mode). */
+RQ_API int rq_state_apply_mode(rq_state* s, const rq_gate* gates, uint64_t n,
+                        int32_t mode, rq_measurement* out, uint64_t cap,
+                        uint64_t* nout);
+
+/* apply_single_qubit_gate (state.rs:214-229): m = 8 doubles, (re,im) pairs. */
+RQ_API int rq_state_apply_1q_matrix(rq_state* s, uint32_t qubit, const double* m);
+
+/* apply_two_qubit_gate (state.rs:238-276): m = 32 doubles, 4x4 row-major,
+ * row/column index = q1_bit*2 + q2_bit. */
+RQ_API int rq_state_apply_2q_matrix(rq_state* s, uint32_t q1, uint32_t q2,
+                             const double* m);
+
+/* Prepared plans: the gate list of Simulator::run_with_config
+ * (simulator.rs:69-79) planned once for states of s's qubit count and
+ * precision, with its tables uploaded to the device.  rq_plan_execute only
+ * launches kernels on the state's stream (no host sync, no allocation), so a
+ * plan can be replayed cheaply or captured in a CUDA graph.  Unitary gates
+ * only (Measure / Reset are rejected with RQ_ERR_CIRCUIT; Barrier is
+ * dropped).  mode: rq_exec_mode. */
+RQ_API int rq_plan_create(const rq_state* s, const rq_gate* gates, uint64_t n,
+                          int32_t mode, rq_plan** out);
+RQ_API int rq_plan_execute(rq_state* s, const rq_plan* p);
+RQ_API int rq_plan_get_stats(const rq_plan* p, rq_plan_stats* out);
+RQ_API int rq_plan_destroy(rq_plan* p);
+
+/* ------------------------------------------------------------------------ */
+/* measurement (state.rs:288-352)                                            */
+/* ------------------------------------------------------------------------ */
+
+RQ_API int rq_state_measure(rq_state* s, uint32_t qubit, rq_measurement* out);
+RQ_API int rq_state_measure_all(rq_state* s, rq_measurement* out /* num_qubits */);
+RQ_API int rq_state_reset_qubit(rq_state* s, uint32_t qubit);
+
+/* Shot sampling without collapse.  Reproduces, shot by shot, the outcome of
+ * Simulator::run_shots (simulator.rs:107-147): shot s measures `qubits` in
+ * the given order with draws 0,1,2,... of key base_seed+s, outcome 1 iff
+ * u >= P(qubit=0 | earlier outcomes).  out_bits[s] has bit q set iff qubit q
+ * was measured as 1.  The state is not modified. */
+RQ_API int rq_state_sample(rq_state* s, const uint32_t* qubits, uint32_t nqubits,
+                    uint64_t base_seed, uint64_t shots, uint64_t* out_bits);
+
+/* ------------------------------------------------------------------------ */
+/* reductions (state.rs:123-137, 362-435)                                    */
+/* ------------------------------------------------------------------------ */
+
+/* |a_i|^2 for all i into host memory (2^n doubles). */
+RQ_API int rq_state_probabilities(rq_state* s, double* out);
+
+RQ_API int rq_state_probability_of_qubit(rq_state* s, uint32_t qubit, double* out);
+
+/* expectation_value(PauliString) (state.rs:362-400), FP64 accumulation. */
+RQ_API int rq_state_expectation_value(rq_state* s, const rq_pauli_op* ops,
+                               uint32_t nops, double* out);
+
+/* Many Pauli strings in one call: string k is ops[offsets[k] .. offsets[k+1]).
+ * out[k] = <P_k>. */
+RQ_API int rq_state_expectation_batch(rq_state* s, const rq_pauli_op* ops,
+                               const uint32_t* offsets, uint32_t nstrings,
+                               double* out);
+
+/* expectation_hamiltonian (state.rs:403-408): sum_k coeffs[k] <P_k>. */
+RQ_API int rq_state_expectation_hamiltonian(rq_state* s, const double* coeffs,
+                                     const rq_pauli_op* ops,
+                                     const uint32_t* offsets, uint32_t nterms,
+                                     double* out);
+
+RQ_API int rq_state_norm_sq(rq_state* s, double* out);
+RQ_API int rq_state_normalize(rq_state* s);                         /* state.rs:415-423 */
+RQ_API int rq_state_fidelity(rq_state* a, rq_state* b, double* out); /* state.rs:426-435 */
+
+/* ------------------------------------------------------------------------ */
+/* host transfer (state_vector / amplitudes_mut / from_amplitudes)           */
+/* ------------------------------------------------------------------------ */
+
+/* 2^n complex values as 2^(n+1) interleaved doubles. */
+RQ_API int rq_state_download(rq_state* s, double* interleaved);
+RQ_API int rq_state_upload(rq_state* s, const double* interleaved);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RUQU_CUDA_H */

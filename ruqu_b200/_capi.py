@@ -1,0 +1,98 @@
+"""ctypes binding of libruqu_cuda.so (the C ABI declared in include/ruqu_cuda.h).
+
+The library is the only compute path: if it is missing this module raises
+at import, and every call that fails on the device raises QuantumError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libruqu_cuda.so")
+
+RQ_F32, RQ_F64 = 0, 1
+RQ_EXEC_AUTO, RQ_EXEC_PER_GATE, RQ_EXEC_SWEEP = 0, 1, 2
+
+(RQ_OK, RQ_ERR_QUBIT_LIMIT_EXCEEDED, RQ_ERR_INVALID_QUBIT_INDEX, RQ_ERR_MEMORY_ALLOCATION,
+ RQ_ERR_INVALID_STATE_VECTOR, RQ_ERR_CIRCUIT, RQ_ERR_CUDA, RQ_ERR_TIMEOUT, RQ_ERR_INVALID_ARGUMENT) = range(9)
+
+
+class RqGate(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("q0", C.c_uint32), ("q1", C.c_uint32), ("pad", C.c_uint32),
+                ("angle", C.c_double), ("m", C.c_double * 8)]
+
+
+class RqMeasurement(C.Structure):
+    _fields_ = [("qubit", C.c_uint32), ("result", C.c_int32), ("probability", C.c_double)]
+
+
+class RqPauliOp(C.Structure):
+    _fields_ = [("qubit", C.c_uint32), ("op", C.c_int32)]
+
+
+class RqPlanStats(C.Structure):
+    _fields_ = [("gates", C.c_uint64), ("launches", C.c_uint64), ("sweeps", C.c_uint64), ("phases", C.c_uint64),
+                ("ops", C.c_uint64), ("hbm_bytes", C.c_uint64)]
+
+
+# name -> (restype, argtypes); every symbol here is declared in include/ruqu_cuda.h
+_P = C.POINTER
+_u32, _u64, _i32, _dbl, _vp = C.c_uint32, C.c_uint64, C.c_int32, C.c_double, C.c_void_p
+SIGNATURES = {
+    "rq_last_error_message": (C.c_char_p, []),
+    "rq_version": (_i32, []),
+    "rq_uniform": (_dbl, [_u64, _u32, _u64]),
+    "rq_device_set": (C.c_int, [_i32]),
+    "rq_device_count": (C.c_int, [_P(_i32)]),
+    "rq_plan_create": (C.c_int, [_vp, _P(RqGate), _u64, _i32, _P(_vp)]),
+    "rq_plan_execute": (C.c_int, [_vp, _vp]),
+    "rq_plan_get_stats": (C.c_int, [_vp, _P(RqPlanStats)]),
+    "rq_plan_destroy": (C.c_int, [_vp]),
+    "rq_state_create": (C.c_int, [_u32, _i32, _u64, _i32, _P(_vp)]),
+    "rq_state_from_amplitudes": (C.c_int, [_P(_dbl), _u64, _u32, _i32, _u64, _P(_vp)]),
+    "rq_state_destroy": (C.c_int, [_vp]),
+    "rq_state_reset": (C.c_int, [_vp]),
+    "rq_state_num_qubits": (C.c_int, [_vp, _P(_u32)]),
+    "rq_state_precision": (C.c_int, [_vp, _P(_i32)]),
+    "rq_state_device_ptr": (C.c_int, [_vp, _P(_vp), _P(_vp)]),
+    "rq_state_synchronize": (C.c_int, [_vp]),
+    "rq_state_apply": (C.c_int, [_vp, _P(RqGate), _u64, _P(RqMeasurement), _u64, _P(_u64)]),
+    "rq_state_apply_mode": (C.c_int, [_vp, _P(RqGate), _u64, _i32, _P(RqMeasurement), _u64, _P(_u64)]),
+    "rq_state_apply_1q_matrix": (C.c_int, [_vp, _u32, _P(_dbl)]),
+    "rq_state_apply_2q_matrix": (C.c_int, [_vp, _u32, _u32, _P(_dbl)]),
+    "rq_state_measure": (C.c_int, [_vp, _u32, _P(RqMeasurement)]),
+    "rq_state_measure_all": (C.c_int, [_vp, _P(RqMeasurement)]),
+    "rq_state_reset_qubit": (C.c_int, [_vp, _u32]),
+    "rq_state_sample": (C.c_int, [_vp, _P(_u32), _u32, _u64, _u64, _P(_u64)]),
+    "rq_state_probabilities": (C.c_int, [_vp, _P(_dbl)]),
+    "rq_state_probability_of_qubit": (C.c_int, [_vp, _u32, _P(_dbl)]),
+    "rq_state_expectation_value": (C.c_int, [_vp, _P(RqPauliOp), _u32, _P(_dbl)]),
+    "rq_state_expectation_batch": (C.c_int, [_vp, _P(RqPauliOp), _P(_u32), _u32, _P(_dbl)]),
+    "rq_state_expectation_hamiltonian": (C.c_int, [_vp, _P(_dbl), _P(RqPauliOp), _P(_u32), _u32, _P(_dbl)]),
+    "rq_state_norm_sq": (C.c_int, [_vp, _P(_dbl)]),
+    "rq_state_normalize": (C.c_int, [_vp]),
+    "rq_state_fidelity": (C.c_int, [_vp, _vp, _P(_dbl)]),
+    "rq_state_download": (C.c_int, [_vp, _P(_dbl)]),
+    "rq_state_upload": (C.c_int, [_vp, _P(_dbl)]),
+}
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: the CUDA library is the only compute path of ruqu_b200. "
+            "Build it with `python -m ruqu_b200.build`.")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    return lib.rq_last_error_message().decode(errors="replace")

@@ -1,0 +1,656 @@
+// rq_capi.cu -- the extern "C" boundary (include/ruqu_cuda.h).
+//
+// Host-side validation mirrors QuantumState::apply_gate (state.rs:158-204)
+// and the constructors (state.rs:31-96); gate matrices are built on the host
+// in f64 exactly as Gate::matrix_1q / matrix_2q do (gate.rs:72-198) and are
+// narrowed to f32 for f32 states like convert_matrix_1q/2q
+// (mixed_precision.rs:556-591).  Kernels live in rq_gates.cu, rq_reduce.cu,
+// rq_sample.cu and rq_sweep.cu; nothing here computes on amplitudes.
+#include "rq_internal.cuh"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <random>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_last_error;
+
+const double kFrac1Sqrt2 = 0.70710678118654752440;
+
+bool is_2q(int k) { return k == RQ_GATE_CNOT || k == RQ_GATE_CZ || k == RQ_GATE_SWAP || k == RQ_GATE_RZZ; }
+
+// Gate::matrix_1q (gate.rs:72-146) as 8 doubles, (re,im) row-major
+bool matrix_1q(const rq_gate& g, double m[8]) {
+    auto set = [&](double a, double b, double c, double d, double e, double f, double h, double i) {
+        m[0] = a; m[1] = b; m[2] = c; m[3] = d; m[4] = e; m[5] = f; m[6] = h; m[7] = i;
+    };
+    const double s = kFrac1Sqrt2;
+    switch (g.kind) {
+        case RQ_GATE_H: set(s, 0, s, 0, s, 0, -s, -0.0); return true;
+        case RQ_GATE_X: set(0, 0, 1, 0, 1, 0, 0, 0); return true;
+        case RQ_GATE_Y: set(0, 0, -0.0, -1, 0, 1, 0, 0); return true;
+        case RQ_GATE_Z: set(1, 0, 0, 0, 0, 0, -1, -0.0); return true;
+        case RQ_GATE_S: set(1, 0, 0, 0, 0, 0, 0, 1); return true;
+        case RQ_GATE_SDG: set(1, 0, 0, 0, 0, 0, -0.0, -1); return true;
+        case RQ_GATE_T: set(1, 0, 0, 0, 0, 0, s, s); return true;
+        case RQ_GATE_TDG: set(1, 0, 0, 0, 0, 0, s, -s); return true;
+        case RQ_GATE_RX: {
+            double h = g.angle / 2.0, c = std::cos(h), sn = -std::sin(h);
+            set(c, 0, 0, sn, 0, sn, c, 0); return true;
+        }
+        case RQ_GATE_RY: {
+            double h = g.angle / 2.0, c = std::cos(h), sn = std::sin(h);
+            set(c, 0, -sn, 0, sn, 0, c, 0); return true;
+        }
+        case RQ_GATE_RZ: {
+            double h = g.angle / 2.0;
+            set(std::cos(-h), std::sin(-h), 0, 0, 0, 0, std::cos(h), std::sin(h)); return true;
+        }
+        case RQ_GATE_PHASE: set(1, 0, 0, 0, 0, 0, std::cos(g.angle), std::sin(g.angle)); return true;
+        case RQ_GATE_UNITARY1Q: std::memcpy(m, g.m, sizeof(double) * 8); return true;
+        default: return false;
+    }
+}
+
+bool is_diag_1q(int k) {
+    return k == RQ_GATE_Z || k == RQ_GATE_S || k == RQ_GATE_SDG || k == RQ_GATE_T || k == RQ_GATE_TDG ||
+           k == RQ_GATE_RZ || k == RQ_GATE_PHASE;
+}
+
+int validate_gate(const rq_state* s, const rq_gate& g) {
+    if (g.kind < RQ_GATE_H || g.kind > RQ_GATE_UNITARY1Q)
+        return rq::fail(RQ_ERR_CIRCUIT, "circuit error: unsupported gate kind " + std::to_string(g.kind));
+    if (g.kind == RQ_GATE_BARRIER) return RQ_OK;
+    uint32_t qs[2] = {g.q0, g.q1};
+    int nq = is_2q(g.kind) ? 2 : 1;
+    for (int k = 0; k < nq; ++k)
+        if (qs[k] >= s->nq)
+            return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "invalid qubit index " + std::to_string(qs[k]) + " for " +
+                                                            std::to_string(s->nq) + "-qubit system");
+    if (nq == 2 && g.q0 == g.q1)
+        return rq::fail(RQ_ERR_CIRCUIT, "circuit error: two-qubit gate requires distinct qubits, got " +
+                                            std::to_string(g.q0) + " and " + std::to_string(g.q1));
+    return RQ_OK;
+}
+
+int device_of_current() {
+    int d = 0;
+    cudaGetDevice(&d);
+    return d;
+}
+
+int set_device(const rq_state* s) {
+    RQ_CUDA(cudaSetDevice(s->device));
+    return RQ_OK;
+}
+
+int check_create(uint32_t nq, int32_t prec) {
+    if (prec != RQ_F32 && prec != RQ_F64) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "precision must be RQ_F32 or RQ_F64");
+    uint32_t maxq = prec == RQ_F32 ? RQ_MAX_QUBITS_F32 : RQ_MAX_QUBITS_F64;
+    if (nq == 0) return rq::fail(RQ_ERR_CIRCUIT, "circuit error: cannot create quantum state with 0 qubits");
+    if (nq > maxq)
+        return rq::fail(RQ_ERR_QUBIT_LIMIT_EXCEEDED, "qubit limit exceeded: requested " + std::to_string(nq) +
+                                                         ", maximum " + std::to_string(maxq));
+    return RQ_OK;
+}
+
+int alloc_state(uint32_t nq, int32_t prec, uint64_t seed, rq_state** out) {
+    rq_state* s = new rq_state();
+    s->nq = nq;
+    s->prec = prec;
+    s->n = 1ull << nq;
+    s->seed = seed;
+    s->device = device_of_current();
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete s;
+        return rq::cuda_fail(e, "cudaStreamCreateWithFlags");
+    }
+    e = cudaMalloc(&s->amps, s->bytes());
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        size_t need = s->bytes();
+        cudaStreamDestroy(s->stream);
+        delete s;
+        return rq::fail(RQ_ERR_MEMORY_ALLOCATION, "memory allocation failed: need " + std::to_string(need) + " bytes");
+    }
+    *out = s;
+    return RQ_OK;
+}
+
+uint64_t entropy_seed() {
+    std::random_device rd;
+    return ((uint64_t)rd() << 32) ^ rd();
+}
+
+int to_masks(const rq_state* s, const rq_pauli_op* ops, uint32_t nops, rq::PauliMask* m) {
+    m->xmask = 0;
+    m->pmask = 0;
+    m->ny = 0;
+    for (uint32_t k = 0; k < nops; ++k) {
+        uint32_t q = ops[k].qubit;
+        int op = ops[k].op;
+        if (op < RQ_PAULI_I || op > RQ_PAULI_Z)
+            return rq::fail(RQ_ERR_INVALID_ARGUMENT, "invalid Pauli operator " + std::to_string(op));
+        if (op == RQ_PAULI_I) continue;
+        if (q >= s->nq)
+            return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "invalid qubit index " + std::to_string(q) + " for " +
+                                                            std::to_string(s->nq) + "-qubit system");
+        uint64_t b = 1ull << q;
+        if (op == RQ_PAULI_X || op == RQ_PAULI_Y) m->xmask ^= b;
+        if (op == RQ_PAULI_Y || op == RQ_PAULI_Z) m->pmask ^= b;
+        if (op == RQ_PAULI_Y) m->ny += 1;
+    }
+    m->ny &= 3u;
+    return RQ_OK;
+}
+
+int do_measure(rq_state* s, uint32_t q, rq_measurement* out) {
+    double p0 = 0.0;
+    RQ_TRY(rq::prob_bit(s, q, 0, &p0));
+    double u = rqd::uniform(s->seed, 0, s->draws++);
+    int result = u >= p0 ? 1 : 0;
+    double prob = result ? 1.0 - p0 : p0;
+    double nf = prob > 0.0 ? 1.0 / std::sqrt(prob) : 0.0;
+    RQ_TRY(rq::collapse(s, q, result, nf));
+    if (out) {
+        out->qubit = q;
+        out->result = result;
+        out->probability = prob;
+    }
+    return RQ_OK;
+}
+
+int do_reset(rq_state* s, uint32_t q) {
+    rq_measurement m;
+    RQ_TRY(do_measure(s, q, &m));
+    if (m.result) {
+        double x[8] = {0, 0, 1, 0, 1, 0, 0, 0};
+        RQ_TRY(rq::gate1q(s, q, x));
+    }
+    return RQ_OK;
+}
+
+}  // namespace
+
+// one unitary gate through the per-gate kernels
+int rq::apply_one_gate(rq_state* s, const rq_gate& g) {
+    switch (g.kind) {
+        case RQ_GATE_CNOT: return rq::gate_cnot(s, g.q0, g.q1);
+        case RQ_GATE_CZ: return rq::gate_cz(s, g.q0, g.q1);
+        case RQ_GATE_SWAP: return rq::gate_swap(s, g.q0, g.q1);
+        case RQ_GATE_RZZ: {
+            double h = g.angle / 2.0;
+            double en_r = std::cos(-h), en_i = std::sin(-h), ep_r = std::cos(h), ep_i = std::sin(h);
+            double d[8] = {en_r, en_i, ep_r, ep_i, ep_r, ep_i, en_r, en_i};
+            return rq::gate2q_diag(s, g.q0, g.q1, d);
+        }
+        default: break;
+    }
+    double m[8];
+    if (!matrix_1q(g, m)) return rq::fail(RQ_ERR_CIRCUIT, "circuit error: unsupported gate");
+    if (is_diag_1q(g.kind)) {
+        double d[4] = {m[0], m[1], m[6], m[7]};
+        return rq::gate1q_diag(s, g.q0, d);
+    }
+    return rq::gate1q(s, g.q0, m);
+}
+
+namespace {
+
+bool is_unitary(int k) { return k != RQ_GATE_MEASURE && k != RQ_GATE_RESET && k != RQ_GATE_BARRIER; }
+
+}  // namespace
+
+// ===========================================================================
+// internal helpers shared by the translation units
+// ===========================================================================
+namespace rq {
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    g_last_error = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+    return RQ_ERR_CUDA;
+}
+
+int num_sms(int device) {
+    static std::mutex mu;
+    static int cache[64] = {0};
+    if (device < 0 || device >= 64) return 148;
+    std::lock_guard<std::mutex> lk(mu);
+    if (cache[device] == 0) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v <= 0) v = 148;
+        cache[device] = v;
+    }
+    return cache[device];
+}
+
+int ensure_partials(rq_state* s, size_t nd) {
+    if (s->partials_cap >= nd) return RQ_OK;
+    if (s->partials) {
+        RQ_CUDA(cudaStreamSynchronize(s->stream));
+        cudaFree(s->partials);
+        s->partials = nullptr;
+        s->partials_cap = 0;
+    }
+    size_t cap = nd < 4096 ? 4096 : nd;
+    RQ_CUDA(cudaMalloc(&s->partials, cap * sizeof(double)));
+    s->partials_cap = cap;
+    return RQ_OK;
+}
+
+int ensure_hbuf(rq_state* s, size_t nd) {
+    if (s->hbuf_cap >= nd) return RQ_OK;
+    if (s->hbuf) {
+        RQ_CUDA(cudaStreamSynchronize(s->stream));
+        cudaFreeHost(s->hbuf);
+        s->hbuf = nullptr;
+        s->hbuf_cap = 0;
+    }
+    size_t cap = nd < 1024 ? 1024 : nd;
+    RQ_CUDA(cudaMallocHost(&s->hbuf, cap * sizeof(double)));
+    s->hbuf_cap = cap;
+    return RQ_OK;
+}
+
+int ensure_tree(rq_state* s, size_t nd) {
+    if (s->tree_cap >= nd) return RQ_OK;
+    if (s->tree) {
+        RQ_CUDA(cudaStreamSynchronize(s->stream));
+        cudaFree(s->tree);
+        s->tree = nullptr;
+        s->tree_cap = 0;
+    }
+    cudaError_t e = cudaMalloc(&s->tree, nd * sizeof(double));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(RQ_ERR_MEMORY_ALLOCATION, "memory allocation failed: need " + std::to_string(nd * sizeof(double)) +
+                                                  " bytes of sampling scratch");
+    }
+    s->tree_cap = nd;
+    return RQ_OK;
+}
+
+}  // namespace rq
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* rq_last_error_message(void) { return g_last_error.c_str(); }
+
+int32_t rq_version(void) { return 100; }
+
+double rq_uniform(uint64_t seed, uint32_t stream, uint64_t index) { return rqd::uniform(seed, stream, index); }
+
+int rq_state_create(uint32_t num_qubits, int32_t precision, uint64_t seed, int32_t seeded, rq_state** out) {
+    if (!out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null output pointer");
+    RQ_TRY(check_create(num_qubits, precision));
+    rq_state* s = nullptr;
+    RQ_TRY(alloc_state(num_qubits, precision, seeded ? seed : entropy_seed(), &s));
+    int rc = rq::init_basis(s, 0);
+    if (rc == RQ_OK) {
+        cudaError_t e = cudaStreamSynchronize(s->stream);
+        if (e != cudaSuccess) rc = rq::cuda_fail(e, "cudaStreamSynchronize");
+    }
+    if (rc != RQ_OK) {
+        rq_state_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return RQ_OK;
+}
+
+int rq_state_from_amplitudes(const double* interleaved, uint64_t len, uint32_t num_qubits, int32_t precision,
+                             uint64_t seed, rq_state** out) {
+    if (!out || (!interleaved && len)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (precision != RQ_F32 && precision != RQ_F64)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "precision must be RQ_F32 or RQ_F64");
+    uint32_t maxq = precision == RQ_F32 ? RQ_MAX_QUBITS_F32 : RQ_MAX_QUBITS_F64;
+    if (num_qubits > maxq)
+        return rq::fail(RQ_ERR_QUBIT_LIMIT_EXCEEDED, "qubit limit exceeded: requested " + std::to_string(num_qubits) +
+                                                         ", maximum " + std::to_string(maxq));
+    if (num_qubits == 0 || len != (1ull << num_qubits))
+        return rq::fail(RQ_ERR_INVALID_STATE_VECTOR, "invalid state vector: length " + std::to_string(len) +
+                                                         " does not match 2^" + std::to_string(num_qubits));
+    rq_state* s = nullptr;
+    RQ_TRY(alloc_state(num_qubits, precision, seed, &s));
+    int rc = rq_state_upload(s, interleaved);
+    if (rc != RQ_OK) {
+        rq_state_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return RQ_OK;
+}
+
+int rq_device_set(int32_t device) {
+    RQ_CUDA(cudaSetDevice(device));
+    return RQ_OK;
+}
+
+int rq_device_count(int32_t* out) {
+    if (!out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    int n = 0;
+    RQ_CUDA(cudaGetDeviceCount(&n));
+    *out = n;
+    return RQ_OK;
+}
+
+int rq_plan_create(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out) {
+    if (!s || !out || (!gates && n)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (mode < RQ_EXEC_AUTO || mode > RQ_EXEC_SWEEP) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "bad execution mode");
+    for (uint64_t k = 0; k < n; ++k) {
+        RQ_TRY(validate_gate(s, gates[k]));
+        if (gates[k].kind == RQ_GATE_MEASURE || gates[k].kind == RQ_GATE_RESET)
+            return rq::fail(RQ_ERR_CIRCUIT, "circuit error: a plan holds unitary gates only");
+    }
+    RQ_TRY(set_device(s));
+    int use_sweep = (mode == RQ_EXEC_SWEEP || (mode == RQ_EXEC_AUTO && s->nq >= 12)) && s->nq >= 7;
+    return rq::plan_build(s, gates, n, use_sweep ? RQ_EXEC_SWEEP : RQ_EXEC_PER_GATE, out);
+}
+
+int rq_plan_execute(rq_state* s, const rq_plan* p) {
+    if (!s || !p) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (!rq::plan_fits(p, s))
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "plan was built for another qubit count, precision or device");
+    RQ_TRY(set_device(s));
+    return rq::plan_launch(s, p);
+}
+
+int rq_plan_get_stats(const rq_plan* p, rq_plan_stats* out) {
+    if (!p || !out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    *out = rq::plan_stats(p);
+    return RQ_OK;
+}
+
+int rq_plan_destroy(rq_plan* p) {
+    rq::plan_free(p);
+    return RQ_OK;
+}
+
+int rq_state_destroy(rq_state* s) {
+    if (!s) return RQ_OK;
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->amps) cudaFree(s->amps);
+    if (s->partials) cudaFree(s->partials);
+    if (s->tree) cudaFree(s->tree);
+    if (s->hbuf) cudaFreeHost(s->hbuf);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return RQ_OK;
+}
+
+int rq_state_reset(rq_state* s) {
+    if (!s) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null state");
+    RQ_TRY(set_device(s));
+    s->draws = 0;
+    return rq::init_basis(s, 0);   // stream-ordered; later calls on s see the reset state
+}
+
+int rq_state_num_qubits(const rq_state* s, uint32_t* out) {
+    if (!s || !out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    *out = s->nq;
+    return RQ_OK;
+}
+
+int rq_state_precision(const rq_state* s, int32_t* out) {
+    if (!s || !out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    *out = s->prec;
+    return RQ_OK;
+}
+
+int rq_state_device_ptr(const rq_state* s, void** out_ptr, void** out_stream) {
+    if (!s) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null state");
+    if (out_ptr) *out_ptr = s->amps;
+    if (out_stream) *out_stream = (void*)s->stream;
+    return RQ_OK;
+}
+
+int rq_state_synchronize(rq_state* s) {
+    if (!s) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null state");
+    RQ_TRY(set_device(s));
+    RQ_CUDA(cudaStreamSynchronize(s->stream));
+    return RQ_OK;
+}
+
+int rq_state_apply_mode(rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_measurement* out,
+                        uint64_t cap, uint64_t* nout) {
+    if (!s || (!gates && n)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (mode < RQ_EXEC_AUTO || mode > RQ_EXEC_SWEEP) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "bad execution mode");
+    RQ_TRY(set_device(s));
+    for (uint64_t k = 0; k < n; ++k) RQ_TRY(validate_gate(s, gates[k]));
+    // states below 7 qubits are smaller than one sweep tile: per-gate kernels
+    int use_sweep = (mode == RQ_EXEC_SWEEP || (mode == RQ_EXEC_AUTO && s->nq >= 12)) && s->nq >= 7;
+    uint64_t nm = 0;
+    uint64_t k = 0;
+    while (k < n) {
+        const rq_gate& g = gates[k];
+        if (g.kind == RQ_GATE_BARRIER) { ++k; continue; }
+        if (g.kind == RQ_GATE_MEASURE || g.kind == RQ_GATE_RESET) {
+            rq_measurement m;
+            if (g.kind == RQ_GATE_MEASURE) {
+                RQ_TRY(do_measure(s, g.q0, &m));
+                if (out && nm < cap) out[nm] = m;
+                ++nm;
+            } else {
+                RQ_TRY(do_reset(s, g.q0));
+            }
+            ++k;
+            continue;
+        }
+        // maximal run of unitary gates (barriers inside a run are no-ops)
+        uint64_t e = k;
+        while (e < n && (is_unitary(gates[e].kind) || gates[e].kind == RQ_GATE_BARRIER)) ++e;
+        if (use_sweep) {
+            std::vector<rq_gate> run;
+            run.reserve(e - k);
+            for (uint64_t j = k; j < e; ++j)
+                if (gates[j].kind != RQ_GATE_BARRIER) run.push_back(gates[j]);
+            RQ_TRY(rq::apply_sweeps(s, run.data(), run.size()));
+        } else {
+            for (uint64_t j = k; j < e; ++j)
+                if (gates[j].kind != RQ_GATE_BARRIER) RQ_TRY(rq::apply_one_gate(s, gates[j]));
+        }
+        k = e;
+    }
+    if (nout) *nout = nm;
+    return RQ_OK;
+}
+
+int rq_state_apply(rq_state* s, const rq_gate* gates, uint64_t n, rq_measurement* out, uint64_t cap,
+                   uint64_t* nout) {
+    return rq_state_apply_mode(s, gates, n, s ? s->exec_mode : RQ_EXEC_AUTO, out, cap, nout);
+}
+
+int rq_state_apply_1q_matrix(rq_state* s, uint32_t qubit, const double* m) {
+    if (!s || !m) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (qubit >= s->nq)
+        return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "invalid qubit index " + std::to_string(qubit) + " for " +
+                                                        std::to_string(s->nq) + "-qubit system");
+    RQ_TRY(set_device(s));
+    return rq::gate1q(s, qubit, m);
+}
+
+int rq_state_apply_2q_matrix(rq_state* s, uint32_t q1, uint32_t q2, const double* m) {
+    if (!s || !m) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    rq_gate g{};
+    g.kind = RQ_GATE_CNOT;
+    g.q0 = q1;
+    g.q1 = q2;
+    RQ_TRY(validate_gate(s, g));
+    RQ_TRY(set_device(s));
+    return rq::gate2q(s, q1, q2, m);
+}
+
+int rq_state_measure(rq_state* s, uint32_t qubit, rq_measurement* out) {
+    if (!s || !out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (qubit >= s->nq)
+        return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "invalid qubit index " + std::to_string(qubit) + " for " +
+                                                        std::to_string(s->nq) + "-qubit system");
+    RQ_TRY(set_device(s));
+    return do_measure(s, qubit, out);
+}
+
+int rq_state_measure_all(rq_state* s, rq_measurement* out) {
+    if (!s || !out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    RQ_TRY(set_device(s));
+    for (uint32_t q = 0; q < s->nq; ++q) RQ_TRY(do_measure(s, q, &out[q]));
+    return RQ_OK;
+}
+
+int rq_state_reset_qubit(rq_state* s, uint32_t qubit) {
+    if (!s) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null state");
+    if (qubit >= s->nq)
+        return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "invalid qubit index " + std::to_string(qubit) + " for " +
+                                                        std::to_string(s->nq) + "-qubit system");
+    RQ_TRY(set_device(s));
+    return do_reset(s, qubit);
+}
+
+int rq_state_sample(rq_state* s, const uint32_t* qubits, uint32_t nqubits, uint64_t base_seed, uint64_t shots,
+                    uint64_t* out_bits) {
+    if (!s || (!out_bits && shots) || (!qubits && nqubits)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    for (uint32_t k = 0; k < nqubits; ++k)
+        if (qubits[k] >= s->nq)
+            return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "invalid qubit index " + std::to_string(qubits[k]) + " for " +
+                                                            std::to_string(s->nq) + "-qubit system");
+    RQ_TRY(set_device(s));
+    return rq::sample(s, qubits, nqubits, base_seed, shots, out_bits);
+}
+
+int rq_state_probabilities(rq_state* s, double* out) {
+    if (!s || !out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    RQ_TRY(set_device(s));
+    double* d = nullptr;
+    RQ_CUDA(cudaMallocAsync((void**)&d, s->n * sizeof(double), s->stream));
+    int rc = rq::probabilities_dev(s, d);
+    cudaError_t e = cudaSuccess;
+    if (rc == RQ_OK) e = cudaMemcpyAsync(out, d, s->n * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    cudaFreeAsync(d, s->stream);
+    RQ_TRY(rc);
+    RQ_CUDA(e);
+    RQ_CUDA(cudaStreamSynchronize(s->stream));
+    return RQ_OK;
+}
+
+int rq_state_probability_of_qubit(rq_state* s, uint32_t qubit, double* out) {
+    if (!s || !out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (qubit >= s->nq)
+        return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "invalid qubit index " + std::to_string(qubit) + " for " +
+                                                        std::to_string(s->nq) + "-qubit system");
+    RQ_TRY(set_device(s));
+    return rq::prob_bit(s, qubit, 1, out);
+}
+
+int rq_state_expectation_value(rq_state* s, const rq_pauli_op* ops, uint32_t nops, double* out) {
+    if (!s || !out || (!ops && nops)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    rq::PauliMask m;
+    RQ_TRY(to_masks(s, ops, nops, &m));
+    RQ_TRY(set_device(s));
+    return rq::pauli_expect(s, &m, 1, out);
+}
+
+int rq_state_expectation_batch(rq_state* s, const rq_pauli_op* ops, const uint32_t* offsets, uint32_t nstrings,
+                               double* out) {
+    if (!s || (!out && nstrings) || (!offsets && nstrings)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    std::vector<rq::PauliMask> masks(nstrings);
+    for (uint32_t k = 0; k < nstrings; ++k) {
+        if (offsets[k + 1] < offsets[k]) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing");
+        RQ_TRY(to_masks(s, ops + offsets[k], offsets[k + 1] - offsets[k], &masks[k]));
+    }
+    RQ_TRY(set_device(s));
+    return rq::pauli_expect(s, masks.data(), nstrings, out);
+}
+
+int rq_state_expectation_hamiltonian(rq_state* s, const double* coeffs, const rq_pauli_op* ops,
+                                     const uint32_t* offsets, uint32_t nterms, double* out) {
+    if (!out || (!coeffs && nterms)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    std::vector<double> ev(nterms);
+    RQ_TRY(rq_state_expectation_batch(s, ops, offsets, nterms, ev.data()));
+    double acc = 0.0;
+    for (uint32_t k = 0; k < nterms; ++k) acc += coeffs[k] * ev[k];
+    *out = acc;
+    return RQ_OK;
+}
+
+int rq_state_norm_sq(rq_state* s, double* out) {
+    if (!s || !out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    RQ_TRY(set_device(s));
+    return rq::norm_sq(s, out);
+}
+
+int rq_state_normalize(rq_state* s) {
+    double ns = 0.0;
+    RQ_TRY(rq_state_norm_sq(s, &ns));
+    if (ns > 0.0) RQ_TRY(rq::scale_all(s, 1.0 / std::sqrt(ns)));
+    return RQ_OK;
+}
+
+int rq_state_fidelity(rq_state* a, rq_state* b, double* out) {
+    if (!a || !b || !out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (a->nq != b->nq) {
+        *out = 0.0;
+        return RQ_OK;
+    }
+    RQ_TRY(set_device(a));
+    double re = 0, im = 0;
+    RQ_TRY(rq::inner(a, b, &re, &im));
+    *out = re * re + im * im;
+    return RQ_OK;
+}
+
+int rq_state_download(rq_state* s, double* out) {
+    if (!s || !out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    RQ_TRY(set_device(s));
+    size_t bytes = s->n * 2 * sizeof(double);
+    if (s->prec == RQ_F64) {
+        RQ_CUDA(cudaMemcpyAsync(out, s->amps, bytes, cudaMemcpyDeviceToHost, s->stream));
+        RQ_CUDA(cudaStreamSynchronize(s->stream));
+        return RQ_OK;
+    }
+    double* d = nullptr;
+    RQ_CUDA(cudaMallocAsync((void**)&d, bytes, s->stream));
+    int rc = rq::download_f64(s, d);
+    cudaError_t e = cudaSuccess;
+    if (rc == RQ_OK) e = cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, s->stream);
+    cudaFreeAsync(d, s->stream);
+    RQ_TRY(rc);
+    RQ_CUDA(e);
+    RQ_CUDA(cudaStreamSynchronize(s->stream));
+    return RQ_OK;
+}
+
+int rq_state_upload(rq_state* s, const double* in) {
+    if (!s || !in) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    RQ_TRY(set_device(s));
+    size_t bytes = s->n * 2 * sizeof(double);
+    if (s->prec == RQ_F64) {
+        RQ_CUDA(cudaMemcpyAsync(s->amps, in, bytes, cudaMemcpyHostToDevice, s->stream));
+        RQ_CUDA(cudaStreamSynchronize(s->stream));
+        return RQ_OK;
+    }
+    double* d = nullptr;
+    RQ_CUDA(cudaMallocAsync((void**)&d, bytes, s->stream));
+    cudaError_t e = cudaMemcpyAsync(d, in, bytes, cudaMemcpyHostToDevice, s->stream);
+    int rc = e == cudaSuccess ? rq::upload_f64(s, d) : rq::cuda_fail(e, "cudaMemcpyAsync");
+    cudaFreeAsync(d, s->stream);
+    RQ_TRY(rc);
+    RQ_CUDA(cudaStreamSynchronize(s->stream));
+    return RQ_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,268 @@
+// rq_reduce.cu -- FP64-accumulated reductions over the state.
+//
+// Counterparts of probabilities / probability_of_qubit (state.rs:123-137),
+// expectation_value / expectation_hamiltonian (state.rs:362-408), normalize
+// and fidelity (state.rs:415-435).  Every reduction accumulates in FP64 (also
+// for f32 states) and is deterministic: a fixed grid writes one partial per
+// block and term, and a second kernel sums the partials in a fixed order.
+#include "rq_internal.cuh"
+
+#include <algorithm>
+#include <map>
+
+namespace {
+
+using rqd::C2;
+using rqd::insert0;
+
+constexpr int TPB = 256;
+constexpr int KMAX = 8;   // Pauli strings per pass
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// sum `v` over the block; result valid in thread 0
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    v = warp_sum(v);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+        r = warp_sum(r);
+    }
+    return r;
+}
+
+template <typename V>
+__device__ __forceinline__ double norm2(V x) {
+    double re = (double)x.x, im = (double)x.y;
+    return re * re + im * im;
+}
+
+// sum of |a_i|^2 over i with bit q == want (q = 64: all i)
+template <typename T>
+__global__ void k_prob(const typename C2<T>::t* __restrict__ a, uint64_t count, uint32_t q, int want,
+                       double* __restrict__ partials) {
+    __shared__ double sh[32];
+    double acc = 0.0;
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < count;
+         p += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t i = q < 64 ? (insert0(p, q) | ((uint64_t)want << q)) : p;
+        acc += norm2(a[i]);
+    }
+    double r = block_sum(acc, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = r;
+}
+
+struct TermChunk {
+    uint64_t pmask[KMAX];
+    int odd[KMAX];
+    int k;
+};
+
+// Pauli strings sharing one xmask.  x == 0: acc_k += s_k(i)|a_i|^2.
+// x != 0: pairs (i, j = i^x) with the top bit h of x clear in i,
+// z = conj(a_j) a_i, acc_k += s_k(i) * (odd_k ? Im z : Re z).
+template <typename T>
+__global__ void k_pauli(const typename C2<T>::t* __restrict__ a, uint64_t count, uint64_t x, uint32_t h,
+                        TermChunk tc, double* __restrict__ partials, uint32_t slot0, uint32_t stride) {
+    __shared__ double sh[32];
+    double acc[KMAX];
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k) acc[k] = 0.0;
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < count;
+         p += (uint64_t)gridDim.x * blockDim.x) {
+        double re, im;
+        uint64_t i;
+        if (x == 0) {
+            i = p;
+            re = norm2(a[i]);
+            im = 0.0;
+        } else {
+            i = insert0(p, h);
+            auto ai = a[i];
+            auto aj = a[i ^ x];
+            double air = ai.x, aii = ai.y, ajr = aj.x, aji = aj.y;
+            re = ajr * air + aji * aii;
+            im = ajr * aii - aji * air;
+        }
+#pragma unroll
+        for (int k = 0; k < KMAX; ++k) {
+            if (k < tc.k) {
+                double v = tc.odd[k] ? im : re;
+                acc[k] += (__popcll(i & tc.pmask[k]) & 1) ? -v : v;
+            }
+        }
+    }
+    for (int k = 0; k < tc.k; ++k) {
+        double r = block_sum(acc[k], sh);
+        if (threadIdx.x == 0) partials[(size_t)(slot0 + k) * stride + blockIdx.x] = r;
+    }
+}
+
+// <a|b> = sum conj(a_i) b_i
+template <typename TA, typename TB>
+__global__ void k_inner(const typename C2<TA>::t* __restrict__ a, const typename C2<TB>::t* __restrict__ b,
+                        uint64_t n, double* __restrict__ partials, uint32_t stride) {
+    __shared__ double sh[32];
+    double re = 0.0, im = 0.0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        auto x = a[i];
+        auto y = b[i];
+        double xr = x.x, xi = x.y, yr = y.x, yi = y.y;
+        re += xr * yr + xi * yi;
+        im += xr * yi - xi * yr;
+    }
+    double r = block_sum(re, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = r;
+    r = block_sum(im, sh);
+    if (threadIdx.x == 0) partials[stride + blockIdx.x] = r;
+}
+
+// out[k] = sum_b partials[k*stride + b], fixed order
+__global__ void k_finalize(const double* __restrict__ partials, uint32_t nblocks, uint32_t stride,
+                           double* __restrict__ out) {
+    __shared__ double sh[32];
+    const double* p = partials + (size_t)blockIdx.x * stride;
+    double acc = 0.0;
+    for (uint32_t b = threadIdx.x; b < nblocks; b += blockDim.x) acc += p[b];
+    double r = block_sum(acc, sh);
+    if (threadIdx.x == 0) out[blockIdx.x] = r;
+}
+
+// p_i = re*re + im*im, rounded exactly as a host computation without FMA
+template <typename T>
+__global__ void k_probs(const typename C2<T>::t* __restrict__ a, uint64_t n, double* __restrict__ out) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        auto x = a[i];
+        double re = x.x, im = x.y;
+        out[i] = __dadd_rn(__dmul_rn(re, re), __dmul_rn(im, im));
+    }
+}
+
+int reduction_grid(rq_state* s) { return rq::num_sms(s->device) * 4; }
+
+// finalize `nout` partial rows and copy them to host
+int finish(rq_state* s, unsigned nblocks, unsigned stride, unsigned nout, double* host) {
+    double* dout = s->partials + (size_t)nout * stride;
+    k_finalize<<<nout, TPB, 0, s->stream>>>(s->partials, nblocks, stride, dout);
+    RQ_CUDA(cudaGetLastError());
+    RQ_TRY(rq::ensure_hbuf(s, nout));
+    RQ_CUDA(cudaMemcpyAsync(s->hbuf, dout, nout * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    RQ_CUDA(cudaStreamSynchronize(s->stream));
+    for (unsigned k = 0; k < nout; ++k) host[k] = s->hbuf[k];
+    return RQ_OK;
+}
+
+inline double re_ipow(uint32_t k) {
+    switch (k & 3u) {
+        case 0: return 1.0;
+        case 2: return -1.0;
+        default: return 0.0;
+    }
+}
+
+}  // namespace
+
+namespace rq {
+
+int prob_bit(rq_state* s, uint32_t q, int want_one, double* out) {
+    unsigned G = reduction_grid(s);
+    uint64_t count = q < 64 ? s->n >> 1 : s->n;
+    G = std::min<unsigned>(G, grid_for(count, TPB, num_sms(s->device), 4));
+    RQ_TRY(ensure_partials(s, 2 * (size_t)G + 8));
+    if (s->prec == RQ_F32)
+        k_prob<float><<<G, TPB, 0, s->stream>>>((const float2*)s->amps, count, q, want_one, s->partials);
+    else
+        k_prob<double><<<G, TPB, 0, s->stream>>>((const double2*)s->amps, count, q, want_one, s->partials);
+    RQ_CUDA(cudaGetLastError());
+    return finish(s, G, G, 1, out);
+}
+
+int norm_sq(rq_state* s, double* out) { return prob_bit(s, 64, 0, out); }
+
+int pauli_expect(rq_state* s, const PauliMask* terms, uint32_t nterms, double* out) {
+    if (nterms == 0) return RQ_OK;
+    unsigned G = reduction_grid(s);
+    RQ_TRY(ensure_partials(s, (size_t)nterms * G + nterms + 8));
+    // group by xmask (stable), chunks of KMAX
+    std::map<uint64_t, std::vector<uint32_t>> groups;
+    for (uint32_t k = 0; k < nterms; ++k) groups[terms[k].xmask].push_back(k);
+    std::vector<uint32_t> slot_of(nterms);
+    uint32_t slot = 0;
+    for (auto& kv : groups) {
+        uint64_t x = kv.first;
+        uint32_t h = x ? 63 - __builtin_clzll(x) : 0;
+        uint64_t count = x ? s->n >> 1 : s->n;
+        const auto& idx = kv.second;
+        for (size_t c0 = 0; c0 < idx.size(); c0 += KMAX) {
+            TermChunk tc{};
+            tc.k = (int)std::min<size_t>(KMAX, idx.size() - c0);
+            for (int k = 0; k < tc.k; ++k) {
+                const PauliMask& t = terms[idx[c0 + k]];
+                tc.pmask[k] = t.pmask;
+                tc.odd[k] = x ? (__builtin_popcountll(x & t.pmask) & 1) : 0;
+                slot_of[idx[c0 + k]] = slot + k;
+            }
+            if (s->prec == RQ_F32)
+                k_pauli<float><<<G, TPB, 0, s->stream>>>((const float2*)s->amps, count, x, h, tc, s->partials, slot, G);
+            else
+                k_pauli<double><<<G, TPB, 0, s->stream>>>((const double2*)s->amps, count, x, h, tc, s->partials, slot, G);
+            RQ_CUDA(cudaGetLastError());
+            slot += tc.k;
+        }
+    }
+    std::vector<double> sums(nterms);
+    RQ_TRY(finish(s, G, G, nterms, sums.data()));
+    for (uint32_t k = 0; k < nterms; ++k) {
+        const PauliMask& t = terms[k];
+        double acc = sums[slot_of[k]];
+        if (t.xmask == 0) {
+            out[k] = acc * re_ipow(t.ny);
+        } else if (!(__builtin_popcountll(t.xmask & t.pmask) & 1)) {
+            out[k] = 2.0 * acc * re_ipow(t.ny);
+        } else {
+            out[k] = 2.0 * acc * re_ipow(t.ny + 1);
+        }
+    }
+    return RQ_OK;
+}
+
+int inner(rq_state* a, rq_state* b, double* re, double* im) {
+    unsigned G = reduction_grid(a);
+    RQ_TRY(ensure_partials(a, 2 * (size_t)G + 8));
+    // b's pending work must be done before a's stream reads it
+    RQ_CUDA(cudaStreamSynchronize(b->stream));
+    if (a->prec == RQ_F32 && b->prec == RQ_F32)
+        k_inner<float, float><<<G, TPB, 0, a->stream>>>((const float2*)a->amps, (const float2*)b->amps, a->n, a->partials, G);
+    else if (a->prec == RQ_F32)
+        k_inner<float, double><<<G, TPB, 0, a->stream>>>((const float2*)a->amps, (const double2*)b->amps, a->n, a->partials, G);
+    else if (b->prec == RQ_F32)
+        k_inner<double, float><<<G, TPB, 0, a->stream>>>((const double2*)a->amps, (const float2*)b->amps, a->n, a->partials, G);
+    else
+        k_inner<double, double><<<G, TPB, 0, a->stream>>>((const double2*)a->amps, (const double2*)b->amps, a->n, a->partials, G);
+    RQ_CUDA(cudaGetLastError());
+    double r[2];
+    RQ_TRY(finish(a, G, G, 2, r));
+    *re = r[0];
+    *im = r[1];
+    return RQ_OK;
+}
+
+int probabilities_dev(rq_state* s, double* dev_out) {
+    unsigned g = grid_for(s->n, TPB, num_sms(s->device));
+    if (s->prec == RQ_F32) k_probs<float><<<g, TPB, 0, s->stream>>>((const float2*)s->amps, s->n, dev_out);
+    else k_probs<double><<<g, TPB, 0, s->stream>>>((const double2*)s->amps, s->n, dev_out);
+    RQ_CUDA(cudaGetLastError());
+    return RQ_OK;
+}
+
+}  // namespace rq

@@ -1,0 +1,724 @@
+// rq_sweep.cu -- multi-gate sweeps: many gates per HBM pass.
+//
+// The reference applies every gate as its own full pass over the state
+// (state.rs:214-276, called once per gate from simulator.rs:69-79).  Here a
+// host planner cuts the gate list into sweeps.  A sweep owns a set L of m
+// "local" qubits (always including qubits 0..c-1, so every HBM access is a
+// contiguous 2^c-amplitude chunk); each CTA loads one 2^m-amplitude tile
+// (all combinations of the local bits for one value of the other bits) into
+// shared memory with coalesced 16-byte loads, runs the sweep's gates on it,
+// and writes it back: 2*S bytes of HBM traffic per sweep instead of per gate.
+//
+// Inside a tile the gates run in phases.  In a phase every thread holds 2^RB
+// amplitudes in registers whose indices differ in RB chosen local bits (the
+// phase's register slots); a non-diagonal 1-qubit gate or a CNOT target must
+// sit on a register slot, diagonal gates (Rz, Phase, S, T, Z, CZ, Rzz) and
+// CNOT controls may sit on any bit because they only read index bits.
+// Between phases the tile goes back through shared memory (XOR-swizzled so
+// the strided reads of any slot choice stay nearly bank-conflict free).
+// Adjacent 1-qubit gates on the same qubit are multiplied into one 2x2 on
+// the host (a generalisation of optimizer::fuse_gates, optimizer.rs:46-94).
+#include "rq_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+#include <vector>
+#include <cstdlib>
+
+namespace {
+
+using rqd::C2;
+
+enum OpType : uint8_t { OP_U1 = 0, OP_D1 = 1, OP_CX = 2, OP_CZ = 3, OP_ZZ = 4 };
+
+constexpr int RBMAX = 5;
+constexpr int MMAX = 14;
+
+struct SwOp {
+    uint8_t type;
+    int8_t k0, k1;   // register slot of q0 / q1 in this phase, -1 if not a slot
+    uint8_t q0, q1;  // global qubits
+    uint8_t pad[3];
+    uint32_t mat;    // first complex entry in the matrix table
+};
+
+struct PhaseDesc {
+    uint32_t op_begin, op_end;
+    uint32_t nt;              // number of thread bits
+    uint8_t tbit_local[16];   // thread bit b -> local bit index
+    uint8_t tbit_global[16];  // thread bit b -> global qubit
+    uint16_t lut[1 << RBMAX]; // register index -> local offset
+};
+
+struct SweepDesc {
+    uint32_t n, m, c;
+    uint32_t nonlocal_count;
+    uint8_t local_global[32];   // local bit -> global qubit
+    uint8_t nonlocal[64];       // non-local bits in ascending order
+    uint32_t phase_begin, phase_end;
+    uint64_t gj[1 << RBMAX];    // deposit of the per-thread vector offsets
+};
+
+// 16-byte vector type per precision: 2 complex f32 or 1 complex f64
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using t = float4; static constexpr int EPV = 2; };
+template <> struct Vec16<double> { using t = double2; static constexpr int EPV = 1; };
+
+template <typename T>
+__device__ __forceinline__ uint32_t swz(uint32_t e) {
+    // 128-byte rows: 16 complex f32 or 8 complex f64 per row
+    constexpr int CB = sizeof(typename C2<T>::t) == 8 ? 4 : 3;
+    uint32_t r = e >> CB;
+    uint32_t f = r ^ (r >> CB) ^ (r >> (2 * CB)) ^ (r >> (3 * CB));
+    return e ^ (f & ((1u << CB) - 1));
+}
+
+template <typename V, typename T>
+__device__ __forceinline__ V cmul(V a, T br, T bi) {
+    V r;
+    r.x = a.x * br - a.y * bi;
+    r.y = a.x * bi + a.y * br;
+    return r;
+}
+
+template <int K, int NR, typename V, typename T>
+__device__ __forceinline__ void op_u1(V* reg, const T* __restrict__ m) {
+    const T m00r = m[0], m00i = m[1], m01r = m[2], m01i = m[3];
+    const T m10r = m[4], m10i = m[5], m11r = m[6], m11i = m[7];
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+        if (i & (1 << K)) continue;
+        const int j = i | (1 << K);
+        V x = reg[i], y = reg[j];
+        V o0, o1;
+        o0.x = m00r * x.x - m00i * x.y + m01r * y.x - m01i * y.y;
+        o0.y = m00r * x.y + m00i * x.x + m01r * y.y + m01i * y.x;
+        o1.x = m10r * x.x - m10i * x.y + m11r * y.x - m11i * y.y;
+        o1.y = m10r * x.y + m10i * x.x + m11r * y.y + m11i * y.x;
+        reg[i] = o0;
+        reg[j] = o1;
+    }
+}
+
+// CNOT with its target on slot K; control = slot ck (>=0) or uniform bit cu
+template <int K, int NR, typename V>
+__device__ __forceinline__ void op_cx(V* reg, int ck, int cu) {
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+        if (i & (1 << K)) continue;
+        const int j = i | (1 << K);
+        const bool c = ck >= 0 ? ((i >> ck) & 1) : cu;
+        V x = reg[i], y = reg[j];
+        reg[i] = c ? y : x;
+        reg[j] = c ? x : y;
+    }
+}
+
+template <int NR, typename V, typename T>
+__device__ __forceinline__ void dispatch_u1(int k, V* reg, const T* m) {
+    switch (k) {
+        case 0: op_u1<0, NR>(reg, m); break;
+        case 1: op_u1<1, NR>(reg, m); break;
+        case 2: op_u1<2, NR>(reg, m); break;
+        case 3: if constexpr (NR > 8) op_u1<3, NR>(reg, m); break;
+        case 4: if constexpr (NR > 16) op_u1<4, NR>(reg, m); break;
+        default: break;
+    }
+}
+
+template <int NR, typename V>
+__device__ __forceinline__ void dispatch_cx(int k, V* reg, int ck, int cu) {
+    switch (k) {
+        case 0: op_cx<0, NR>(reg, ck, cu); break;
+        case 1: op_cx<1, NR>(reg, ck, cu); break;
+        case 2: op_cx<2, NR>(reg, ck, cu); break;
+        case 3: if constexpr (NR > 8) op_cx<3, NR>(reg, ck, cu); break;
+        case 4: if constexpr (NR > 16) op_cx<4, NR>(reg, ck, cu); break;
+        default: break;
+    }
+}
+
+template <typename T, int RB>
+__global__ void __launch_bounds__(256, 2) k_sweep(typename C2<T>::t* __restrict__ amps, const SweepDesc d,
+                                               const PhaseDesc* __restrict__ phases, const SwOp* __restrict__ ops,
+                                               const T* __restrict__ mats, uint64_t ntiles) {
+    using V = typename C2<T>::t;
+    using VV = typename Vec16<T>::t;
+    constexpr int NR = 1 << RB;
+    constexpr int EPV = Vec16<T>::EPV;
+    constexpr int VPT = NR / EPV;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* sm = reinterpret_cast<V*>(smem_raw);
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t T_ = blockDim.x;
+    const uint64_t cmask = (1ull << d.c) - 1;
+
+    // deposit of this thread's vector offset (local bits of EPV*tid) into global positions
+    uint64_t dep_tid = 0;
+    {
+        uint64_t x = (uint64_t)tid * EPV;
+        dep_tid = x & cmask;
+        for (uint32_t b = d.c; b < d.m; ++b)
+            if ((x >> b) & 1ull) dep_tid |= 1ull << d.local_global[b];
+    }
+
+    for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        uint64_t base = 0;
+        for (uint32_t b = 0; b < d.nonlocal_count; ++b)
+            if ((tile >> b) & 1ull) base |= 1ull << d.nonlocal[b];
+
+        // ---- load tile (coalesced 16-byte vectors, 8 in flight per thread) ----
+#pragma unroll 1
+        for (int j0 = 0; j0 < VPT; j0 += 8) {
+            VV v[8];
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj)
+                v[jj] = __ldcs(reinterpret_cast<const VV*>(amps + (base | dep_tid | d.gj[j0 + jj])));
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj) {
+                const uint32_t e = (tid + T_ * (j0 + jj)) * EPV;
+                if constexpr (EPV == 2) {
+                    sm[swz<T>(e)] = make_float2(v[jj].x, v[jj].y);
+                    sm[swz<T>(e + 1)] = make_float2(v[jj].z, v[jj].w);
+                } else {
+                    sm[swz<T>(e)] = *reinterpret_cast<V*>(&v[jj]);
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- phases ----
+        for (uint32_t p = d.phase_begin; p < d.phase_end; ++p) {
+            const PhaseDesc& ph = phases[p];
+            uint32_t ebase = 0;
+            uint64_t U = base;
+            for (uint32_t b = 0; b < ph.nt; ++b)
+                if ((tid >> b) & 1u) {
+                    ebase |= 1u << ph.tbit_local[b];
+                    U |= 1ull << ph.tbit_global[b];
+                }
+            V reg[NR];
+#pragma unroll
+            for (int i = 0; i < NR; ++i) reg[i] = sm[swz<T>(ebase | ph.lut[i])];
+
+            for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
+                const SwOp op = ops[o];
+                const T* mm = mats + 2 * op.mat;
+                switch (op.type) {
+                    case OP_U1: dispatch_u1<NR>(op.k0, reg, mm); break;
+                    case OP_CX: dispatch_cx<NR>(op.k1, reg, op.k0, (int)((U >> op.q0) & 1ull)); break;
+                    case OP_D1: {
+                        const T d0r = mm[0], d0i = mm[1], d1r = mm[2], d1i = mm[3];
+                        const int kk = op.k0;
+                        const int ub = (int)((U >> op.q0) & 1ull);
+#pragma unroll
+                        for (int i = 0; i < NR; ++i) {
+                            const int b = kk >= 0 ? ((i >> kk) & 1) : ub;
+                            reg[i] = cmul(reg[i], b ? d1r : d0r, b ? d1i : d0i);
+                        }
+                        break;
+                    }
+                    case OP_CZ: {
+                        const int k0 = op.k0, k1 = op.k1;
+                        const int u0 = (int)((U >> op.q0) & 1ull), u1 = (int)((U >> op.q1) & 1ull);
+#pragma unroll
+                        for (int i = 0; i < NR; ++i) {
+                            const int b0 = k0 >= 0 ? ((i >> k0) & 1) : u0;
+                            const int b1 = k1 >= 0 ? ((i >> k1) & 1) : u1;
+                            if (b0 & b1) {
+                                reg[i].x = -reg[i].x;
+                                reg[i].y = -reg[i].y;
+                            }
+                        }
+                        break;
+                    }
+                    case OP_ZZ: {
+                        // diag(en, ep, ep, en): en for equal bits, ep for different bits
+                        const T er = mm[0], ei = mm[1], pr = mm[2], pi = mm[3];
+                        const int k0 = op.k0, k1 = op.k1;
+                        const int u0 = (int)((U >> op.q0) & 1ull), u1 = (int)((U >> op.q1) & 1ull);
+#pragma unroll
+                        for (int i = 0; i < NR; ++i) {
+                            const int b0 = k0 >= 0 ? ((i >> k0) & 1) : u0;
+                            const int b1 = k1 >= 0 ? ((i >> k1) & 1) : u1;
+                            const bool diff = (b0 ^ b1) != 0;
+                            reg[i] = cmul(reg[i], diff ? pr : er, diff ? pi : ei);
+                        }
+                        break;
+                    }
+                    default: break;
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < NR; ++i) sm[swz<T>(ebase | ph.lut[i])] = reg[i];
+            __syncthreads();
+        }
+
+        // ---- store tile ----
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) {
+            const uint32_t e = (tid + T_ * j) * EPV;
+            const uint64_t g = base | dep_tid | d.gj[j];
+            VV v;
+            if constexpr (EPV == 2) {
+                float2 a = sm[swz<T>(e)], b = sm[swz<T>(e + 1)];
+                v = make_float4(a.x, a.y, b.x, b.y);
+            } else {
+                V a = sm[swz<T>(e)];
+                v = *reinterpret_cast<VV*>(&a);
+            }
+            __stcs(reinterpret_cast<VV*>(amps + g), v);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host planner
+// ---------------------------------------------------------------------------
+
+struct PGate {
+    uint8_t type;
+    uint32_t q0, q1;
+    double m[8];   // U1: 2x2; D1: d0,d1; ZZ: en,ep
+};
+
+uint64_t qmask(const PGate& g) {
+    uint64_t m = 1ull << g.q0;
+    if (g.type == OP_CX || g.type == OP_CZ || g.type == OP_ZZ) m |= 1ull << g.q1;
+    return m;
+}
+
+// qubits that must be register slots (and therefore local)
+uint64_t needs(const PGate& g) {
+    if (g.type == OP_U1) return 1ull << g.q0;
+    if (g.type == OP_CX) return 1ull << g.q1;
+    return 0;
+}
+
+bool is_1q(uint8_t t) { return t == OP_U1 || t == OP_D1; }
+
+// c = a * b (2x2 complex, row-major (re,im))
+void mat2_mul(const double* a, const double* b, double* c) {
+    double r[8];
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j) {
+            double re = 0, im = 0;
+            for (int k = 0; k < 2; ++k) {
+                double ar = a[(i * 2 + k) * 2], ai = a[(i * 2 + k) * 2 + 1];
+                double br = b[(k * 2 + j) * 2], bi = b[(k * 2 + j) * 2 + 1];
+                re += ar * br - ai * bi;
+                im += ar * bi + ai * br;
+            }
+            r[(i * 2 + j) * 2] = re;
+            r[(i * 2 + j) * 2 + 1] = im;
+        }
+    std::memcpy(c, r, sizeof(r));
+}
+
+void as_matrix(const PGate& g, double* m) {
+    if (g.type == OP_U1) {
+        std::memcpy(m, g.m, sizeof(double) * 8);
+    } else {  // D1
+        double r[8] = {g.m[0], g.m[1], 0, 0, 0, 0, g.m[2], g.m[3]};
+        std::memcpy(m, r, sizeof(r));
+    }
+}
+
+// fuse `nxt` (applied after `cur`) into cur; both 1-qubit on the same qubit
+void fuse_into(PGate& cur, const PGate& nxt) {
+    if (cur.type == OP_D1 && nxt.type == OP_D1) {
+        double a[2] = {cur.m[0], cur.m[1]}, b[2] = {cur.m[2], cur.m[3]};
+        cur.m[0] = nxt.m[0] * a[0] - nxt.m[1] * a[1];
+        cur.m[1] = nxt.m[0] * a[1] + nxt.m[1] * a[0];
+        cur.m[2] = nxt.m[2] * b[0] - nxt.m[3] * b[1];
+        cur.m[3] = nxt.m[2] * b[1] + nxt.m[3] * b[0];
+        return;
+    }
+    double A[8], B[8], C[8];
+    as_matrix(cur, A);
+    as_matrix(nxt, B);
+    mat2_mul(B, A, C);
+    cur.type = OP_U1;
+    std::memcpy(cur.m, C, sizeof(C));
+}
+
+struct Sweep {
+    uint64_t L;               // local qubit mask
+    std::vector<PGate> ops;   // in execution order (after fusion)
+};
+
+std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c) {
+    std::vector<Sweep> out;
+    std::vector<char> taken(gates.size(), 0);
+    size_t first = 0;
+    const uint64_t base = (c >= 64) ? ~0ull : ((1ull << c) - 1);
+    while (first < gates.size()) {
+        Sweep sw;
+        sw.L = base;
+        uint64_t blocked = 0;
+        std::vector<int> last(n, -1);   // index in sw.ops of the last op on each qubit
+        for (size_t k = first; k < gates.size(); ++k) {
+            if (taken[k]) continue;
+            const PGate& g = gates[k];
+            uint64_t qm = qmask(g);
+            if (qm & blocked) {
+                blocked |= qm;
+                continue;
+            }
+            uint64_t L2 = sw.L | needs(g);
+            if ((uint32_t)__builtin_popcountll(L2) > m) {
+                blocked |= qm;
+                continue;
+            }
+            sw.L = L2;
+            taken[k] = 1;
+            if (is_1q(g.type) && last[g.q0] >= 0 && is_1q(sw.ops[last[g.q0]].type)) {
+                fuse_into(sw.ops[last[g.q0]], g);
+            } else {
+                sw.ops.push_back(g);
+                int idx = (int)sw.ops.size() - 1;
+                last[g.q0] = idx;
+                if (!is_1q(g.type)) last[g.q1] = idx;
+            }
+        }
+        while (first < gates.size() && taken[first]) ++first;
+        out.push_back(std::move(sw));
+    }
+    return out;
+}
+
+struct PhasePlan {
+    uint64_t R;               // register qubits (global mask)
+    std::vector<int> ops;     // indices into the sweep's op list
+};
+
+std::vector<PhasePlan> plan_phases(const Sweep& sw, uint32_t rb) {
+    std::vector<PhasePlan> out;
+    std::vector<char> taken(sw.ops.size(), 0);
+    size_t first = 0;
+    while (first < sw.ops.size()) {
+        PhasePlan ph;
+        ph.R = 0;
+        uint64_t blocked = 0;
+        for (size_t k = first; k < sw.ops.size(); ++k) {
+            if (taken[k]) continue;
+            const PGate& g = sw.ops[k];
+            uint64_t qm = qmask(g);
+            if (qm & blocked) {
+                blocked |= qm;
+                continue;
+            }
+            uint64_t R2 = ph.R | needs(g);
+            if ((uint32_t)__builtin_popcountll(R2) > rb) {
+                blocked |= qm;
+                continue;
+            }
+            ph.R = R2;
+            taken[k] = 1;
+            ph.ops.push_back((int)k);
+        }
+        // fill the remaining slots with the lowest unused local qubits
+        for (uint32_t q = 0; q < 64 && (uint32_t)__builtin_popcountll(ph.R) < rb; ++q)
+            if (((sw.L >> q) & 1) && !((ph.R >> q) & 1)) ph.R |= 1ull << q;
+        while (first < sw.ops.size() && taken[first]) ++first;
+        out.push_back(std::move(ph));
+    }
+    return out;
+}
+
+bool to_pgates(const rq_gate* gates, uint64_t n, std::vector<PGate>& out) {
+    const double s2 = 0.70710678118654752440;
+    for (uint64_t k = 0; k < n; ++k) {
+        const rq_gate& g = gates[k];
+        PGate p{};
+        p.q0 = g.q0;
+        p.q1 = g.q1;
+        double h = g.angle / 2.0;
+        switch (g.kind) {
+            case RQ_GATE_CNOT: p.type = OP_CX; out.push_back(p); break;
+            case RQ_GATE_CZ: p.type = OP_CZ; out.push_back(p); break;
+            case RQ_GATE_RZZ:
+                p.type = OP_ZZ;
+                p.m[0] = std::cos(-h); p.m[1] = std::sin(-h); p.m[2] = std::cos(h); p.m[3] = std::sin(h);
+                out.push_back(p);
+                break;
+            case RQ_GATE_SWAP: {
+                PGate a{}; a.type = OP_CX; a.q0 = g.q0; a.q1 = g.q1;
+                PGate b{}; b.type = OP_CX; b.q0 = g.q1; b.q1 = g.q0;
+                out.push_back(a); out.push_back(b); out.push_back(a);
+                break;
+            }
+            case RQ_GATE_Z: p.type = OP_D1; p.m[0] = 1; p.m[2] = -1; p.m[3] = -0.0; out.push_back(p); break;
+            case RQ_GATE_S: p.type = OP_D1; p.m[0] = 1; p.m[3] = 1; out.push_back(p); break;
+            case RQ_GATE_SDG: p.type = OP_D1; p.m[0] = 1; p.m[2] = -0.0; p.m[3] = -1; out.push_back(p); break;
+            case RQ_GATE_T: p.type = OP_D1; p.m[0] = 1; p.m[2] = s2; p.m[3] = s2; out.push_back(p); break;
+            case RQ_GATE_TDG: p.type = OP_D1; p.m[0] = 1; p.m[2] = s2; p.m[3] = -s2; out.push_back(p); break;
+            case RQ_GATE_RZ:
+                p.type = OP_D1;
+                p.m[0] = std::cos(-h); p.m[1] = std::sin(-h); p.m[2] = std::cos(h); p.m[3] = std::sin(h);
+                out.push_back(p);
+                break;
+            case RQ_GATE_PHASE:
+                p.type = OP_D1; p.m[0] = 1; p.m[2] = std::cos(g.angle); p.m[3] = std::sin(g.angle);
+                out.push_back(p);
+                break;
+            case RQ_GATE_H: { p.type = OP_U1; double m[8] = {s2, 0, s2, 0, s2, 0, -s2, -0.0}; std::memcpy(p.m, m, sizeof m); out.push_back(p); break; }
+            case RQ_GATE_X: { p.type = OP_U1; double m[8] = {0, 0, 1, 0, 1, 0, 0, 0}; std::memcpy(p.m, m, sizeof m); out.push_back(p); break; }
+            case RQ_GATE_Y: { p.type = OP_U1; double m[8] = {0, 0, -0.0, -1, 0, 1, 0, 0}; std::memcpy(p.m, m, sizeof m); out.push_back(p); break; }
+            case RQ_GATE_RX: {
+                double c = std::cos(h), sn = -std::sin(h);
+                p.type = OP_U1; double m[8] = {c, 0, 0, sn, 0, sn, c, 0}; std::memcpy(p.m, m, sizeof m); out.push_back(p);
+                break;
+            }
+            case RQ_GATE_RY: {
+                double c = std::cos(h), sn = std::sin(h);
+                p.type = OP_U1; double m[8] = {c, 0, -sn, 0, sn, 0, c, 0}; std::memcpy(p.m, m, sizeof m); out.push_back(p);
+                break;
+            }
+            case RQ_GATE_UNITARY1Q: p.type = OP_U1; std::memcpy(p.m, g.m, sizeof p.m); out.push_back(p); break;
+            default: return false;
+        }
+    }
+    return true;
+}
+
+template <typename T>
+int launch_sweep(rq_state* s, const SweepDesc& d, const PhaseDesc* ph, const SwOp* ops, const void* mats,
+                 uint64_t ntiles, uint32_t rb, size_t smem) {
+    using V = typename C2<T>::t;
+    unsigned threads = 1u << (d.m - rb);
+    int sms = rq::num_sms(s->device);
+    auto kern = k_sweep<T, std::is_same<T, float>::value ? 5 : 4>;
+    RQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // persistent grid: exactly the CTAs that can be resident at once
+    int per_sm = 0;
+    RQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)threads, smem));
+    if (per_sm < 1) return rq::fail(RQ_ERR_CUDA, "sweep kernel does not fit on an SM");
+    unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)sms * per_sm);
+    kern<<<grid, threads, smem, s->stream>>>((V*)s->amps, d, ph, ops, (const T*)mats, ntiles);
+    RQ_CUDA(cudaGetLastError());
+    return RQ_OK;
+}
+
+}  // namespace
+
+// Prepared gate program: the sweep plan with its device-side tables, or
+// (per-gate mode) the gate list.  Executing it launches kernels only.
+struct rq_plan {
+    uint32_t nq = 0;
+    int32_t prec = RQ_F64;
+    int device = 0;
+    int32_t mode = RQ_EXEC_SWEEP;
+    std::vector<rq_gate> gates;          // per-gate mode
+    std::vector<SweepDesc> descs;        // sweep mode: one launch each
+    unsigned char* dev = nullptr;        // phases | ops | matrices
+    size_t off_ph = 0, off_ops = 0, off_mat = 0;
+    uint64_t ntiles = 0;
+    size_t smem = 0;
+    uint32_t rb = 0;
+    rq_plan_stats stats{};
+};
+
+namespace rq {
+
+static uint32_t sweep_local_qubits(uint32_t nq, int32_t prec) {
+    uint32_t m = prec == RQ_F32 ? 13 : 12;
+    if (const char* e = std::getenv("RUQU_SWEEP_LOCAL_QUBITS")) {
+        int v = std::atoi(e);
+        uint32_t cap = prec == RQ_F32 ? 14 : 13;
+        if (v >= 8 && (uint32_t)v <= cap) m = (uint32_t)v;
+    }
+    return std::min(nq, m);
+}
+
+int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out) {
+    rq_plan* P = new rq_plan();
+    P->nq = s->nq;
+    P->prec = s->prec;
+    P->device = s->device;
+    const uint32_t nq = s->nq;
+    const uint32_t rb = s->prec == RQ_F32 ? 5 : 4;
+    const uint64_t S = s->bytes();
+    if (mode == RQ_EXEC_PER_GATE || nq < rb + 2) {
+        P->mode = RQ_EXEC_PER_GATE;
+        for (uint64_t k = 0; k < n; ++k)
+            if (gates[k].kind != RQ_GATE_BARRIER) P->gates.push_back(gates[k]);
+        P->stats.gates = P->gates.size();
+        P->stats.launches = P->gates.size();
+        for (auto& g : P->gates) {
+            uint64_t b = 2 * S;
+            if (g.kind == RQ_GATE_CNOT || g.kind == RQ_GATE_SWAP) b = S;
+            else if (g.kind == RQ_GATE_CZ) b = S / 2;
+            else if (g.kind == RQ_GATE_Z || g.kind == RQ_GATE_S || g.kind == RQ_GATE_SDG || g.kind == RQ_GATE_T ||
+                     g.kind == RQ_GATE_TDG || g.kind == RQ_GATE_PHASE) b = S;
+            P->stats.hbm_bytes += b;
+        }
+        *out = P;
+        return RQ_OK;
+    }
+    P->mode = RQ_EXEC_SWEEP;
+    const uint32_t m = sweep_local_qubits(nq, s->prec);
+    const uint32_t c = std::min<uint32_t>(m, 5);
+    std::vector<PGate> pg;
+    std::vector<rq_gate> filtered;
+    for (uint64_t k = 0; k < n; ++k)
+        if (gates[k].kind != RQ_GATE_BARRIER) filtered.push_back(gates[k]);
+    if (!to_pgates(filtered.data(), filtered.size(), pg)) {
+        delete P;
+        return fail(RQ_ERR_CIRCUIT, "circuit error: only unitary gates can be planned");
+    }
+    auto sweeps = plan_sweeps(pg, nq, m, c);
+
+    std::vector<PhaseDesc> phases;
+    std::vector<SwOp> ops;
+    std::vector<double> mats;
+    for (auto& sw : sweeps) {
+        uint64_t L = sw.L;
+        for (uint32_t q = 0; q < nq && (uint32_t)__builtin_popcountll(L) < m; ++q) L |= 1ull << q;
+        sw.L = L;
+        SweepDesc d{};
+        d.n = nq;
+        d.m = m;
+        d.c = c;
+        uint32_t li = 0, ni = 0;
+        uint8_t local_index[64];
+        for (uint32_t q = 0; q < nq; ++q) {
+            if ((L >> q) & 1) { local_index[q] = (uint8_t)li; d.local_global[li++] = (uint8_t)q; }
+            else d.nonlocal[ni++] = (uint8_t)q;
+        }
+        d.nonlocal_count = ni;
+        const uint32_t EPV = s->prec == RQ_F32 ? 2 : 1;
+        const uint32_t t = m - rb;
+        const uint32_t VPT = (1u << rb) / EPV;
+        for (uint32_t j = 0; j < VPT; ++j) {
+            uint64_t x = (uint64_t)j * (1ull << t) * EPV, gsum = 0;
+            for (uint32_t b = 0; b < m; ++b)
+                if ((x >> b) & 1) gsum |= 1ull << d.local_global[b];
+            d.gj[j] = gsum;
+        }
+        d.phase_begin = (uint32_t)phases.size();
+        auto pplan = plan_phases(sw, rb);
+        for (auto& pp : pplan) {
+            PhaseDesc Ph{};
+            Ph.op_begin = (uint32_t)ops.size();
+            int slot_of[64];
+            for (int q = 0; q < 64; ++q) slot_of[q] = -1;
+            uint32_t slots[RBMAX], ns = 0;
+            for (uint32_t q = 0; q < nq; ++q)
+                if ((pp.R >> q) & 1) { slot_of[q] = (int)ns; slots[ns++] = q; }
+            uint32_t nt = 0;
+            for (uint32_t b = 0; b < m; ++b) {
+                uint32_t q = d.local_global[b];
+                if (!((pp.R >> q) & 1)) { Ph.tbit_local[nt] = (uint8_t)b; Ph.tbit_global[nt] = (uint8_t)q; ++nt; }
+            }
+            Ph.nt = nt;
+            for (uint32_t i = 0; i < (1u << rb); ++i) {
+                uint32_t off = 0;
+                for (uint32_t sidx = 0; sidx < ns; ++sidx)
+                    if ((i >> sidx) & 1) off |= 1u << local_index[slots[sidx]];
+                Ph.lut[i] = (uint16_t)off;
+            }
+            for (int oi : pp.ops) {
+                const PGate& g = sw.ops[oi];
+                SwOp o{};
+                o.type = g.type;
+                o.q0 = (uint8_t)g.q0;
+                o.q1 = (uint8_t)g.q1;
+                o.k0 = (int8_t)slot_of[g.q0];
+                o.k1 = (g.type == OP_CX || g.type == OP_CZ || g.type == OP_ZZ) ? (int8_t)slot_of[g.q1] : -1;
+                o.mat = (uint32_t)(mats.size() / 2);
+                int cnt = g.type == OP_U1 ? 8 : (g.type == OP_D1 || g.type == OP_ZZ) ? 4 : 0;
+                for (int k = 0; k < cnt; ++k) mats.push_back(g.m[k]);
+                ops.push_back(o);
+            }
+            Ph.op_end = (uint32_t)ops.size();
+            phases.push_back(Ph);
+        }
+        d.phase_end = (uint32_t)phases.size();
+        P->descs.push_back(d);
+    }
+    if (mats.empty()) mats.push_back(0.0);
+    if (ops.empty()) ops.push_back(SwOp{});
+    if (phases.empty()) phases.push_back(PhaseDesc{});
+
+    size_t mat_elem = s->prec == RQ_F32 ? sizeof(float) : sizeof(double);
+    P->off_ph = 0;
+    P->off_ops = (P->off_ph + phases.size() * sizeof(PhaseDesc) + 255) & ~size_t(255);
+    P->off_mat = (P->off_ops + ops.size() * sizeof(SwOp) + 255) & ~size_t(255);
+    size_t total = P->off_mat + mats.size() * mat_elem;
+    std::vector<unsigned char> host(total);
+    std::memcpy(host.data() + P->off_ph, phases.data(), phases.size() * sizeof(PhaseDesc));
+    std::memcpy(host.data() + P->off_ops, ops.data(), ops.size() * sizeof(SwOp));
+    if (s->prec == RQ_F32) {
+        float* f = reinterpret_cast<float*>(host.data() + P->off_mat);
+        for (size_t k = 0; k < mats.size(); ++k) f[k] = (float)mats[k];
+    } else {
+        std::memcpy(host.data() + P->off_mat, mats.data(), mats.size() * sizeof(double));
+    }
+    cudaError_t e = cudaMalloc((void**)&P->dev, total);
+    if (e == cudaSuccess) e = cudaMemcpy(P->dev, host.data(), total, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        if (P->dev) cudaFree(P->dev);
+        delete P;
+        return cuda_fail(e, "plan upload");
+    }
+    P->smem = ((size_t)1 << m) * s->elem_bytes();
+    P->ntiles = 1ull << (nq - m);
+    P->rb = rb;
+    P->stats.gates = filtered.size();
+    P->stats.sweeps = P->descs.size();
+    P->stats.launches = P->descs.size();
+    P->stats.phases = phases.size();
+    P->stats.ops = ops.size();
+    P->stats.hbm_bytes = 2 * S * P->descs.size();
+    *out = P;
+    return RQ_OK;
+}
+
+int apply_one_gate(rq_state* s, const rq_gate& g);   // rq_capi.cu
+
+int plan_launch(rq_state* s, const rq_plan* P) {
+    if (P->mode == RQ_EXEC_PER_GATE) {
+        for (const auto& g : P->gates) RQ_TRY(apply_one_gate(s, g));
+        return RQ_OK;
+    }
+    const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(P->dev + P->off_ph);
+    const SwOp* op = reinterpret_cast<const SwOp*>(P->dev + P->off_ops);
+    const void* mt = P->dev + P->off_mat;
+    for (const auto& d : P->descs) {
+        if (s->prec == RQ_F32) RQ_TRY(launch_sweep<float>(s, d, ph, op, mt, P->ntiles, P->rb, P->smem));
+        else RQ_TRY(launch_sweep<double>(s, d, ph, op, mt, P->ntiles, P->rb, P->smem));
+    }
+    return RQ_OK;
+}
+
+void plan_free(rq_plan* P) {
+    if (!P) return;
+    if (P->dev) {
+        cudaSetDevice(P->device);
+        cudaFree(P->dev);
+    }
+    delete P;
+}
+
+rq_plan_stats plan_stats(const rq_plan* p) { return p->stats; }
+
+bool plan_fits(const rq_plan* p, const rq_state* s) {
+    return p->nq == s->nq && p->prec == s->prec && p->device == s->device;
+}
+
+int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n) {
+    if (n == 0) return RQ_OK;
+    rq_plan* P = nullptr;
+    RQ_TRY(plan_build(s, gates, n, RQ_EXEC_SWEEP, &P));
+    int rc = plan_launch(s, P);
+    // cudaFree of the program waits for the launches that read it
+    plan_free(P);
+    return rc;
+}
+
+}  // namespace rq
