@@ -1,6 +1,7 @@
 """Build libruqu_cuda.so in-tree with nvcc for sm_100a.
 
-Usage: ``python -m ruqu_b200.build`` (or ``ruqu_b200.build.build()``).
+Usage: ``python ruqu_b200/build.py`` (runs without importing the package, so a
+stale or missing library never blocks its own rebuild).
 Objects go to ``ruqu_b200/_build/``; the shared library to
 ``ruqu_b200/libruqu_cuda.so``, next to the package so it ships with it.
 """
