@@ -258,6 +258,32 @@ RQ_API int rq_state_expectation_hamiltonian(rq_state* s, const double* coeffs,
                                      const uint32_t* offsets, uint32_t nterms,
                                      double* out);
 
+/* Allocation-free variant of rq_state_expectation_batch.  No counterpart in
+ * the reference.  For callers that must not allocate device memory -- for
+ * example code that runs with a fixed memory budget already handed out, or a
+ * process whose allocator is owned by another framework -- this entry point
+ * takes the amplitudes as a caller-owned device pointer (interleaved complex,
+ * 2^num_qubits values of `precision`) and keeps its reduction partials in one
+ * fixed static device array of RQ_NOALLOC_SCRATCH_DOUBLES doubles (~1.1 MB per
+ * GPU that loads the library, held until the process exits).
+ *   - at most RQ_NOALLOC_MAX_STRINGS strings per call; more is rejected with
+ *     RQ_ERR_INVALID_ARGUMENT and nothing runs;
+ *   - the first call on a device looks up the scratch address for that device
+ *     (with the device current); make that first call before any stream
+ *     capture;
+ *   - every call shares the one scratch array, so calls that overlap on the
+ *     GPU (other streams, other host threads) race: serialise them;
+ *   - runs on `stream` (a cudaStream_t, NULL = the legacy default stream) on
+ *     the current device and returns after the results are in out[] (host).
+ * It calls no cudaMalloc / cudaFree and no allocating library routine. */
+#define RQ_NOALLOC_MAX_STRINGS 128u
+#define RQ_NOALLOC_MAX_BLOCKS 1024u
+#define RQ_NOALLOC_SCRATCH_DOUBLES ((RQ_NOALLOC_MAX_STRINGS + 1u) * RQ_NOALLOC_MAX_BLOCKS)
+RQ_API int rq_expectation_batch_noalloc(const void* device_amps, uint32_t num_qubits,
+                                        int32_t precision, const rq_pauli_op* ops,
+                                        const uint32_t* offsets, uint32_t nstrings,
+                                        double* out, void* stream);
+
 RQ_API int rq_state_norm_sq(rq_state* s, double* out);
 RQ_API int rq_state_normalize(rq_state* s);                         /* state.rs:415-423 */
 RQ_API int rq_state_fidelity(rq_state* a, rq_state* b, double* out); /* state.rs:426-435 */

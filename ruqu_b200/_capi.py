@@ -71,6 +71,7 @@ SIGNATURES = {
     "rq_state_expectation_batch": (C.c_int, [_vp, _P(RqPauliOp), _P(_u32), _u32, _P(_dbl)]),
     "rq_state_expectation_hamiltonian": (C.c_int, [_vp, _P(_dbl), _P(RqPauliOp), _P(_u32), _u32, _P(_dbl)]),
     "rq_state_norm_sq": (C.c_int, [_vp, _P(_dbl)]),
+    "rq_expectation_batch_noalloc": (C.c_int, [_vp, _u32, _i32, _P(RqPauliOp), _P(_u32), _u32, _P(_dbl), _vp]),
     "rq_state_normalize": (C.c_int, [_vp]),
     "rq_state_fidelity": (C.c_int, [_vp, _vp, _P(_dbl)]),
     "rq_state_download": (C.c_int, [_vp, _P(_dbl)]),
@@ -82,7 +83,7 @@ def _load() -> C.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(
             f"{LIB_PATH} is missing: the CUDA library is the only compute path of ruqu_b200. "
-            "Build it with `python -m ruqu_b200.build`.")
+            "Build it with `python ruqu_b200/build.py`.")
     lib = C.CDLL(LIB_PATH)
     for name, (res, args) in SIGNATURES.items():
         fn = getattr(lib, name)

@@ -9,6 +9,9 @@
 
 #include <algorithm>
 #include <map>
+#include <mutex>
+#include <string>
+#include <vector>
 
 namespace {
 
@@ -266,3 +269,128 @@ int probabilities_dev(rq_state* s, double* dev_out) {
 }
 
 }  // namespace rq
+
+// ---------------------------------------------------------------------------
+// Allocation-free expectation values (rq_expectation_batch_noalloc).
+//
+// Some callers cannot allocate device memory at all (their budget is fixed, or
+// another framework owns the allocator).  For them the partial sums of the
+// Pauli-string reduction live in this one static device array instead of the
+// per-state buffer.  It is fixed in size, exists once per GPU that loads the
+// library, and is shared by every call: two calls in flight at once on the GPU
+// would overwrite each other's partials, so callers must serialise them.
+// Nothing in it has to start at zero: every slot a call reads back was
+// written by that same call's first kernel.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_noalloc_scratch[RQ_NOALLOC_SCRATCH_DOUBLES];
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[kMaxDevices] = {nullptr};
+
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked up
+// once per device, with that device current, and cached.
+int noalloc_scratch_address(int device, double** out) {
+    if (device < 0 || device >= kMaxDevices) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return rq::cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        g_noalloc_addr[device] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_addr[device];
+    return RQ_OK;
+}
+
+}  // namespace
+
+extern "C" int rq_expectation_batch_noalloc(const void* device_amps, uint32_t num_qubits, int32_t precision,
+                                            const rq_pauli_op* ops, const uint32_t* offsets, uint32_t nstrings,
+                                            double* out, void* stream_handle) {
+    if (!device_amps || (!out && nstrings) || (!offsets && nstrings))
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (precision != RQ_F32 && precision != RQ_F64)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "precision must be RQ_F32 or RQ_F64");
+    uint32_t maxq = precision == RQ_F32 ? RQ_MAX_QUBITS_F32 : RQ_MAX_QUBITS_F64;
+    if (num_qubits == 0 || num_qubits > maxq)
+        return rq::fail(RQ_ERR_QUBIT_LIMIT_EXCEEDED, "num_qubits must be in 1.." + std::to_string(maxq));
+    if (nstrings > RQ_NOALLOC_MAX_STRINGS)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "rq_expectation_batch_noalloc takes at most " +
+                                                     std::to_string(RQ_NOALLOC_MAX_STRINGS) + " Pauli strings per call, got " +
+                                                     std::to_string(nstrings));
+    if (nstrings == 0) return RQ_OK;
+    // Pauli strings in mask form (same rules as rq_state_expectation_batch)
+    std::vector<rq::PauliMask> terms(nstrings);
+    for (uint32_t k = 0; k < nstrings; ++k) {
+        if (offsets[k + 1] < offsets[k]) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing");
+        rq::PauliMask m{0, 0, 0};
+        for (uint32_t j = offsets[k]; j < offsets[k + 1]; ++j) {
+            uint32_t q = ops[j].qubit;
+            int op = ops[j].op;
+            if (op < RQ_PAULI_I || op > RQ_PAULI_Z)
+                return rq::fail(RQ_ERR_INVALID_ARGUMENT, "invalid Pauli operator " + std::to_string(op));
+            if (op == RQ_PAULI_I) continue;
+            if (q >= num_qubits)
+                return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "invalid qubit index " + std::to_string(q) + " for " +
+                                                                std::to_string(num_qubits) + "-qubit system");
+            uint64_t b = 1ull << q;
+            if (op == RQ_PAULI_X || op == RQ_PAULI_Y) m.xmask ^= b;
+            if (op == RQ_PAULI_Y || op == RQ_PAULI_Z) m.pmask ^= b;
+            if (op == RQ_PAULI_Y) m.ny += 1;
+        }
+        m.ny &= 3u;
+        terms[k] = m;
+    }
+    int device = 0;
+    RQ_CUDA(cudaGetDevice(&device));
+    double* scratch = nullptr;
+    RQ_TRY(noalloc_scratch_address(device, &scratch));
+    cudaStream_t st = static_cast<cudaStream_t>(stream_handle);
+    const uint64_t n = 1ull << num_qubits;
+    unsigned G = (unsigned)std::min<int>(rq::num_sms(device) * 4, (int)RQ_NOALLOC_MAX_BLOCKS);
+    // partials occupy [0, nstrings*G); the finalised sums follow at nstrings*G
+    std::map<uint64_t, std::vector<uint32_t>> groups;
+    for (uint32_t k = 0; k < nstrings; ++k) groups[terms[k].xmask].push_back(k);
+    std::vector<uint32_t> slot_of(nstrings);
+    uint32_t slot = 0;
+    for (auto& kv : groups) {
+        uint64_t x = kv.first;
+        uint32_t h = x ? 63 - __builtin_clzll(x) : 0;
+        uint64_t count = x ? n >> 1 : n;
+        const auto& idx = kv.second;
+        for (size_t c0 = 0; c0 < idx.size(); c0 += KMAX) {
+            TermChunk tc{};
+            tc.k = (int)std::min<size_t>(KMAX, idx.size() - c0);
+            for (int k = 0; k < tc.k; ++k) {
+                const rq::PauliMask& t = terms[idx[c0 + k]];
+                tc.pmask[k] = t.pmask;
+                tc.odd[k] = x ? (__builtin_popcountll(x & t.pmask) & 1) : 0;
+                slot_of[idx[c0 + k]] = slot + k;
+            }
+            if (precision == RQ_F32)
+                k_pauli<float><<<G, TPB, 0, st>>>((const float2*)device_amps, count, x, h, tc, scratch, slot, G);
+            else
+                k_pauli<double><<<G, TPB, 0, st>>>((const double2*)device_amps, count, x, h, tc, scratch, slot, G);
+            RQ_CUDA(cudaGetLastError());
+            slot += tc.k;
+        }
+    }
+    double* sums = scratch + (size_t)nstrings * G;
+    k_finalize<<<nstrings, TPB, 0, st>>>(scratch, G, G, sums);
+    RQ_CUDA(cudaGetLastError());
+    std::vector<double> host(nstrings);
+    RQ_CUDA(cudaMemcpyAsync(host.data(), sums, nstrings * sizeof(double), cudaMemcpyDeviceToHost, st));
+    RQ_CUDA(cudaStreamSynchronize(st));
+    for (uint32_t k = 0; k < nstrings; ++k) {
+        const rq::PauliMask& t = terms[k];
+        double acc = host[slot_of[k]];
+        if (t.xmask == 0) out[k] = acc * re_ipow(t.ny);
+        else if (!(__builtin_popcountll(t.xmask & t.pmask) & 1)) out[k] = 2.0 * acc * re_ipow(t.ny);
+        else out[k] = 2.0 * acc * re_ipow(t.ny + 1);
+    }
+    return RQ_OK;
+}
