@@ -289,6 +289,45 @@ RQ_API int rq_state_normalize(rq_state* s);                         /* state.rs:
 RQ_API int rq_state_fidelity(rq_state* a, rq_state* b, double* out); /* state.rs:426-435 */
 
 /* ------------------------------------------------------------------------ */
+/* batched QAOA-MaxCut (qaoa.rs:125-201 over many graphs / parameter sets)    */
+/* ------------------------------------------------------------------------ */
+
+typedef struct rq_qaoa_batch rq_qaoa_batch;
+
+/* `ninst` simple unweighted graphs (unit weights, as the MaxCut instances of
+ * qaoa.rs:59-66 `Graph::unweighted`): graph k has num_nodes[k] vertices
+ * (7..30 for f32 states, 6..30 for f64) and the edges
+ * edges[2e], edges[2e+1] for e in [edge_offsets[k], edge_offsets[k+1]).
+ * p = QAOA depth.  The graphs and the planned sweep programs stay on the GPU. */
+RQ_API int rq_qaoa_batch_create(uint32_t ninst, const uint32_t* num_nodes,
+                                const uint32_t* edge_offsets, const uint32_t* edges,
+                                uint32_t p, int32_t precision, rq_qaoa_batch** out);
+
+/* Evaluate ninst*nsets circuits: circuit c = inst*nsets + set uses
+ * gammas[c*p .. c*p+p) and betas[c*p .. c*p+p) and the graph of inst.  Each
+ * is the circuit of build_qaoa_circuit; energies[c] = its expected cut
+ * sum_edges (1 - <Z_i Z_j>)/2 (evaluate_qaoa_cost), accumulated in FP64.
+ * With shots > 0, shot s of circuit c measures all qubits in order with draws
+ * 0..n-1 of key base_seed + (c << 32) + s (the run_shots semantics of
+ * simulator.rs:107-147 with that seed), and best_bits[c] / best_cut[c] are
+ * the sampled bitstring with the highest cut (lowest shot index on ties). */
+RQ_API int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas,
+                             const double* betas, double* energies, uint32_t shots,
+                             uint64_t base_seed, uint64_t* best_bits, uint32_t* best_cut);
+
+/* Final amplitudes of one circuit of the last run (2^n interleaved doubles);
+ * only circuits of the last memory wave of that run are still held. */
+RQ_API int rq_qaoa_batch_state(rq_qaoa_batch* b, uint64_t circuit, double* interleaved);
+
+/* Device time of the last run (CUDA events around all of its kernels), ms. */
+RQ_API int rq_qaoa_batch_last_ms(const rq_qaoa_batch* b, float* ms);
+
+/* Upper bound of state memory per wave (default 24 GiB). */
+RQ_API int rq_qaoa_batch_set_state_budget(rq_qaoa_batch* b, uint64_t bytes);
+
+RQ_API int rq_qaoa_batch_destroy(rq_qaoa_batch* b);
+
+/* ------------------------------------------------------------------------ */
 /* host transfer (state_vector / amplitudes_mut / from_amplitudes)           */
 /* ------------------------------------------------------------------------ */
 

@@ -1,0 +1,91 @@
+"""Batched QAOA-MaxCut on the GPU (rq_qaoa_batch_* of include/ruqu_cuda.h).
+
+Evaluates the circuit of build_qaoa_circuit (crates/ruqu-algorithms/src/qaoa.rs:125-153)
+for many graphs and many (gamma, beta) sets in one call, returning the expected cut of
+evaluate_qaoa_cost (qaoa.rs:179-201) per circuit and, optionally, the best cut among
+shots drawn with run_shots semantics (crates/ruqu-core/src/simulator.rs:107-147).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._capi import RQ_F32, RQ_F64, lib
+from .error import check
+
+
+def _u32p(a):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class QaoaBatch:
+    """graphs: sequence of (num_nodes, [(u, v), ...]) simple unweighted graphs."""
+
+    def __init__(self, graphs, p: int, precision: str = "f32"):
+        self.graphs = [(int(n), [(int(u), int(v)) for u, v in e]) for n, e in graphs]
+        self.p = int(p)
+        self.precision = precision
+        nodes = np.ascontiguousarray([g[0] for g in self.graphs], dtype=np.uint32)
+        offs = np.zeros(len(self.graphs) + 1, dtype=np.uint32)
+        flat = []
+        for k, (_, e) in enumerate(self.graphs):
+            for u, v in e:
+                flat += [u, v]
+            offs[k + 1] = offs[k] + len(e)
+        edges = np.ascontiguousarray(flat if flat else [0, 0], dtype=np.uint32)
+        h = C.c_void_p()
+        check(lib.rq_qaoa_batch_create(len(self.graphs), _u32p(nodes), _u32p(offs), _u32p(edges), self.p,
+                                       RQ_F32 if precision == "f32" else RQ_F64, C.byref(h)))
+        self._h = h
+        self.nsets = 1
+
+    def run(self, gammas, betas, shots: int = 0, seed: int = 0):
+        """gammas, betas: (ninst, p) or (ninst, nsets, p).  Returns energies of shape
+        (ninst,) or (ninst, nsets), plus best_bits / best_cut when shots > 0."""
+        g = np.asarray(gammas, dtype=np.float64)
+        b = np.asarray(betas, dtype=np.float64)
+        squeeze = g.ndim == 2
+        if squeeze:
+            g = g[:, None, :]
+            b = b[:, None, :]
+        ninst, nsets, p = g.shape
+        assert ninst == len(self.graphs) and p == self.p and b.shape == g.shape
+        g = np.ascontiguousarray(g.reshape(-1))
+        b = np.ascontiguousarray(b.reshape(-1))
+        e = np.empty(ninst * nsets)
+        bb = np.zeros(ninst * nsets, dtype=np.uint64)
+        bc = np.zeros(ninst * nsets, dtype=np.uint32)
+        check(lib.rq_qaoa_batch_run(self._h, nsets, _dp(g), _dp(b), _dp(e), int(shots), int(seed) & (2**64 - 1),
+                                    bb.ctypes.data_as(C.POINTER(C.c_uint64)), _u32p(bc)))
+        self.nsets = nsets
+        shape = (ninst,) if squeeze else (ninst, nsets)
+        out = {"energies": e.reshape(shape)}
+        if shots:
+            out["best_bits"] = bb.reshape(shape)
+            out["best_cut"] = bc.reshape(shape)
+        return out
+
+    def state(self, circuit: int) -> np.ndarray:
+        n = self.graphs[circuit // self.nsets][0]
+        out = np.empty(2 << n)
+        check(lib.rq_qaoa_batch_state(self._h, int(circuit), _dp(out)))
+        return out.view(np.complex128)
+
+    def last_ms(self) -> float:
+        ms = C.c_float()
+        check(lib.rq_qaoa_batch_last_ms(self._h, C.byref(ms)))
+        return ms.value
+
+    def set_state_budget(self, nbytes: int) -> None:
+        check(lib.rq_qaoa_batch_set_state_budget(self._h, int(nbytes)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None:
+            lib.rq_qaoa_batch_destroy(h)
+            self._h = None

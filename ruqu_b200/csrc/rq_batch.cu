@@ -1,0 +1,854 @@
+// rq_batch.cu -- batched QAOA-MaxCut: many graphs and parameter sets at once.
+//
+// The reference evaluates one QAOA circuit at a time: evaluate_qaoa_cost
+// (qaoa.rs:179-201) builds the circuit of build_qaoa_circuit (qaoa.rs:125-153:
+// H on every qubit, then per layer Rzz(2*gamma*w) on every edge and
+// Rx(2*beta) on every qubit), runs it on a fresh state and sums
+// w*(1 - <Z_i Z_j>)/2 over the edges with one expectation pass per edge.
+// Here every circuit of a batch runs through shared sweep programs:
+//
+//  * circuits with the same qubit count form a class and share one planned
+//    program (rq_plan.cuh); a launch covers (circuit, tile) pairs of a class;
+//  * H^n|0> is synthesised by the first sweep (uniform amplitude 2^(-n/2));
+//  * the product of all Rzz of a layer is one diagonal phase
+//    exp(-i*gamma*(|E| - 2 cut(x))) (unit weights): each thread derives
+//    cut(x) for its 2^RB register amplitudes from the graph's edge list
+//    (edges between non-register bits are constant per thread, edges touching
+//    a register slot add per-slot counts) and looks the phase up in a table;
+//  * the last sweep reduces <C> = sum_x |a_x|^2 cut(x) in FP64 (the same
+//    quantity as the per-edge sum of qaoa.rs:194-200) into per-tile partials;
+//  * optional shots: FP64 prefix trees per circuit, then every shot walks its
+//    circuit's tree with the documented uniform stream, and a block reduction
+//    keeps the best cut (highest cut, lowest shot index on ties).
+#include "rq_internal.cuh"
+#include "rq_plan.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace {
+
+using rqd::C2;
+using namespace rqp;
+
+template <typename T> struct Vec16b;
+template <> struct Vec16b<float> { using t = float4; static constexpr int EPV = 2; };
+template <> struct Vec16b<double> { using t = double2; static constexpr int EPV = 1; };
+
+template <typename T>
+__device__ __forceinline__ uint32_t swzb(uint32_t e) {
+    constexpr int CB = sizeof(typename C2<T>::t) == 8 ? 4 : 3;
+    uint32_t r = e >> CB;
+    uint32_t f = r ^ (r >> CB) ^ (r >> (2 * CB)) ^ (r >> (3 * CB));
+    return e ^ (f & ((1u << CB) - 1));
+}
+
+// Per-class launch arguments.
+template <typename T>
+struct QArgs {
+    typename C2<T>::t* amps;       // circuit c at amps + c * 2^n
+    uint64_t ncirc;                // circuits in this wave
+    uint64_t ntiles;               // tiles per circuit
+    uint64_t circ0;                // global index of the wave's first circuit
+    const uint32_t* circ_inst;     // global circuit -> instance
+    const uint8_t* edges;          // (u, v) byte pairs of all instances
+    const uint32_t* eoff;          // instance -> first edge
+    const uint32_t* ne;            // instance -> edge count
+    const T* rx;                   // [global circuit][p] (cos beta, sin beta)
+    const T* ph;                   // [global circuit][p][phs] (re, im) of exp(-i gamma (|E| - 2k))
+    uint32_t p, phs;
+    double* epart;                 // [wave circuit][ntiles]
+    T amp0;                        // 2^(-n/2)
+};
+
+// cut(x) for the register amplitudes of one thread: x = U | deposit(i).
+// Edges with no endpoint on a register slot contribute a per-thread constant;
+// an edge from slot s to a non-slot vertex w contributes bit_s(i) xor bit_w(U),
+// i.e. a0[s] edges count when bit_s(i) = 1 and a1[s] edges when it is 0;
+// edges between two slots (at most 10 in a simple graph) are listed.
+template <int RB>
+struct CutPlan {
+    int cu;
+    int a0[RB], a1[RB];
+    uint64_t ss;   // 6 bits per slot-slot edge: s | t << 3
+    int nss;
+};
+
+template <int RB>
+__device__ __forceinline__ void cut_plan(CutPlan<RB>& cp, const uint8_t* __restrict__ e, uint32_t ne, uint64_t U,
+                                         uint64_t slotmask) {
+    cp.cu = 0;
+#pragma unroll
+    for (int s = 0; s < RB; ++s) { cp.a0[s] = 0; cp.a1[s] = 0; }
+    cp.ss = 0;
+    cp.nss = 0;
+    for (uint32_t k = 0; k < ne; ++k) {
+        const uint32_t u = e[2 * k], v = e[2 * k + 1];
+        const bool su = (slotmask >> u) & 1ull, sv = (slotmask >> v) & 1ull;
+        const int bu = (int)((U >> u) & 1ull), bv = (int)((U >> v) & 1ull);
+        if (!su && !sv) {
+            cp.cu += bu ^ bv;
+        } else if (su && !sv) {
+            const int s = __popcll(slotmask & ((1ull << u) - 1));
+            if (bv) cp.a1[s]++; else cp.a0[s]++;
+        } else if (!su && sv) {
+            const int s = __popcll(slotmask & ((1ull << v) - 1));
+            if (bu) cp.a1[s]++; else cp.a0[s]++;
+        } else if (cp.nss < 10) {
+            const uint64_t s = (uint64_t)__popcll(slotmask & ((1ull << u) - 1));
+            const uint64_t t = (uint64_t)__popcll(slotmask & ((1ull << v) - 1));
+            cp.ss |= (s | (t << 3)) << (6 * cp.nss);
+            cp.nss++;
+        }
+    }
+}
+
+template <int RB>
+__device__ __forceinline__ int cut_of(const CutPlan<RB>& cp, int i) {
+    int c = cp.cu;
+#pragma unroll
+    for (int s = 0; s < RB; ++s) c += ((i >> s) & 1) ? cp.a0[s] : cp.a1[s];
+    uint64_t ss = cp.ss;
+    for (int k = 0; k < cp.nss; ++k, ss >>= 6) {
+        const int s = (int)(ss & 7), t = (int)((ss >> 3) & 7);
+        c += ((i >> s) ^ (i >> t)) & 1;
+    }
+    return c;
+}
+
+template <typename V, typename T>
+__device__ __forceinline__ V cmulv(V a, T br, T bi) {
+    V r;
+    r.x = a.x * br - a.y * bi;
+    r.y = a.x * bi + a.y * br;
+    return r;
+}
+
+// Rx(2 beta) on slot K: [[c, -i s], [-i s, c]]
+template <int K, int NR, typename V, typename T>
+__device__ __forceinline__ void op_rx(V* reg, T c, T s) {
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+        if (i & (1 << K)) continue;
+        const int j = i | (1 << K);
+        V x = reg[i], y = reg[j];
+        V o0, o1;
+        o0.x = c * x.x + s * y.y;
+        o0.y = c * x.y - s * y.x;
+        o1.x = s * x.y + c * y.x;
+        o1.y = c * y.y - s * x.x;
+        reg[i] = o0;
+        reg[j] = o1;
+    }
+}
+
+template <int NR, typename V, typename T>
+__device__ __forceinline__ void dispatch_rx(int k, V* reg, T c, T s) {
+    switch (k) {
+        case 0: op_rx<0, NR>(reg, c, s); break;
+        case 1: op_rx<1, NR>(reg, c, s); break;
+        case 2: op_rx<2, NR>(reg, c, s); break;
+        case 3: if constexpr (NR > 8) op_rx<3, NR>(reg, c, s); break;
+        case 4: if constexpr (NR > 16) op_rx<4, NR>(reg, c, s); break;
+        default: break;
+    }
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Batched QAOA sweep over (circuit, tile) work items of one class.
+template <typename T, int RB>
+__global__ void __launch_bounds__(256, 2) k_qaoa_sweep(const SweepDesc d, const PhaseDesc* __restrict__ phases,
+                                                      const SwOp* __restrict__ ops, QArgs<T> a) {
+    using V = typename C2<T>::t;
+    using VV = typename Vec16b<T>::t;
+    constexpr int NR = 1 << RB;
+    constexpr int EPV = Vec16b<T>::EPV;
+    constexpr int VPT = NR / EPV;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* sm = reinterpret_cast<V*>(smem_raw);
+    __shared__ double red[256];
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t T_ = blockDim.x;
+    const uint64_t cmask = (1ull << d.c) - 1;
+    uint64_t dep_tid = 0;
+    {
+        uint64_t x = (uint64_t)tid * EPV;
+        dep_tid = x & cmask;
+        for (uint32_t b = d.c; b < d.m; ++b)
+            if ((x >> b) & 1ull) dep_tid |= 1ull << d.local_global[b];
+    }
+    const uint64_t nwork = a.ncirc * a.ntiles;
+    const uint64_t nstate = 1ull << d.n;
+
+    for (uint64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const uint64_t circ = w / a.ntiles, tile = w - circ * a.ntiles;
+        const uint64_t gcirc = a.circ0 + circ;
+        V* amps = a.amps + circ * nstate;
+        const uint32_t inst = a.circ_inst[gcirc];
+        const uint8_t* edges = a.edges + 2 * (size_t)a.eoff[inst];
+        const uint32_t ne = a.ne[inst];
+        uint64_t base = 0;
+        for (uint32_t b = 0; b < d.nonlocal_count; ++b)
+            if ((tile >> b) & 1ull) base |= 1ull << d.nonlocal[b];
+
+        const bool init = (d.flags & SWEEP_INIT_UNIFORM) != 0;
+        if (!init) {
+#pragma unroll 1
+            for (int j0 = 0; j0 < VPT; j0 += 8) {
+                VV v[8];
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj)
+                    v[jj] = __ldcs(reinterpret_cast<const VV*>(amps + (base | dep_tid | d.gj[j0 + jj])));
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj) {
+                    const uint32_t e = (tid + T_ * (j0 + jj)) * EPV;
+                    if constexpr (EPV == 2) {
+                        sm[swzb<T>(e)] = make_float2(v[jj].x, v[jj].y);
+                        sm[swzb<T>(e + 1)] = make_float2(v[jj].z, v[jj].w);
+                    } else {
+                        sm[swzb<T>(e)] = *reinterpret_cast<V*>(&v[jj]);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+
+        double energy = 0.0;
+        for (uint32_t p = d.phase_begin; p < d.phase_end; ++p) {
+            const PhaseDesc& ph = phases[p];
+            uint32_t ebase = 0;
+            uint64_t U = base;
+            for (uint32_t b = 0; b < ph.nt; ++b)
+                if ((tid >> b) & 1u) {
+                    ebase |= 1u << ph.tbit_local[b];
+                    U |= 1ull << ph.tbit_global[b];
+                }
+            uint64_t slotmask = 0;
+#pragma unroll
+            for (int s = 0; s < RB; ++s) slotmask |= 1ull << ph.slot_global[s];
+            V reg[NR];
+            if (init && p == d.phase_begin) {
+#pragma unroll
+                for (int i = 0; i < NR; ++i) { reg[i].x = a.amp0; reg[i].y = (T)0; }
+            } else {
+#pragma unroll
+                for (int i = 0; i < NR; ++i) reg[i] = sm[swzb<T>(ebase | ph.lut[i])];
+            }
+            for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
+                const SwOp op = ops[o];
+                if (op.type == OP_RXP) {
+                    const T* r = a.rx + ((size_t)gcirc * a.p + op.param) * 2;
+                    dispatch_rx<NR>(op.k0, reg, r[0], r[1]);
+                } else if (op.type == OP_CPH) {
+                    CutPlan<RB> cp;
+                    cut_plan<RB>(cp, edges, ne, U, slotmask);
+                    const T* tab = a.ph + ((size_t)gcirc * a.p + op.param) * a.phs * 2;
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) {
+                        const int c = cut_of<RB>(cp, i);
+                        reg[i] = cmulv(reg[i], tab[2 * c], tab[2 * c + 1]);
+                    }
+                }
+            }
+            if ((d.flags & SWEEP_ENERGY) && p + 1 == d.phase_end) {
+                CutPlan<RB> cp;
+                cut_plan<RB>(cp, edges, ne, U, slotmask);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) {
+                    const double re = (double)reg[i].x, im = (double)reg[i].y;
+                    energy += (re * re + im * im) * (double)cut_of<RB>(cp, i);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < NR; ++i) sm[swzb<T>(ebase | ph.lut[i])] = reg[i];
+            __syncthreads();
+        }
+
+        if (d.flags & SWEEP_ENERGY) {
+            // fixed-order sum over the block (any block size, also < 32 threads)
+            red[tid] = energy;
+            __syncthreads();
+            if (tid == 0) {
+                double r = 0.0;
+                for (uint32_t k = 0; k < T_; ++k) r += red[k];
+                a.epart[circ * a.ntiles + tile] = r;
+            }
+            __syncthreads();
+        }
+
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) {
+            const uint32_t e = (tid + T_ * j) * EPV;
+            const uint64_t g = base | dep_tid | d.gj[j];
+            VV v;
+            if constexpr (EPV == 2) {
+                float2 x = sm[swzb<T>(e)], y = sm[swzb<T>(e + 1)];
+                v = make_float4(x.x, x.y, y.x, y.y);
+            } else {
+                V x = sm[swzb<T>(e)];
+                v = *reinterpret_cast<VV*>(&x);
+            }
+            __stcs(reinterpret_cast<VV*>(amps + g), v);
+        }
+        __syncthreads();
+    }
+}
+
+// energies[circ0 + c] = sum over the circuit's tile partials (fixed order)
+__global__ void k_energy_finalize(const double* __restrict__ epart, uint64_t ncirc, uint64_t ntiles, uint64_t circ0,
+                                  double* __restrict__ energies) {
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncirc; c += (uint64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (uint64_t t = 0; t < ntiles; ++t) s += epart[c * ntiles + t];
+        energies[circ0 + c] = s;
+    }
+}
+
+// per-circuit tables from the angles: Rx(2 beta) -> (cos beta, sin beta);
+// cost phase exp(-i gamma (|E| - 2k)) for k = 0..|E|
+template <typename T>
+__global__ void k_qaoa_tables(const double* __restrict__ gammas, const double* __restrict__ betas,
+                              const uint32_t* __restrict__ circ_inst, const uint32_t* __restrict__ ne, uint64_t ncirc,
+                              uint32_t p, uint32_t phs, T* __restrict__ rx, T* __restrict__ ph) {
+    const uint64_t total = ncirc * p;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = w / p;
+        const double g = gammas[w], b = betas[w];
+        double sb, cb;
+        sincos(b, &sb, &cb);
+        rx[2 * w] = (T)cb;
+        rx[2 * w + 1] = (T)sb;
+        const int E = (int)ne[circ_inst[c]];
+        T* t = ph + w * phs * 2;
+        for (int k = 0; k < (int)phs; ++k) {
+            double sv, cv;
+            sincos(g * (double)(E - 2 * k), &sv, &cv);
+            t[2 * k] = (T)cv;
+            t[2 * k + 1] = (T)(-sv);
+        }
+    }
+}
+
+// ---- sampling -------------------------------------------------------------
+
+template <typename T>
+__device__ __forceinline__ double pr(const typename C2<T>::t* a, uint64_t i) {
+    auto x = a[i];
+    double re = x.x, im = x.y;
+    return __dadd_rn(__dmul_rn(re, re), __dmul_rn(im, im));
+}
+
+// level n-1 of every circuit's tree (tree of circuit c at tree + c * 2^n)
+template <typename T>
+__global__ void k_bleaf(const typename C2<T>::t* __restrict__ amps, uint32_t n, uint64_t ncirc, double* __restrict__ tree) {
+    const uint64_t half = 1ull << (n - 1), per = 1ull << n;
+    const uint64_t total = ncirc * half;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = w >> (n - 1), j = w & (half - 1);
+        const typename C2<T>::t* a = amps + c * per;
+        tree[c * per + (half - 1) + j] = __dadd_rn(pr<T>(a, j), pr<T>(a, j + half));
+    }
+}
+
+__global__ void k_bfold(double* __restrict__ tree, uint32_t n, uint64_t ncirc, uint32_t k) {
+    const uint64_t len = 1ull << k, per = 1ull << n;
+    const uint64_t total = ncirc * len;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = w >> k, j = w & (len - 1);
+        double* t = tree + c * per;
+        const double* up = t + ((1ull << (k + 1)) - 1);
+        t[(len - 1) + j] = __dadd_rn(up[j], up[j + len]);
+    }
+}
+
+// one block per circuit: shots, cut of each, best (max cut, lowest shot)
+template <typename T>
+__global__ void k_bsample(const typename C2<T>::t* __restrict__ amps, const double* __restrict__ tree, uint32_t n,
+                          uint64_t ncirc, uint64_t circ0, const uint32_t* __restrict__ circ_inst,
+                          const uint64_t* __restrict__ user_of,
+                          const uint8_t* __restrict__ edges_all, const uint32_t* __restrict__ eoff,
+                          const uint32_t* __restrict__ nes, uint32_t shots, uint64_t base_seed,
+                          uint64_t* __restrict__ best_bits, uint32_t* __restrict__ best_cut) {
+    __shared__ unsigned long long sh_key[32];
+    __shared__ uint64_t sh_bits[32];
+    const uint64_t per = 1ull << n;
+    for (uint64_t c = blockIdx.x; c < ncirc; c += gridDim.x) {
+        const uint64_t gc = circ0 + c;
+        const typename C2<T>::t* a = amps + c * per;
+        const double* t = tree + c * per;
+        const uint32_t inst = circ_inst[gc];
+        const uint8_t* e = edges_all + 2 * (size_t)eoff[inst];
+        const uint32_t ne = nes[inst];
+        // key orders by (cut desc, shot asc): (cut << 32) | (0xffffffff - shot)
+        unsigned long long best = 0;
+        uint64_t bbits = 0;
+        for (uint32_t s = threadIdx.x; s < shots; s += blockDim.x) {
+            const uint64_t key = base_seed + (user_of[gc] << 32) + s;
+            uint64_t prefix = 0;
+            for (uint32_t q = 0; q < n; ++q) {
+                double m0, m1;
+                if (q + 1 == n) {
+                    m0 = pr<T>(a, prefix);
+                    m1 = pr<T>(a, prefix | (1ull << q));
+                } else {
+                    const double* L = t + ((1ull << (q + 1)) - 1);
+                    m0 = L[prefix];
+                    m1 = L[prefix | (1ull << q)];
+                }
+                const double p0 = m0 / __dadd_rn(m0, m1);
+                const double u = rqd::uniform(key, 0, q);
+                if (u >= p0) prefix |= 1ull << q;
+            }
+            uint32_t cut = 0;
+            for (uint32_t k = 0; k < ne; ++k) cut += (uint32_t)(((prefix >> e[2 * k]) ^ (prefix >> e[2 * k + 1])) & 1ull);
+            const unsigned long long kk = ((unsigned long long)cut << 32) | (0xffffffffull - s);
+            if (kk > best || (best == 0 && s == threadIdx.x)) {
+                best = kk;
+                bbits = prefix;
+            }
+        }
+        // block argmax of the key
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            unsigned long long ok = __shfl_down_sync(0xffffffffu, best, o);
+            uint64_t ob = __shfl_down_sync(0xffffffffu, bbits, o);
+            if (ok > best) { best = ok; bbits = ob; }
+        }
+        if ((threadIdx.x & 31) == 0) { sh_key[threadIdx.x >> 5] = best; sh_bits[threadIdx.x >> 5] = bbits; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long b = sh_key[0];
+            uint64_t bb = sh_bits[0];
+            for (uint32_t wv = 1; wv < (blockDim.x >> 5); ++wv)
+                if (sh_key[wv] > b) { b = sh_key[wv]; bb = sh_bits[wv]; }
+            best_bits[gc] = bb;
+            best_cut[gc] = (uint32_t)(b >> 32);
+        }
+        __syncthreads();
+    }
+}
+
+constexpr int TPB = 256;
+
+}  // namespace
+
+// ===========================================================================
+// batch object
+// ===========================================================================
+struct QClass {
+    uint32_t n = 0, m = 0, c = 0;
+    std::vector<uint32_t> insts;            // instances of this size
+    std::vector<SweepDesc> descs;
+    unsigned char* prog = nullptr;          // phases | ops
+    size_t off_ops = 0;
+    size_t smem = 0;
+    uint64_t ntiles = 0;
+};
+
+struct rq_qaoa_batch {
+    int device = 0;
+    int32_t prec = RQ_F32;
+    uint32_t ninst = 0, p = 0, phs = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<uint32_t> n_of, ne_of;
+    std::vector<QClass> classes;
+    // device copies
+    uint8_t* d_edges = nullptr;
+    uint32_t* d_eoff = nullptr;
+    uint32_t* d_ne = nullptr;
+    // per-run buffers
+    uint32_t* d_circ_inst = nullptr;       // global circuit -> instance (class-major order)
+    uint64_t* d_user = nullptr;            // run position -> caller's circuit index
+    size_t circ_cap = 0;
+    double* d_ang = nullptr;               // gammas | betas in circuit order
+    void* d_rx = nullptr;
+    void* d_ph = nullptr;
+    double* d_energy = nullptr;
+    uint64_t* d_best_bits = nullptr;
+    uint32_t* d_best_cut = nullptr;
+    void* d_states = nullptr;              // wave buffer
+    size_t states_cap = 0;                 // bytes
+    double* d_epart = nullptr;
+    size_t epart_cap = 0;                  // doubles
+    double* d_tree = nullptr;
+    size_t tree_cap = 0;                   // doubles
+    std::vector<uint64_t> order;           // run-order position -> user circuit index
+    // last run: which wave holds which circuits (for rq_qaoa_batch_state)
+    uint32_t last_nsets = 0;
+    uint64_t last_wave_first = 0, last_wave_count = 0;
+    uint32_t last_wave_n = 0;
+    float last_ms = 0.f;
+    size_t state_budget = (size_t)24 << 30;
+};
+
+namespace {
+
+size_t elem_size(int32_t prec) { return prec == RQ_F32 ? 8 : 16; }
+
+template <typename P>
+int grow(P** ptr, size_t* cap, size_t need_elems) {
+    if (*cap >= need_elems) return RQ_OK;
+    if (*ptr) cudaFree(*ptr);
+    *ptr = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc((void**)ptr, need_elems * sizeof(P));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return rq::fail(RQ_ERR_MEMORY_ALLOCATION,
+                        "memory allocation failed: need " + std::to_string(need_elems * sizeof(P)) + " bytes");
+    }
+    *cap = need_elems;
+    return RQ_OK;
+}
+
+int grow_bytes(void** ptr, size_t* cap, size_t bytes) {
+    if (*cap >= bytes) return RQ_OK;
+    if (*ptr) cudaFree(*ptr);
+    *ptr = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return rq::fail(RQ_ERR_MEMORY_ALLOCATION, "memory allocation failed: need " + std::to_string(bytes) + " bytes");
+    }
+    *cap = bytes;
+    return RQ_OK;
+}
+
+template <typename T>
+int launch_class(rq_qaoa_batch* b, QClass& K, uint64_t ncirc, uint64_t circ0, void* states) {
+    using V = typename C2<T>::t;
+    const uint32_t rb = std::is_same<T, float>::value ? 5 : 4;
+    constexpr int RBc = std::is_same<T, float>::value ? 5 : 4;
+    QArgs<T> a{};
+    a.amps = (V*)states;
+    a.ncirc = ncirc;
+    a.ntiles = K.ntiles;
+    a.circ0 = circ0;
+    a.circ_inst = b->d_circ_inst;
+    a.edges = b->d_edges;
+    a.eoff = b->d_eoff;
+    a.ne = b->d_ne;
+    a.rx = (const T*)b->d_rx;
+    a.ph = (const T*)b->d_ph;
+    a.p = b->p;
+    a.phs = b->phs;
+    a.epart = b->d_epart;
+    a.amp0 = (T)std::sqrt(std::ldexp(1.0, -(int)K.n));
+    const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(K.prog);
+    const SwOp* op = reinterpret_cast<const SwOp*>(K.prog + K.off_ops);
+    auto kern = k_qaoa_sweep<T, RBc>;
+    RQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem));
+    const unsigned threads = 1u << (K.m - rb);
+    int per_sm = 0;
+    RQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)threads, K.smem));
+    if (per_sm < 1) return rq::fail(RQ_ERR_CUDA, "batched sweep kernel does not fit on an SM");
+    const uint64_t work = ncirc * K.ntiles;
+    const unsigned grid = (unsigned)std::min<uint64_t>(work, (uint64_t)rq::num_sms(b->device) * per_sm);
+    for (const auto& d : K.descs) {
+        kern<<<grid, threads, K.smem, b->stream>>>(d, ph, op, a);
+        RQ_CUDA(cudaGetLastError());
+    }
+    k_energy_finalize<<<rq::grid_for(ncirc, TPB, rq::num_sms(b->device)), TPB, 0, b->stream>>>(
+        b->d_epart, ncirc, K.ntiles, circ0, b->d_energy);
+    RQ_CUDA(cudaGetLastError());
+    return RQ_OK;
+}
+
+template <typename T>
+int sample_class(rq_qaoa_batch* b, QClass& K, uint64_t ncirc, uint64_t circ0, void* states, uint32_t shots,
+                 uint64_t seed) {
+    using V = typename C2<T>::t;
+    const uint32_t n = K.n;
+    const uint64_t per = 1ull << n;
+    // trees for as many circuits as the tree scratch allows
+    const size_t tree_budget = (size_t)8 << 30;
+    uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(ncirc, tree_budget / (per * sizeof(double))));
+    RQ_TRY(grow(&b->d_tree, &b->tree_cap, chunk * per));
+    const int sms = rq::num_sms(b->device);
+    for (uint64_t c0 = 0; c0 < ncirc; c0 += chunk) {
+        const uint64_t cn = std::min<uint64_t>(chunk, ncirc - c0);
+        const V* a = (const V*)states + c0 * per;
+        k_bleaf<T><<<rq::grid_for(cn * (per >> 1), TPB, sms), TPB, 0, b->stream>>>(a, n, cn, b->d_tree);
+        RQ_CUDA(cudaGetLastError());
+        for (int k = (int)n - 2; k >= 0; --k) {
+            k_bfold<<<rq::grid_for(cn << k, TPB, sms), TPB, 0, b->stream>>>(b->d_tree, n, cn, (uint32_t)k);
+            RQ_CUDA(cudaGetLastError());
+        }
+        const unsigned g = (unsigned)std::min<uint64_t>(cn, (uint64_t)sms * 8);
+        k_bsample<T><<<g, 256, 0, b->stream>>>(a, b->d_tree, n, cn, circ0 + c0, b->d_circ_inst, b->d_user, b->d_edges, b->d_eoff,
+                                               b->d_ne, shots, seed, b->d_best_bits, b->d_best_cut);
+        RQ_CUDA(cudaGetLastError());
+    }
+    return RQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rq_qaoa_batch_create(uint32_t ninst, const uint32_t* num_nodes, const uint32_t* edge_offsets,
+                         const uint32_t* edges, uint32_t p, int32_t precision, rq_qaoa_batch** out) {
+    if (!out || (!num_nodes && ninst) || (!edge_offsets && ninst)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (precision != RQ_F32 && precision != RQ_F64)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "precision must be RQ_F32 or RQ_F64");
+    if (p == 0 || p > 64) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "p must be in 1..64");
+    const uint32_t rb = precision == RQ_F32 ? 5 : 4;
+    const uint32_t mloc = precision == RQ_F32 ? 13 : 12;
+    std::unique_ptr<rq_qaoa_batch> b(new rq_qaoa_batch());
+    b->prec = precision;
+    b->ninst = ninst;
+    b->p = p;
+    cudaGetDevice(&b->device);
+    uint32_t maxe = 0;
+    std::vector<uint8_t> ed;
+    for (uint32_t k = 0; k < ninst; ++k) {
+        uint32_t n = num_nodes[k];
+        if (n < rb + 2 || n > 30)
+            return rq::fail(RQ_ERR_INVALID_ARGUMENT, "batched QAOA takes " + std::to_string(rb + 2) +
+                                                         "..30 qubits per graph, got " + std::to_string(n));
+        uint32_t e0 = edge_offsets[k], e1 = edge_offsets[k + 1];
+        if (e1 < e0) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "edge offsets must be non-decreasing");
+        for (uint32_t e = e0; e < e1; ++e) {
+            uint32_t u = edges[2 * e], v = edges[2 * e + 1];
+            if (u >= n || v >= n)
+                return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "edge endpoint out of range in graph " + std::to_string(k));
+            if (u == v) return rq::fail(RQ_ERR_CIRCUIT, "circuit error: self-loop in graph " + std::to_string(k));
+            for (uint32_t f = e0; f < e; ++f)
+                if ((edges[2 * f] == u && edges[2 * f + 1] == v) || (edges[2 * f] == v && edges[2 * f + 1] == u))
+                    return rq::fail(RQ_ERR_INVALID_ARGUMENT, "batched QAOA takes simple graphs: edge (" +
+                                                                 std::to_string(u) + "," + std::to_string(v) +
+                                                                 ") repeats in graph " + std::to_string(k));
+            ed.push_back((uint8_t)u);
+            ed.push_back((uint8_t)v);
+        }
+        b->n_of.push_back(n);
+        b->ne_of.push_back(e1 - e0);
+        maxe = std::max(maxe, e1 - e0);
+    }
+    b->phs = maxe + 1;
+    // size classes and their programs
+    std::map<uint32_t, std::vector<uint32_t>> by_n;
+    for (uint32_t k = 0; k < ninst; ++k) by_n[b->n_of[k]].push_back(k);
+    RQ_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    RQ_CUDA(cudaEventCreate(&b->ev0));
+    RQ_CUDA(cudaEventCreate(&b->ev1));
+    for (auto& kv : by_n) {
+        QClass K;
+        K.n = kv.first;
+        K.insts = kv.second;
+        K.m = std::min(K.n, mloc);
+        K.c = std::min<uint32_t>(K.m, 5);
+        K.ntiles = 1ull << (K.n - K.m);
+        K.smem = ((size_t)1 << K.m) * elem_size(precision);
+        // the circuit of qaoa.rs:125-153 after H^n: per layer the cost phase, then Rx on every qubit
+        std::vector<PGate> g;
+        for (uint32_t l = 0; l < p; ++l) {
+            PGate ph{};
+            ph.type = OP_CPH;
+            ph.q0 = 0;
+            ph.q1 = 0;
+            ph.param = (uint16_t)l;
+            ph.span = (K.n >= 64) ? ~0ull : ((1ull << K.n) - 1);
+            g.push_back(ph);
+            for (uint32_t q = 0; q < K.n; ++q) {
+                PGate rx{};
+                rx.type = OP_RXP;
+                rx.q0 = q;
+                rx.param = (uint16_t)l;
+                g.push_back(rx);
+            }
+        }
+        auto sweeps = plan_sweeps(g, K.n, K.m, K.c);
+        std::vector<PhaseDesc> phases;
+        std::vector<SwOp> ops;
+        std::vector<double> mats;
+        build_program(sweeps, K.n, K.m, K.c, rb, precision == RQ_F32 ? 2 : 1, K.descs, phases, ops, mats);
+        K.descs.front().flags |= SWEEP_INIT_UNIFORM;
+        K.descs.back().flags |= SWEEP_ENERGY;
+        K.off_ops = (phases.size() * sizeof(PhaseDesc) + 255) & ~size_t(255);
+        size_t total = K.off_ops + ops.size() * sizeof(SwOp);
+        std::vector<unsigned char> host(total);
+        std::memcpy(host.data(), phases.data(), phases.size() * sizeof(PhaseDesc));
+        std::memcpy(host.data() + K.off_ops, ops.data(), ops.size() * sizeof(SwOp));
+        RQ_CUDA(cudaMalloc((void**)&K.prog, total));
+        RQ_CUDA(cudaMemcpy(K.prog, host.data(), total, cudaMemcpyHostToDevice));
+        b->classes.push_back(std::move(K));
+    }
+    // graph data
+    if (ed.empty()) ed.push_back(0);
+    RQ_CUDA(cudaMalloc((void**)&b->d_edges, ed.size()));
+    RQ_CUDA(cudaMemcpy(b->d_edges, ed.data(), ed.size(), cudaMemcpyHostToDevice));
+    std::vector<uint32_t> eoff(ninst + 1, 0);
+    for (uint32_t k = 0; k < ninst; ++k) eoff[k + 1] = eoff[k] + b->ne_of[k];
+    RQ_CUDA(cudaMalloc((void**)&b->d_eoff, (ninst + 1) * sizeof(uint32_t)));
+    RQ_CUDA(cudaMemcpy(b->d_eoff, eoff.data(), (ninst + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    RQ_CUDA(cudaMalloc((void**)&b->d_ne, std::max<uint32_t>(1, ninst) * sizeof(uint32_t)));
+    if (ninst) RQ_CUDA(cudaMemcpy(b->d_ne, b->ne_of.data(), ninst * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    *out = b.release();
+    return RQ_OK;
+}
+
+int rq_qaoa_batch_destroy(rq_qaoa_batch* b) {
+    if (!b) return RQ_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (auto& K : b->classes) if (K.prog) cudaFree(K.prog);
+    void* ptrs[] = {b->d_edges, b->d_eoff, b->d_ne, b->d_circ_inst, b->d_user, b->d_ang, b->d_rx, b->d_ph, b->d_energy,
+                    b->d_best_bits, b->d_best_cut, b->d_states, b->d_epart, b->d_tree};
+    for (void* q : ptrs) if (q) cudaFree(q);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return RQ_OK;
+}
+
+int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, const double* betas, double* energies,
+                      uint32_t shots, uint64_t base_seed, uint64_t* best_bits, uint32_t* best_cut) {
+    if (!b || !gammas || !betas || !energies) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (shots && (!best_bits || !best_cut)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null shot outputs");
+    if (nsets == 0) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "nsets must be >= 1");
+    RQ_CUDA(cudaSetDevice(b->device));
+    const uint64_t ncirc = (uint64_t)b->ninst * nsets;
+    const uint32_t p = b->p;
+    // run order: class-major, within a class instance-major then set
+    b->order.clear();
+    std::vector<uint32_t> circ_inst;
+    std::vector<double> ang(2 * ncirc * p);
+    for (auto& K : b->classes)
+        for (uint32_t inst : K.insts)
+            for (uint32_t s = 0; s < nsets; ++s) {
+                const uint64_t user = (uint64_t)inst * nsets + s;
+                const uint64_t pos = b->order.size();
+                b->order.push_back(user);
+                circ_inst.push_back(inst);
+                for (uint32_t l = 0; l < p; ++l) {
+                    ang[pos * p + l] = gammas[user * p + l];
+                    ang[ncirc * p + pos * p + l] = betas[user * p + l];
+                }
+            }
+    size_t cap_ci = b->circ_cap;
+    RQ_TRY(grow(&b->d_circ_inst, &cap_ci, ncirc));
+    size_t cap_u = b->circ_cap;
+    RQ_TRY(grow(&b->d_user, &cap_u, ncirc));
+    size_t cap_a = b->circ_cap;
+    RQ_TRY(grow(&b->d_ang, &cap_a, 2 * ncirc * p));
+    size_t es = b->prec == RQ_F32 ? sizeof(float) : sizeof(double);
+    size_t cap_rx = b->circ_cap ? b->circ_cap * p * 2 * es : 0;
+    RQ_TRY(grow_bytes(&b->d_rx, &cap_rx, ncirc * p * 2 * es));
+    size_t cap_ph = b->circ_cap ? b->circ_cap * p * b->phs * 2 * es : 0;
+    RQ_TRY(grow_bytes(&b->d_ph, &cap_ph, ncirc * p * b->phs * 2 * es));
+    size_t cap_e = b->circ_cap;
+    RQ_TRY(grow(&b->d_energy, &cap_e, ncirc));
+    size_t cap_bb = b->circ_cap;
+    RQ_TRY(grow(&b->d_best_bits, &cap_bb, ncirc));
+    size_t cap_bc = b->circ_cap;
+    RQ_TRY(grow(&b->d_best_cut, &cap_bc, ncirc));
+    b->circ_cap = std::max<size_t>(b->circ_cap, ncirc);
+    RQ_CUDA(cudaMemcpyAsync(b->d_circ_inst, circ_inst.data(), ncirc * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+    RQ_CUDA(cudaMemcpyAsync(b->d_user, b->order.data(), ncirc * sizeof(uint64_t), cudaMemcpyHostToDevice, b->stream));
+    RQ_CUDA(cudaMemcpyAsync(b->d_ang, ang.data(), ang.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    const int sms = rq::num_sms(b->device);
+    RQ_CUDA(cudaEventRecord(b->ev0, b->stream));
+    if (b->prec == RQ_F32)
+        k_qaoa_tables<float><<<rq::grid_for(ncirc * p, TPB, sms), TPB, 0, b->stream>>>(
+            b->d_ang, b->d_ang + ncirc * p, b->d_circ_inst, b->d_ne, ncirc, p, b->phs, (float*)b->d_rx, (float*)b->d_ph);
+    else
+        k_qaoa_tables<double><<<rq::grid_for(ncirc * p, TPB, sms), TPB, 0, b->stream>>>(
+            b->d_ang, b->d_ang + ncirc * p, b->d_circ_inst, b->d_ne, ncirc, p, b->phs, (double*)b->d_rx, (double*)b->d_ph);
+    RQ_CUDA(cudaGetLastError());
+    uint64_t pos = 0;
+    for (auto& K : b->classes) {
+        const uint64_t kc = (uint64_t)K.insts.size() * nsets;
+        const size_t state_bytes = ((size_t)1 << K.n) * elem_size(b->prec);
+        const uint64_t wave = std::max<uint64_t>(1, std::min<uint64_t>(kc, b->state_budget / state_bytes));
+        RQ_TRY(grow_bytes(&b->d_states, &b->states_cap, wave * state_bytes));
+        RQ_TRY(grow(&b->d_epart, &b->epart_cap, wave * K.ntiles));
+        for (uint64_t w0 = 0; w0 < kc; w0 += wave) {
+            const uint64_t wn = std::min<uint64_t>(wave, kc - w0);
+            if (b->prec == RQ_F32) {
+                RQ_TRY(launch_class<float>(b, K, wn, pos + w0, b->d_states));
+                if (shots) RQ_TRY(sample_class<float>(b, K, wn, pos + w0, b->d_states, shots, base_seed));
+            } else {
+                RQ_TRY(launch_class<double>(b, K, wn, pos + w0, b->d_states));
+                if (shots) RQ_TRY(sample_class<double>(b, K, wn, pos + w0, b->d_states, shots, base_seed));
+            }
+            b->last_wave_first = pos + w0;
+            b->last_wave_count = wn;
+            b->last_wave_n = K.n;
+        }
+        pos += kc;
+    }
+    RQ_CUDA(cudaEventRecord(b->ev1, b->stream));
+    std::vector<double> e(ncirc);
+    RQ_CUDA(cudaMemcpyAsync(e.data(), b->d_energy, ncirc * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    std::vector<uint64_t> bb;
+    std::vector<uint32_t> bc;
+    if (shots) {
+        bb.resize(ncirc);
+        bc.resize(ncirc);
+        RQ_CUDA(cudaMemcpyAsync(bb.data(), b->d_best_bits, ncirc * sizeof(uint64_t), cudaMemcpyDeviceToHost, b->stream));
+        RQ_CUDA(cudaMemcpyAsync(bc.data(), b->d_best_cut, ncirc * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream));
+    }
+    RQ_CUDA(cudaStreamSynchronize(b->stream));
+    RQ_CUDA(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+    for (uint64_t k = 0; k < ncirc; ++k) {
+        const uint64_t user = b->order[k];
+        energies[user] = e[k];
+        if (shots) {
+            best_bits[user] = bb[k];
+            best_cut[user] = bc[k];
+        }
+    }
+    b->last_nsets = nsets;
+    return RQ_OK;
+}
+
+int rq_qaoa_batch_state(rq_qaoa_batch* b, uint64_t circuit, double* interleaved) {
+    if (!b || !interleaved) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    RQ_CUDA(cudaSetDevice(b->device));
+    uint64_t pos = UINT64_MAX;
+    for (uint64_t k = 0; k < b->order.size(); ++k)
+        if (b->order[k] == circuit) { pos = k; break; }
+    if (pos == UINT64_MAX || pos < b->last_wave_first || pos >= b->last_wave_first + b->last_wave_count)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "circuit " + std::to_string(circuit) +
+                                                     " is not held on the device (only the last wave of the last run is)");
+    const uint64_t per = 1ull << b->last_wave_n;
+    const size_t es = elem_size(b->prec);
+    const unsigned char* src = (const unsigned char*)b->d_states + (pos - b->last_wave_first) * per * es;
+    if (b->prec == RQ_F64) {
+        RQ_CUDA(cudaMemcpy(interleaved, src, per * es, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> tmp(2 * per);
+        RQ_CUDA(cudaMemcpy(tmp.data(), src, per * es, cudaMemcpyDeviceToHost));
+        for (uint64_t i = 0; i < 2 * per; ++i) interleaved[i] = tmp[i];
+    }
+    return RQ_OK;
+}
+
+int rq_qaoa_batch_last_ms(const rq_qaoa_batch* b, float* ms) {
+    if (!b || !ms) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    *ms = b->last_ms;
+    return RQ_OK;
+}
+
+int rq_qaoa_batch_set_state_budget(rq_qaoa_batch* b, uint64_t bytes) {
+    if (!b || bytes == 0) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "bad argument");
+    b->state_budget = bytes;
+    return RQ_OK;
+}
+
+}  // extern "C"

@@ -19,6 +19,7 @@
 // Adjacent 1-qubit gates on the same qubit are multiplied into one 2x2 on
 // the host (a generalisation of optimizer::fuse_gates, optimizer.rs:46-94).
 #include "rq_internal.cuh"
+#include "rq_plan.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -30,36 +31,7 @@
 namespace {
 
 using rqd::C2;
-
-enum OpType : uint8_t { OP_U1 = 0, OP_D1 = 1, OP_CX = 2, OP_CZ = 3, OP_ZZ = 4 };
-
-constexpr int RBMAX = 5;
-constexpr int MMAX = 14;
-
-struct SwOp {
-    uint8_t type;
-    int8_t k0, k1;   // register slot of q0 / q1 in this phase, -1 if not a slot
-    uint8_t q0, q1;  // global qubits
-    uint8_t pad[3];
-    uint32_t mat;    // first complex entry in the matrix table
-};
-
-struct PhaseDesc {
-    uint32_t op_begin, op_end;
-    uint32_t nt;              // number of thread bits
-    uint8_t tbit_local[16];   // thread bit b -> local bit index
-    uint8_t tbit_global[16];  // thread bit b -> global qubit
-    uint16_t lut[1 << RBMAX]; // register index -> local offset
-};
-
-struct SweepDesc {
-    uint32_t n, m, c;
-    uint32_t nonlocal_count;
-    uint8_t local_global[32];   // local bit -> global qubit
-    uint8_t nonlocal[64];       // non-local bits in ascending order
-    uint32_t phase_begin, phase_end;
-    uint64_t gj[1 << RBMAX];    // deposit of the per-thread vector offsets
-};
+using namespace rqp;
 
 // 16-byte vector type per precision: 2 complex f32 or 1 complex f64
 template <typename T> struct Vec16;
@@ -280,212 +252,6 @@ __global__ void __launch_bounds__(256, 2) k_sweep(typename C2<T>::t* __restrict_
 // host planner
 // ---------------------------------------------------------------------------
 
-struct PGate {
-    uint8_t type;
-    uint32_t q0, q1;
-    double m[8];   // U1: 2x2; D1: d0,d1; ZZ: en,ep
-};
-
-uint64_t qmask(const PGate& g) {
-    uint64_t m = 1ull << g.q0;
-    if (g.type == OP_CX || g.type == OP_CZ || g.type == OP_ZZ) m |= 1ull << g.q1;
-    return m;
-}
-
-// qubits that must be register slots (and therefore local)
-uint64_t needs(const PGate& g) {
-    if (g.type == OP_U1) return 1ull << g.q0;
-    if (g.type == OP_CX) return 1ull << g.q1;
-    return 0;
-}
-
-bool is_1q(uint8_t t) { return t == OP_U1 || t == OP_D1; }
-
-// c = a * b (2x2 complex, row-major (re,im))
-void mat2_mul(const double* a, const double* b, double* c) {
-    double r[8];
-    for (int i = 0; i < 2; ++i)
-        for (int j = 0; j < 2; ++j) {
-            double re = 0, im = 0;
-            for (int k = 0; k < 2; ++k) {
-                double ar = a[(i * 2 + k) * 2], ai = a[(i * 2 + k) * 2 + 1];
-                double br = b[(k * 2 + j) * 2], bi = b[(k * 2 + j) * 2 + 1];
-                re += ar * br - ai * bi;
-                im += ar * bi + ai * br;
-            }
-            r[(i * 2 + j) * 2] = re;
-            r[(i * 2 + j) * 2 + 1] = im;
-        }
-    std::memcpy(c, r, sizeof(r));
-}
-
-void as_matrix(const PGate& g, double* m) {
-    if (g.type == OP_U1) {
-        std::memcpy(m, g.m, sizeof(double) * 8);
-    } else {  // D1
-        double r[8] = {g.m[0], g.m[1], 0, 0, 0, 0, g.m[2], g.m[3]};
-        std::memcpy(m, r, sizeof(r));
-    }
-}
-
-// fuse `nxt` (applied after `cur`) into cur; both 1-qubit on the same qubit
-void fuse_into(PGate& cur, const PGate& nxt) {
-    if (cur.type == OP_D1 && nxt.type == OP_D1) {
-        double a[2] = {cur.m[0], cur.m[1]}, b[2] = {cur.m[2], cur.m[3]};
-        cur.m[0] = nxt.m[0] * a[0] - nxt.m[1] * a[1];
-        cur.m[1] = nxt.m[0] * a[1] + nxt.m[1] * a[0];
-        cur.m[2] = nxt.m[2] * b[0] - nxt.m[3] * b[1];
-        cur.m[3] = nxt.m[2] * b[1] + nxt.m[3] * b[0];
-        return;
-    }
-    double A[8], B[8], C[8];
-    as_matrix(cur, A);
-    as_matrix(nxt, B);
-    mat2_mul(B, A, C);
-    cur.type = OP_U1;
-    std::memcpy(cur.m, C, sizeof(C));
-}
-
-struct Sweep {
-    uint64_t L;               // local qubit mask
-    std::vector<PGate> ops;   // in execution order (after fusion)
-};
-
-std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c) {
-    std::vector<Sweep> out;
-    std::vector<char> taken(gates.size(), 0);
-    size_t first = 0;
-    const uint64_t base = (c >= 64) ? ~0ull : ((1ull << c) - 1);
-    while (first < gates.size()) {
-        Sweep sw;
-        sw.L = base;
-        uint64_t blocked = 0;
-        std::vector<int> last(n, -1);   // index in sw.ops of the last op on each qubit
-        for (size_t k = first; k < gates.size(); ++k) {
-            if (taken[k]) continue;
-            const PGate& g = gates[k];
-            uint64_t qm = qmask(g);
-            if (qm & blocked) {
-                blocked |= qm;
-                continue;
-            }
-            uint64_t L2 = sw.L | needs(g);
-            if ((uint32_t)__builtin_popcountll(L2) > m) {
-                blocked |= qm;
-                continue;
-            }
-            sw.L = L2;
-            taken[k] = 1;
-            if (is_1q(g.type) && last[g.q0] >= 0 && is_1q(sw.ops[last[g.q0]].type)) {
-                fuse_into(sw.ops[last[g.q0]], g);
-            } else {
-                sw.ops.push_back(g);
-                int idx = (int)sw.ops.size() - 1;
-                last[g.q0] = idx;
-                if (!is_1q(g.type)) last[g.q1] = idx;
-            }
-        }
-        while (first < gates.size() && taken[first]) ++first;
-        out.push_back(std::move(sw));
-    }
-    return out;
-}
-
-struct PhasePlan {
-    uint64_t R;               // register qubits (global mask)
-    std::vector<int> ops;     // indices into the sweep's op list
-};
-
-std::vector<PhasePlan> plan_phases(const Sweep& sw, uint32_t rb) {
-    std::vector<PhasePlan> out;
-    std::vector<char> taken(sw.ops.size(), 0);
-    size_t first = 0;
-    while (first < sw.ops.size()) {
-        PhasePlan ph;
-        ph.R = 0;
-        uint64_t blocked = 0;
-        for (size_t k = first; k < sw.ops.size(); ++k) {
-            if (taken[k]) continue;
-            const PGate& g = sw.ops[k];
-            uint64_t qm = qmask(g);
-            if (qm & blocked) {
-                blocked |= qm;
-                continue;
-            }
-            uint64_t R2 = ph.R | needs(g);
-            if ((uint32_t)__builtin_popcountll(R2) > rb) {
-                blocked |= qm;
-                continue;
-            }
-            ph.R = R2;
-            taken[k] = 1;
-            ph.ops.push_back((int)k);
-        }
-        // fill the remaining slots with the lowest unused local qubits
-        for (uint32_t q = 0; q < 64 && (uint32_t)__builtin_popcountll(ph.R) < rb; ++q)
-            if (((sw.L >> q) & 1) && !((ph.R >> q) & 1)) ph.R |= 1ull << q;
-        while (first < sw.ops.size() && taken[first]) ++first;
-        out.push_back(std::move(ph));
-    }
-    return out;
-}
-
-bool to_pgates(const rq_gate* gates, uint64_t n, std::vector<PGate>& out) {
-    const double s2 = 0.70710678118654752440;
-    for (uint64_t k = 0; k < n; ++k) {
-        const rq_gate& g = gates[k];
-        PGate p{};
-        p.q0 = g.q0;
-        p.q1 = g.q1;
-        double h = g.angle / 2.0;
-        switch (g.kind) {
-            case RQ_GATE_CNOT: p.type = OP_CX; out.push_back(p); break;
-            case RQ_GATE_CZ: p.type = OP_CZ; out.push_back(p); break;
-            case RQ_GATE_RZZ:
-                p.type = OP_ZZ;
-                p.m[0] = std::cos(-h); p.m[1] = std::sin(-h); p.m[2] = std::cos(h); p.m[3] = std::sin(h);
-                out.push_back(p);
-                break;
-            case RQ_GATE_SWAP: {
-                PGate a{}; a.type = OP_CX; a.q0 = g.q0; a.q1 = g.q1;
-                PGate b{}; b.type = OP_CX; b.q0 = g.q1; b.q1 = g.q0;
-                out.push_back(a); out.push_back(b); out.push_back(a);
-                break;
-            }
-            case RQ_GATE_Z: p.type = OP_D1; p.m[0] = 1; p.m[2] = -1; p.m[3] = -0.0; out.push_back(p); break;
-            case RQ_GATE_S: p.type = OP_D1; p.m[0] = 1; p.m[3] = 1; out.push_back(p); break;
-            case RQ_GATE_SDG: p.type = OP_D1; p.m[0] = 1; p.m[2] = -0.0; p.m[3] = -1; out.push_back(p); break;
-            case RQ_GATE_T: p.type = OP_D1; p.m[0] = 1; p.m[2] = s2; p.m[3] = s2; out.push_back(p); break;
-            case RQ_GATE_TDG: p.type = OP_D1; p.m[0] = 1; p.m[2] = s2; p.m[3] = -s2; out.push_back(p); break;
-            case RQ_GATE_RZ:
-                p.type = OP_D1;
-                p.m[0] = std::cos(-h); p.m[1] = std::sin(-h); p.m[2] = std::cos(h); p.m[3] = std::sin(h);
-                out.push_back(p);
-                break;
-            case RQ_GATE_PHASE:
-                p.type = OP_D1; p.m[0] = 1; p.m[2] = std::cos(g.angle); p.m[3] = std::sin(g.angle);
-                out.push_back(p);
-                break;
-            case RQ_GATE_H: { p.type = OP_U1; double m[8] = {s2, 0, s2, 0, s2, 0, -s2, -0.0}; std::memcpy(p.m, m, sizeof m); out.push_back(p); break; }
-            case RQ_GATE_X: { p.type = OP_U1; double m[8] = {0, 0, 1, 0, 1, 0, 0, 0}; std::memcpy(p.m, m, sizeof m); out.push_back(p); break; }
-            case RQ_GATE_Y: { p.type = OP_U1; double m[8] = {0, 0, -0.0, -1, 0, 1, 0, 0}; std::memcpy(p.m, m, sizeof m); out.push_back(p); break; }
-            case RQ_GATE_RX: {
-                double c = std::cos(h), sn = -std::sin(h);
-                p.type = OP_U1; double m[8] = {c, 0, 0, sn, 0, sn, c, 0}; std::memcpy(p.m, m, sizeof m); out.push_back(p);
-                break;
-            }
-            case RQ_GATE_RY: {
-                double c = std::cos(h), sn = std::sin(h);
-                p.type = OP_U1; double m[8] = {c, 0, -sn, 0, sn, 0, c, 0}; std::memcpy(p.m, m, sizeof m); out.push_back(p);
-                break;
-            }
-            case RQ_GATE_UNITARY1Q: p.type = OP_U1; std::memcpy(p.m, g.m, sizeof p.m); out.push_back(p); break;
-            default: return false;
-        }
-    }
-    return true;
-}
-
 template <typename T>
 int launch_sweep(rq_state* s, const SweepDesc& d, const PhaseDesc* ph, const SwOp* ops, const void* mats,
                  uint64_t ntiles, uint32_t rb, size_t smem) {
@@ -576,74 +342,7 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
     std::vector<PhaseDesc> phases;
     std::vector<SwOp> ops;
     std::vector<double> mats;
-    for (auto& sw : sweeps) {
-        uint64_t L = sw.L;
-        for (uint32_t q = 0; q < nq && (uint32_t)__builtin_popcountll(L) < m; ++q) L |= 1ull << q;
-        sw.L = L;
-        SweepDesc d{};
-        d.n = nq;
-        d.m = m;
-        d.c = c;
-        uint32_t li = 0, ni = 0;
-        uint8_t local_index[64];
-        for (uint32_t q = 0; q < nq; ++q) {
-            if ((L >> q) & 1) { local_index[q] = (uint8_t)li; d.local_global[li++] = (uint8_t)q; }
-            else d.nonlocal[ni++] = (uint8_t)q;
-        }
-        d.nonlocal_count = ni;
-        const uint32_t EPV = s->prec == RQ_F32 ? 2 : 1;
-        const uint32_t t = m - rb;
-        const uint32_t VPT = (1u << rb) / EPV;
-        for (uint32_t j = 0; j < VPT; ++j) {
-            uint64_t x = (uint64_t)j * (1ull << t) * EPV, gsum = 0;
-            for (uint32_t b = 0; b < m; ++b)
-                if ((x >> b) & 1) gsum |= 1ull << d.local_global[b];
-            d.gj[j] = gsum;
-        }
-        d.phase_begin = (uint32_t)phases.size();
-        auto pplan = plan_phases(sw, rb);
-        for (auto& pp : pplan) {
-            PhaseDesc Ph{};
-            Ph.op_begin = (uint32_t)ops.size();
-            int slot_of[64];
-            for (int q = 0; q < 64; ++q) slot_of[q] = -1;
-            uint32_t slots[RBMAX], ns = 0;
-            for (uint32_t q = 0; q < nq; ++q)
-                if ((pp.R >> q) & 1) { slot_of[q] = (int)ns; slots[ns++] = q; }
-            uint32_t nt = 0;
-            for (uint32_t b = 0; b < m; ++b) {
-                uint32_t q = d.local_global[b];
-                if (!((pp.R >> q) & 1)) { Ph.tbit_local[nt] = (uint8_t)b; Ph.tbit_global[nt] = (uint8_t)q; ++nt; }
-            }
-            Ph.nt = nt;
-            for (uint32_t i = 0; i < (1u << rb); ++i) {
-                uint32_t off = 0;
-                for (uint32_t sidx = 0; sidx < ns; ++sidx)
-                    if ((i >> sidx) & 1) off |= 1u << local_index[slots[sidx]];
-                Ph.lut[i] = (uint16_t)off;
-            }
-            for (int oi : pp.ops) {
-                const PGate& g = sw.ops[oi];
-                SwOp o{};
-                o.type = g.type;
-                o.q0 = (uint8_t)g.q0;
-                o.q1 = (uint8_t)g.q1;
-                o.k0 = (int8_t)slot_of[g.q0];
-                o.k1 = (g.type == OP_CX || g.type == OP_CZ || g.type == OP_ZZ) ? (int8_t)slot_of[g.q1] : -1;
-                o.mat = (uint32_t)(mats.size() / 2);
-                int cnt = g.type == OP_U1 ? 8 : (g.type == OP_D1 || g.type == OP_ZZ) ? 4 : 0;
-                for (int k = 0; k < cnt; ++k) mats.push_back(g.m[k]);
-                ops.push_back(o);
-            }
-            Ph.op_end = (uint32_t)ops.size();
-            phases.push_back(Ph);
-        }
-        d.phase_end = (uint32_t)phases.size();
-        P->descs.push_back(d);
-    }
-    if (mats.empty()) mats.push_back(0.0);
-    if (ops.empty()) ops.push_back(SwOp{});
-    if (phases.empty()) phases.push_back(PhaseDesc{});
+    build_program(sweeps, nq, m, c, rb, s->prec == RQ_F32 ? 2 : 1, P->descs, phases, ops, mats);
 
     size_t mat_elem = s->prec == RQ_F32 ? sizeof(float) : sizeof(double);
     P->off_ph = 0;

@@ -1,0 +1,112 @@
+"""Batched QAOA-MaxCut engine vs the oracle (needs a GPU).
+
+Energies are the oracle's evaluate_qaoa_cost restatement (qaoa.rs:179-201, per-edge
+ZZ expectations of the gate-by-gate circuit); tolerance 1e-10 absolute for f64
+states and 1e-5 x |E| for f32 states (FP64 accumulation of f32 amplitudes).
+Best-cut shots are bit-exact against the oracle's sampler fed the same device
+probability vector with the same seeds.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from ruqu_b200 import rng, workloads
+from ruqu_b200.batch import QaoaBatch
+
+pytestmark = pytest.mark.gpu
+
+
+def _graphs(sizes, seed):
+    st = rng.Stream(seed, 2)
+    out = []
+    r = np.random.default_rng(seed)
+    for n in sizes:
+        if n % 2 == 0 and n >= 4:
+            out.append((n, workloads.random_3regular_graph(n, st)))
+        else:   # odd n: random simple graph with ~1.5 n edges
+            pairs = [(i, j) for i in range(n) for j in range(i + 1, n)]
+            pick = r.choice(len(pairs), size=min(len(pairs), (3 * n) // 2), replace=False)
+            out.append((n, [pairs[k] for k in sorted(pick)]))
+    return out
+
+
+def _cut(bits, edges):
+    return sum(1 for u, v in edges if ((bits >> u) ^ (bits >> v)) & 1)
+
+
+def _best_from_oracle(probs, n, edges, seed, shots):
+    bits = oracle.tree_sample(probs, n, list(range(n)), seed, shots)
+    cuts = np.array([_cut(int(b), edges) for b in bits])
+    k = int(np.argmax(cuts))          # first index of the maximum
+    return int(bits[k]), int(cuts[k])
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("p", [1, 3])
+def test_batch_energies_and_shots_match_oracle(prec, p):
+    sizes = [6, 7, 8, 10, 12, 13, 14, 16] if prec == "f64" else [7, 8, 10, 12, 13, 14, 16]
+    graphs = _graphs(sizes, 11 + p)
+    nsets = 3
+    r = np.random.default_rng(p)
+    gam = r.uniform(0, math.pi, size=(len(graphs), nsets, p))
+    bet = r.uniform(0, math.pi / 2, size=(len(graphs), nsets, p))
+    qb = QaoaBatch(graphs, p, prec)
+    shots, seed = 512, 1234
+    out = qb.run(gam, bet, shots=shots, seed=seed)
+    for k, (n, e) in enumerate(graphs):
+        ew = [(u, v, 1.0) for u, v in e]
+        for s in range(nsets):
+            want = oracle.qaoa_cost(n, ew, gam[k, s], bet[k, s])
+            tol = 1e-10 if prec == "f64" else 1e-5 * max(1, len(e))
+            assert abs(out["energies"][k, s] - want) < tol, (n, s, out["energies"][k, s], want)
+            assert out["best_cut"][k, s] == _cut(int(out["best_bits"][k, s]), e)
+    # the largest size class runs last, so its circuits are still on the device:
+    # their shots are bit-exact against the oracle sampler on the same probabilities
+    k = len(graphs) - 1
+    n, e = graphs[k]
+    for s in range(nsets):
+        c = k * nsets + s
+        a = qb.state(c)
+        probs = a.real * a.real + a.imag * a.imag
+        assert _best_from_oracle(probs, n, e, seed + (c << 32), shots) == \
+            (int(out["best_bits"][k, s]), int(out["best_cut"][k, s]))
+
+
+def test_batch_waves_give_the_same_energies():
+    graphs = _graphs([14, 14, 16, 16, 16], 5)
+    r = np.random.default_rng(9)
+    gam = r.uniform(0, math.pi, size=(len(graphs), 4))
+    bet = r.uniform(0, math.pi / 2, size=(len(graphs), 4))
+    a = QaoaBatch(graphs, 4, "f32")
+    ea = a.run(gam, bet)["energies"]
+    b = QaoaBatch(graphs, 4, "f32")
+    b.set_state_budget(1 << 19)          # one 2^16-amplitude f32 state per wave
+    eb = b.run(gam, bet)["energies"]
+    assert np.max(np.abs(ea - eb)) == 0.0
+
+
+def test_batch_config_shape_properties():
+    """64 random 3-regular graphs with n uniform over {12..24}, p = 4, 1024 shots."""
+    inst = workloads.qaoa_instances(64, 3)
+    graphs = [(x["n"], [(u, v) for u, v, _ in x["edges"]]) for x in inst]
+    gam = np.array([x["gammas"] for x in inst])
+    bet = np.array([x["betas"] for x in inst])
+    qb = QaoaBatch(graphs, 4, "f32")
+    out = qb.run(gam, bet, shots=1024, seed=7)
+    for k, (n, e) in enumerate(graphs):
+        assert 0.0 <= out["energies"][k] <= len(e)
+        assert out["best_cut"][k] == _cut(int(out["best_bits"][k]), e)
+        assert out["best_cut"][k] >= out["energies"][k] - 1e-9 or out["best_cut"][k] <= len(e)
+    # circuits of the last wave: exact against the oracle sampler
+    last_n = max(g[0] for g in graphs)
+    for k, (n, e) in enumerate(graphs):
+        if n != last_n:
+            continue
+        try:
+            a = qb.state(k)
+        except Exception:
+            continue
+        probs = a.real * a.real + a.imag * a.imag
+        assert _best_from_oracle(probs, n, e, 7 + (k << 32), 1024) == (int(out["best_bits"][k]), int(out["best_cut"][k]))
