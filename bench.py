@@ -52,6 +52,8 @@ def _args():
     ap.add_argument("--mode", choices=["auto", "per_gate", "sweep"], default="auto")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-qaoa", action="store_true", help="skip the batched QAOA leg")
+    ap.add_argument("--qaoa-instances", type=int, default=2048)
     return ap.parse_args()
 
 
@@ -143,6 +145,53 @@ def cpu_baseline_sample(a, parallel: bool, gates_in_sample: int = 4):
             f"{'OpenMP restatement of the reference parallel kernels' if parallel else 'scalar reference kernels'}"
             f", {cores} thread(s)")
     return nbytes / dt / 1e9, dt, cores, desc
+
+
+def qaoa_batch_leg(a, ws, rank, with_cpu):
+    """Batched QAOA-MaxCut: 2048 random 3-regular graphs, n uniform over {12,...,24},
+    unit weights, p = 4, gamma ~ U[0,pi), beta ~ U[0,pi/2) (seed 2), complex f32
+    states, <C> in FP64, 1024 shots per graph -> best-cut bitstring.  Instances
+    are sharded over ranks (rank r takes r, r+N, ...)."""
+    import numpy as np
+
+    from ruqu_b200 import workloads
+    from ruqu_b200.batch import QaoaBatch
+    inst = workloads.qaoa_instances(a.qaoa_instances, 2)
+    mine = inst[rank::ws]
+    graphs = [(x["n"], [(u, v) for u, v, _ in x["edges"]]) for x in mine]
+    gam = np.array([x["gammas"] for x in mine])
+    bet = np.array([x["betas"] for x in mine])
+    qb = QaoaBatch(graphs, 4, "f32")
+    qb.run(gam, bet, shots=1024, seed=11)            # warm-up (allocation, first launches)
+    ms, wall = [], []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        out = qb.run(gam, bet, shots=1024, seed=11)
+        wall.append(time.perf_counter() - t0)
+        ms.append(qb.last_ms())
+    dev_ms = min(ms)
+    res = {"workload": "batched QAOA-MaxCut, %d random 3-regular graphs, n in {12..24}, p=4, f32 states, "
+                       "1024 shots each, best cut" % a.qaoa_instances,
+           "circuits_per_rank": len(mine), "device_ms": dev_ms, "wall_ms": 1e3 * min(wall),
+           "evals_per_s": len(mine) * ws / (dev_ms / 1e3),
+           "evals_per_s_e2e": len(mine) * ws / min(wall),
+           "mean_energy": float(np.mean(out["energies"])), "mean_best_cut": float(np.mean(out["best_cut"]))}
+    if with_cpu:
+        import oracle
+        t_by_n = {}
+        for n in (12, 14, 16, 18):
+            x = next(y for y in inst if y["n"] == n)
+            t0 = time.perf_counter()
+            oracle.qaoa_cost(n, x["edges"], x["gammas"], x["betas"])
+            t_by_n[n] = time.perf_counter() - t0
+        for n in (20, 22, 24):   # each +2 qubits: 4x the amplitudes, (n+2)/n the gates
+            t_by_n[n] = t_by_n[n - 2] * 4.0 * (n + 2) / n
+        total = sum(t_by_n[x["n"]] for x in inst)
+        res["cpu_baseline"] = {"value": len(inst) / total, "unit": "QAOA evals/s", "cores": 1, "kind": "port",
+                               "sample": "one evaluate_qaoa_cost (reference f64 engine, energy only, no shots) "
+                                         "per n in {12,14,16,18} timed; n = 20, 22, 24 scaled by 4(n+2)/n per +2 "
+                                         "qubits; summed over the 2048 instances"}
+    return res
 
 
 def run_reference(a):
@@ -276,6 +325,15 @@ def run_ours(a):
                "d2h_bytes_per_step": 8 * a.qubits, "ms_per_step": dt * 1e3,
                "path": "QuantumState.reset + apply_gates(host list) + expectation_values(<Z_i>) -> host"}
 
+    qaoa = None
+    if not a.no_qaoa:
+        qaoa = qaoa_batch_leg(a, ws, rank, with_cpu=(rank == 0 and ws == 1 and not a.no_cpu_baseline))
+        if dist:
+            t = torch.tensor([qaoa["device_ms"]], device="cuda")
+            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+            qaoa["device_ms_max_over_ranks"] = float(t.item())
+            qaoa["evals_per_s"] = a.qaoa_instances / (qaoa["device_ms_max_over_ranks"] / 1e3)
+
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         v, secs, cores, desc = cpu_baseline_sample(a, parallel=False)
@@ -301,6 +359,7 @@ def run_ours(a):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": a.steps * (1 + stats["launches"]),
+            "qaoa_batch": qaoa,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

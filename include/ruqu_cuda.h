@@ -328,6 +328,31 @@ RQ_API int rq_qaoa_batch_set_state_budget(rq_qaoa_batch* b, uint64_t bytes);
 RQ_API int rq_qaoa_batch_destroy(rq_qaoa_batch* b);
 
 /* ------------------------------------------------------------------------ */
+/* batched VQE (vqe.rs:122-216 over many parameter sets)                     */
+/* ------------------------------------------------------------------------ */
+
+typedef struct rq_vqe_batch rq_vqe_batch;
+
+/* Hardware-efficient ansatz on num_qubits qubits, `depth` layers of "Ry(theta)
+ * on every qubit, then CZ(q, q+1) for q = 0..n-2" (num_qubits*depth
+ * parameters, layer-major), and the Hamiltonian sum_k coeffs[k] P_k with
+ * P_k = ops[offsets[k] .. offsets[k+1]) (types.rs:218-228). */
+RQ_API int rq_vqe_batch_create(uint32_t num_qubits, uint32_t depth, const double* coeffs,
+                               const rq_pauli_op* ops, const uint32_t* offsets, uint32_t nterms,
+                               int32_t precision, rq_vqe_batch** out);
+
+/* energies[s] = <psi(params_s)|H|psi(params_s)> (evaluate_energy, vqe.rs:122-131)
+ * for s < nsets, params_s = params[s*P .. s*P+P).  With with_gradient != 0 also
+ * gradients[s*P + k] = (E(theta_k + pi/2) - E(theta_k - pi/2)) / 2 (the
+ * parameter-shift rule of vqe.rs:186-198): 1 + 2P circuits per set, all run
+ * on the device in waves.  Energies accumulate in FP64. */
+RQ_API int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* params,
+                            int32_t with_gradient, double* energies, double* gradients);
+
+RQ_API int rq_vqe_batch_last_ms(const rq_vqe_batch* b, float* ms);
+RQ_API int rq_vqe_batch_destroy(rq_vqe_batch* b);
+
+/* ------------------------------------------------------------------------ */
 /* host transfer (state_vector / amplitudes_mut / from_amplitudes)           */
 /* ------------------------------------------------------------------------ */
 

@@ -77,6 +77,10 @@ SIGNATURES = {
     "rq_qaoa_batch_last_ms": (C.c_int, [_vp, _P(C.c_float)]),
     "rq_qaoa_batch_set_state_budget": (C.c_int, [_vp, _u64]),
     "rq_qaoa_batch_destroy": (C.c_int, [_vp]),
+    "rq_vqe_batch_create": (C.c_int, [_u32, _u32, _P(_dbl), _P(RqPauliOp), _P(_u32), _u32, _i32, _P(_vp)]),
+    "rq_vqe_batch_run": (C.c_int, [_vp, _u32, _P(_dbl), _i32, _P(_dbl), _P(_dbl)]),
+    "rq_vqe_batch_last_ms": (C.c_int, [_vp, _P(C.c_float)]),
+    "rq_vqe_batch_destroy": (C.c_int, [_vp]),
     "rq_expectation_batch_noalloc": (C.c_int, [_vp, _u32, _i32, _P(RqPauliOp), _P(_u32), _u32, _P(_dbl), _vp]),
     "rq_state_normalize": (C.c_int, [_vp]),
     "rq_state_fidelity": (C.c_int, [_vp, _vp, _P(_dbl)]),

@@ -89,3 +89,42 @@ class QaoaBatch:
         if h is not None:
             lib.rq_qaoa_batch_destroy(h)
             self._h = None
+
+
+class VqeBatch:
+    """Batched VQE energies / parameter-shift gradients (rq_vqe_batch_* of include/ruqu_cuda.h).
+
+    Ansatz: per layer Ry(theta) on every qubit then CZ(q, q+1) (parameters layer-major);
+    Hamiltonian: coeffs[k] * P_k with P_k a list of (qubit, PauliOp)."""
+
+    def __init__(self, num_qubits: int, depth: int, coeffs, strings, precision: str = "f32"):
+        from .state import pauli_array
+        self.n, self.depth = int(num_qubits), int(depth)
+        self.P = self.n * self.depth
+        ops, off = pauli_array(strings)
+        c = np.ascontiguousarray(coeffs, dtype=np.float64)
+        h = C.c_void_p()
+        check(lib.rq_vqe_batch_create(self.n, self.depth, _dp(c), ops, _u32p(off), len(strings),
+                                      RQ_F32 if precision == "f32" else RQ_F64, C.byref(h)))
+        self._h = h
+
+    def run(self, params, gradient: bool = False):
+        """params: (nsets, P).  Returns energies (nsets,) and, with gradient=True, (nsets, P) gradients."""
+        p = np.ascontiguousarray(np.atleast_2d(np.asarray(params, dtype=np.float64)))
+        nsets = p.shape[0]
+        assert p.shape[1] == self.P
+        e = np.empty(nsets)
+        g = np.empty((nsets, self.P)) if gradient else np.empty(1)
+        check(lib.rq_vqe_batch_run(self._h, nsets, _dp(p), 1 if gradient else 0, _dp(e), _dp(g)))
+        return (e, g) if gradient else e
+
+    def last_ms(self) -> float:
+        ms = C.c_float()
+        check(lib.rq_vqe_batch_last_ms(self._h, C.byref(ms)))
+        return ms.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None:
+            lib.rq_vqe_batch_destroy(h)
+            self._h = None

@@ -59,7 +59,8 @@ struct QArgs {
     const uint8_t* edges;          // (u, v) byte pairs of all instances
     const uint32_t* eoff;          // instance -> first edge
     const uint32_t* ne;            // instance -> edge count
-    const T* rx;                   // [global circuit][p] (cos beta, sin beta)
+    const T* rot;                  // [global circuit][nparam] (cos, sin) of Rx(2 beta) / Ry(theta) half-angles
+    uint32_t nparam;
     const T* ph;                   // [global circuit][p][phs] (re, im) of exp(-i gamma (|E| - 2k))
     uint32_t p, phs;
     double* epart;                 // [wave circuit][ntiles]
@@ -73,18 +74,17 @@ struct QArgs {
 // edges between two slots (at most 10 in a simple graph) are listed.
 template <int RB>
 struct CutPlan {
-    int cu;
-    int a0[RB], a1[RB];
-    uint64_t ss;   // 6 bits per slot-slot edge: s | t << 3
+    int base;          // cut of the register index 0 (all slot bits 0)
+    int delta[RB];     // change of the cut when slot s flips to 1 (slot-slot edges excluded)
+    uint64_t ss;       // 6 bits per slot-slot edge: s | t << 3
     int nss;
 };
 
 template <int RB>
 __device__ __forceinline__ void cut_plan(CutPlan<RB>& cp, const uint8_t* __restrict__ e, uint32_t ne, uint64_t U,
                                          uint64_t slotmask) {
-    cp.cu = 0;
-#pragma unroll
-    for (int s = 0; s < RB; ++s) { cp.a0[s] = 0; cp.a1[s] = 0; }
+    int cu = 0;
+    uint64_t pk = 0;   // 6-bit counters, field 2s+b: edges from slot s to a non-slot vertex whose bit is b
     cp.ss = 0;
     cp.nss = 0;
     for (uint32_t k = 0; k < ne; ++k) {
@@ -92,13 +92,13 @@ __device__ __forceinline__ void cut_plan(CutPlan<RB>& cp, const uint8_t* __restr
         const bool su = (slotmask >> u) & 1ull, sv = (slotmask >> v) & 1ull;
         const int bu = (int)((U >> u) & 1ull), bv = (int)((U >> v) & 1ull);
         if (!su && !sv) {
-            cp.cu += bu ^ bv;
+            cu += bu ^ bv;
         } else if (su && !sv) {
             const int s = __popcll(slotmask & ((1ull << u) - 1));
-            if (bv) cp.a1[s]++; else cp.a0[s]++;
+            pk += 1ull << (6 * (2 * s + bv));
         } else if (!su && sv) {
             const int s = __popcll(slotmask & ((1ull << v) - 1));
-            if (bu) cp.a1[s]++; else cp.a0[s]++;
+            pk += 1ull << (6 * (2 * s + bu));
         } else if (cp.nss < 10) {
             const uint64_t s = (uint64_t)__popcll(slotmask & ((1ull << u) - 1));
             const uint64_t t = (uint64_t)__popcll(slotmask & ((1ull << v) - 1));
@@ -106,13 +106,22 @@ __device__ __forceinline__ void cut_plan(CutPlan<RB>& cp, const uint8_t* __restr
             cp.nss++;
         }
     }
+    // slot bit 0: an edge to a non-slot vertex w counts iff bit_w = 1; slot bit 1: iff bit_w = 0
+    cp.base = cu;
+#pragma unroll
+    for (int s = 0; s < RB; ++s) {
+        const int n0 = (int)((pk >> (12 * s)) & 63), n1 = (int)((pk >> (12 * s + 6)) & 63);
+        cp.base += n1;
+        cp.delta[s] = n0 - n1;
+    }
 }
 
 template <int RB>
 __device__ __forceinline__ int cut_of(const CutPlan<RB>& cp, int i) {
-    int c = cp.cu;
+    int c = cp.base;
 #pragma unroll
-    for (int s = 0; s < RB; ++s) c += ((i >> s) & 1) ? cp.a0[s] : cp.a1[s];
+    for (int s = 0; s < RB; ++s)
+        if ((i >> s) & 1) c += cp.delta[s];
     uint64_t ss = cp.ss;
     for (int k = 0; k < cp.nss; ++k, ss >>= 6) {
         const int s = (int)(ss & 7), t = (int)((ss >> 3) & 7);
@@ -159,6 +168,36 @@ __device__ __forceinline__ void dispatch_rx(int k, V* reg, T c, T s) {
     }
 }
 
+// Ry(theta) on slot K: [[c, -s], [s, c]] with c = cos(theta/2), s = sin(theta/2)
+template <int K, int NR, typename V, typename T>
+__device__ __forceinline__ void op_ry(V* reg, T c, T s) {
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+        if (i & (1 << K)) continue;
+        const int j = i | (1 << K);
+        V x = reg[i], y = reg[j];
+        V o0, o1;
+        o0.x = c * x.x - s * y.x;
+        o0.y = c * x.y - s * y.y;
+        o1.x = s * x.x + c * y.x;
+        o1.y = s * x.y + c * y.y;
+        reg[i] = o0;
+        reg[j] = o1;
+    }
+}
+
+template <int NR, typename V, typename T>
+__device__ __forceinline__ void dispatch_ry(int k, V* reg, T c, T s) {
+    switch (k) {
+        case 0: op_ry<0, NR>(reg, c, s); break;
+        case 1: op_ry<1, NR>(reg, c, s); break;
+        case 2: op_ry<2, NR>(reg, c, s); break;
+        case 3: if constexpr (NR > 8) op_ry<3, NR>(reg, c, s); break;
+        case 4: if constexpr (NR > 16) op_ry<4, NR>(reg, c, s); break;
+        default: break;
+    }
+}
+
 __device__ __forceinline__ double warp_sum_d(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
@@ -167,7 +206,7 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 
 // Batched QAOA sweep over (circuit, tile) work items of one class.
 template <typename T, int RB>
-__global__ void __launch_bounds__(256, 2) k_qaoa_sweep(const SweepDesc d, const PhaseDesc* __restrict__ phases,
+__global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const PhaseDesc* __restrict__ phases,
                                                       const SwOp* __restrict__ ops, QArgs<T> a) {
     using V = typename C2<T>::t;
     using VV = typename Vec16b<T>::t;
@@ -188,6 +227,7 @@ __global__ void __launch_bounds__(256, 2) k_qaoa_sweep(const SweepDesc d, const 
         for (uint32_t b = d.c; b < d.m; ++b)
             if ((x >> b) & 1ull) dep_tid |= 1ull << d.local_global[b];
     }
+    const uint32_t stid = swzb<T>(tid * EPV);   // swz(e) = stid ^ sgj[j] (the swizzle is XOR-linear)
     const uint64_t nwork = a.ncirc * a.ntiles;
     const uint64_t nstate = 1ull << d.n;
 
@@ -195,14 +235,18 @@ __global__ void __launch_bounds__(256, 2) k_qaoa_sweep(const SweepDesc d, const 
         const uint64_t circ = w / a.ntiles, tile = w - circ * a.ntiles;
         const uint64_t gcirc = a.circ0 + circ;
         V* amps = a.amps + circ * nstate;
-        const uint32_t inst = a.circ_inst[gcirc];
-        const uint8_t* edges = a.edges + 2 * (size_t)a.eoff[inst];
-        const uint32_t ne = a.ne[inst];
+        const uint8_t* edges = nullptr;
+        uint32_t ne = 0;
+        if (a.circ_inst) {
+            const uint32_t inst = a.circ_inst[gcirc];
+            edges = a.edges + 2 * (size_t)a.eoff[inst];
+            ne = a.ne[inst];
+        }
         uint64_t base = 0;
         for (uint32_t b = 0; b < d.nonlocal_count; ++b)
             if ((tile >> b) & 1ull) base |= 1ull << d.nonlocal[b];
 
-        const bool init = (d.flags & SWEEP_INIT_UNIFORM) != 0;
+        const bool init = (d.flags & (SWEEP_INIT_UNIFORM | SWEEP_INIT_ZERO)) != 0;
         if (!init) {
 #pragma unroll 1
             for (int j0 = 0; j0 < VPT; j0 += 8) {
@@ -212,12 +256,12 @@ __global__ void __launch_bounds__(256, 2) k_qaoa_sweep(const SweepDesc d, const 
                     v[jj] = __ldcs(reinterpret_cast<const VV*>(amps + (base | dep_tid | d.gj[j0 + jj])));
 #pragma unroll
                 for (int jj = 0; jj < 8; ++jj) {
-                    const uint32_t e = (tid + T_ * (j0 + jj)) * EPV;
+                    const uint32_t se = stid ^ d.sgj[j0 + jj];
                     if constexpr (EPV == 2) {
-                        sm[swzb<T>(e)] = make_float2(v[jj].x, v[jj].y);
-                        sm[swzb<T>(e + 1)] = make_float2(v[jj].z, v[jj].w);
+                        sm[se] = make_float2(v[jj].x, v[jj].y);
+                        sm[se ^ 1u] = make_float2(v[jj].z, v[jj].w);
                     } else {
-                        sm[swzb<T>(e)] = *reinterpret_cast<V*>(&v[jj]);
+                        sm[se] = *reinterpret_cast<V*>(&v[jj]);
                     }
                 }
             }
@@ -234,22 +278,40 @@ __global__ void __launch_bounds__(256, 2) k_qaoa_sweep(const SweepDesc d, const 
                     ebase |= 1u << ph.tbit_local[b];
                     U |= 1ull << ph.tbit_global[b];
                 }
+            const uint32_t sb = swzb<T>(ebase);
             uint64_t slotmask = 0;
 #pragma unroll
             for (int s = 0; s < RB; ++s) slotmask |= 1ull << ph.slot_global[s];
             V reg[NR];
             if (init && p == d.phase_begin) {
+                if (d.flags & SWEEP_INIT_UNIFORM) {
 #pragma unroll
-                for (int i = 0; i < NR; ++i) { reg[i].x = a.amp0; reg[i].y = (T)0; }
+                    for (int i = 0; i < NR; ++i) { reg[i].x = a.amp0; reg[i].y = (T)0; }
+                } else {   // |0...0>
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) { reg[i].x = (i == 0 && U == 0) ? (T)1 : (T)0; reg[i].y = (T)0; }
+                }
             } else {
 #pragma unroll
-                for (int i = 0; i < NR; ++i) reg[i] = sm[swzb<T>(ebase | ph.lut[i])];
+                for (int i = 0; i < NR; ++i) reg[i] = sm[sb ^ ph.slut[i]];
             }
             for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
                 const SwOp op = ops[o];
                 if (op.type == OP_RXP) {
-                    const T* r = a.rx + ((size_t)gcirc * a.p + op.param) * 2;
+                    const T* r = a.rot + ((size_t)gcirc * a.nparam + op.param) * 2;
                     dispatch_rx<NR>(op.k0, reg, r[0], r[1]);
+                } else if (op.type == OP_RYP) {
+                    const T* r = a.rot + ((size_t)gcirc * a.nparam + op.param) * 2;
+                    dispatch_ry<NR>(op.k0, reg, r[0], r[1]);
+                } else if (op.type == OP_CZ) {
+                    const int k0 = op.k0, k1 = op.k1;
+                    const int u0 = (int)((U >> op.q0) & 1ull), u1 = (int)((U >> op.q1) & 1ull);
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) {
+                        const int b0 = k0 >= 0 ? ((i >> k0) & 1) : u0;
+                        const int b1 = k1 >= 0 ? ((i >> k1) & 1) : u1;
+                        if (b0 & b1) { reg[i].x = -reg[i].x; reg[i].y = -reg[i].y; }
+                    }
                 } else if (op.type == OP_CPH) {
                     CutPlan<RB> cp;
                     cut_plan<RB>(cp, edges, ne, U, slotmask);
@@ -271,7 +333,7 @@ __global__ void __launch_bounds__(256, 2) k_qaoa_sweep(const SweepDesc d, const 
                 }
             }
 #pragma unroll
-            for (int i = 0; i < NR; ++i) sm[swzb<T>(ebase | ph.lut[i])] = reg[i];
+            for (int i = 0; i < NR; ++i) sm[sb ^ ph.slut[i]] = reg[i];
             __syncthreads();
         }
 
@@ -289,14 +351,14 @@ __global__ void __launch_bounds__(256, 2) k_qaoa_sweep(const SweepDesc d, const 
 
 #pragma unroll
         for (int j = 0; j < VPT; ++j) {
-            const uint32_t e = (tid + T_ * j) * EPV;
+            const uint32_t se = stid ^ d.sgj[j];
             const uint64_t g = base | dep_tid | d.gj[j];
             VV v;
             if constexpr (EPV == 2) {
-                float2 x = sm[swzb<T>(e)], y = sm[swzb<T>(e + 1)];
+                float2 x = sm[se], y = sm[se ^ 1u];
                 v = make_float4(x.x, x.y, y.x, y.y);
             } else {
-                V x = sm[swzb<T>(e)];
+                V x = sm[se];
                 v = *reinterpret_cast<VV*>(&x);
             }
             __stcs(reinterpret_cast<VV*>(amps + g), v);
@@ -439,6 +501,106 @@ __global__ void k_bsample(const typename C2<T>::t* __restrict__ amps, const doub
     }
 }
 
+
+// ---- batched VQE -------------------------------------------------------------
+
+// Pauli strings sharing one X/Y pattern (same rules as rq_reduce.cu):
+// x == 0: acc += s(i)|a_i|^2 over all i; x != 0: over pairs (i, i^x) with the
+// top bit h of x clear, acc += s(i) * (odd ? Im : Re) of conj(a_{i^x}) a_i.
+struct VGroup {
+    uint64_t x;
+    uint32_t h, t0, nt, pad;
+};
+struct VTerm {
+    uint64_t pmask;
+    uint32_t odd, pad;
+    double factor;   // coeff * the ny / pairing factor
+};
+
+template <typename T>
+__global__ void k_vqe_energy(const typename C2<T>::t* __restrict__ states, uint32_t n, uint64_t ncirc, uint64_t circ0,
+                             const VGroup* __restrict__ groups, uint32_t ngroups, const VTerm* __restrict__ terms,
+                             double* __restrict__ energies) {
+    __shared__ double red[8][8];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint64_t N = 1ull << n;
+    for (uint64_t c = blockIdx.x; c < ncirc; c += gridDim.x) {
+        const typename C2<T>::t* a = states + c * N;
+        double E = 0.0;
+        for (uint32_t g = 0; g < ngroups; ++g) {
+            const VGroup G = groups[g];
+            uint64_t pm[8];
+            uint32_t od[8];
+            double acc[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                pm[k] = k < (int)G.nt ? terms[G.t0 + k].pmask : 0;
+                od[k] = k < (int)G.nt ? terms[G.t0 + k].odd : 0;
+                acc[k] = 0.0;
+            }
+            const uint64_t count = G.x ? N >> 1 : N;
+            for (uint64_t q = threadIdx.x; q < count; q += blockDim.x) {
+                uint64_t i;
+                double re, im;
+                if (G.x == 0) {
+                    i = q;
+                    const auto v = a[i];
+                    const double vr = v.x, vi = v.y;
+                    re = vr * vr + vi * vi;
+                    im = 0.0;
+                } else {
+                    i = rqd::insert0(q, G.h);
+                    const auto ai = a[i];
+                    const auto aj = a[i ^ G.x];
+                    const double air = ai.x, aii = ai.y, ajr = aj.x, aji = aj.y;
+                    re = ajr * air + aji * aii;
+                    im = ajr * aii - aji * air;
+                }
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const double v = od[k] ? im : re;
+                    acc[k] += (__popcll(i & pm[k]) & 1) ? -v : v;
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                double v = warp_sum_d(acc[k]);
+                if (lane == 0) red[warp][k] = v;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (uint32_t k = 0; k < G.nt; ++k) {
+                    double sum = 0.0;
+                    for (uint32_t w = 0; w < nw; ++w) sum += red[w][k];
+                    E += terms[G.t0 + k].factor * sum;
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) energies[circ0 + c] = E;
+    }
+}
+
+// (cos, sin) of theta/2 for every (circuit, parameter): circuit = set * V + v;
+// v = 0 is the set's parameters, v = 1 + 2k / 2 + 2k shift parameter k by +pi/2 / -pi/2
+template <typename T>
+__global__ void k_vqe_rot(const double* __restrict__ params, uint64_t ncirc, uint32_t P, uint32_t V, T* __restrict__ rot) {
+    const uint64_t total = ncirc * P;
+    const double hp = 1.57079632679489661923;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = w / P;
+        const uint32_t k = (uint32_t)(w - c * P);
+        const uint64_t set = c / V;
+        const uint32_t v = (uint32_t)(c - set * V);
+        double th = params[set * P + k];
+        if (v > 0 && (v - 1) / 2 == k) th += (v & 1) ? hp : -hp;
+        double sn, cs;
+        sincos(0.5 * th, &sn, &cs);
+        rot[2 * w] = (T)cs;
+        rot[2 * w + 1] = (T)sn;
+    }
+}
+
 constexpr int TPB = 256;
 
 }  // namespace
@@ -541,7 +703,8 @@ int launch_class(rq_qaoa_batch* b, QClass& K, uint64_t ncirc, uint64_t circ0, vo
     a.edges = b->d_edges;
     a.eoff = b->d_eoff;
     a.ne = b->d_ne;
-    a.rx = (const T*)b->d_rx;
+    a.rot = (const T*)b->d_rx;
+    a.nparam = b->p;
     a.ph = (const T*)b->d_ph;
     a.p = b->p;
     a.phs = b->phs;
@@ -549,7 +712,7 @@ int launch_class(rq_qaoa_batch* b, QClass& K, uint64_t ncirc, uint64_t circ0, vo
     a.amp0 = (T)std::sqrt(std::ldexp(1.0, -(int)K.n));
     const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(K.prog);
     const SwOp* op = reinterpret_cast<const SwOp*>(K.prog + K.off_ops);
-    auto kern = k_qaoa_sweep<T, RBc>;
+    auto kern = k_batch_sweep<T, RBc>;
     RQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem));
     const unsigned threads = 1u << (K.m - rb);
     int per_sm = 0;
@@ -848,6 +1011,248 @@ int rq_qaoa_batch_last_ms(const rq_qaoa_batch* b, float* ms) {
 int rq_qaoa_batch_set_state_budget(rq_qaoa_batch* b, uint64_t bytes) {
     if (!b || bytes == 0) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "bad argument");
     b->state_budget = bytes;
+    return RQ_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// batched VQE: the hardware-efficient ansatz "Ry on every qubit, then a CZ
+// ladder CZ(q, q+1)" per layer, energies of a Pauli-sum Hamiltonian
+// (expectation_hamiltonian, state.rs:403-408) and parameter-shift gradients
+// (run_vqe's rule, vqe.rs:186-198) for many parameter sets at once.
+// ===========================================================================
+struct rq_vqe_batch {
+    int device = 0;
+    int32_t prec = RQ_F32;
+    uint32_t n = 0, depth = 0, P = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<SweepDesc> descs;
+    unsigned char* prog = nullptr;
+    size_t off_ops = 0, smem = 0;
+    uint64_t ntiles = 0;
+    uint32_t m = 0;
+    VGroup* d_groups = nullptr;
+    VTerm* d_terms = nullptr;
+    uint32_t ngroups = 0;
+    double* d_params = nullptr;
+    size_t params_cap = 0;
+    void* d_rot = nullptr;
+    size_t rot_cap = 0;
+    void* d_states = nullptr;
+    size_t states_cap = 0;
+    double* d_energy = nullptr;
+    size_t energy_cap = 0;
+    float last_ms = 0.f;
+    size_t wave_bytes = (size_t)96 << 20;   // states per wave kept around the L2 size
+};
+
+namespace {
+
+template <typename T>
+int vqe_wave(rq_vqe_batch* b, uint64_t ncirc, uint64_t circ0) {
+    using V = typename C2<T>::t;
+    constexpr int RBc = std::is_same<T, float>::value ? 5 : 4;
+    QArgs<T> a{};
+    a.amps = (V*)b->d_states;
+    a.ncirc = ncirc;
+    a.ntiles = b->ntiles;
+    a.circ0 = circ0;
+    a.rot = (const T*)b->d_rot;
+    a.nparam = b->P;
+    const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(b->prog);
+    const SwOp* op = reinterpret_cast<const SwOp*>(b->prog + b->off_ops);
+    auto kern = k_batch_sweep<T, RBc>;
+    RQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem));
+    const unsigned threads = 1u << (b->m - RBc);
+    int per_sm = 0;
+    RQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)threads, b->smem));
+    if (per_sm < 1) return rq::fail(RQ_ERR_CUDA, "batched sweep kernel does not fit on an SM");
+    const int sms = rq::num_sms(b->device);
+    const unsigned grid = (unsigned)std::min<uint64_t>(ncirc * b->ntiles, (uint64_t)sms * per_sm);
+    for (const auto& d : b->descs) {
+        kern<<<grid, threads, b->smem, b->stream>>>(d, ph, op, a);
+        RQ_CUDA(cudaGetLastError());
+    }
+    const unsigned ge = (unsigned)std::min<uint64_t>(ncirc, (uint64_t)sms * 8);
+    k_vqe_energy<T><<<ge, 256, 0, b->stream>>>((const V*)b->d_states, b->n, ncirc, circ0, b->d_groups, b->ngroups,
+                                                 b->d_terms, b->d_energy);
+    RQ_CUDA(cudaGetLastError());
+    return RQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rq_vqe_batch_create(uint32_t num_qubits, uint32_t depth, const double* coeffs, const rq_pauli_op* ops,
+                        const uint32_t* offsets, uint32_t nterms, int32_t precision, rq_vqe_batch** out) {
+    if (!out || (!coeffs && nterms) || (!offsets && nterms)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (precision != RQ_F32 && precision != RQ_F64)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "precision must be RQ_F32 or RQ_F64");
+    const uint32_t rb = precision == RQ_F32 ? 5 : 4;
+    if (num_qubits < rb + 2 || num_qubits > 30)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "batched VQE takes " + std::to_string(rb + 2) + "..30 qubits");
+    if (depth == 0) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "depth must be >= 1");
+    std::unique_ptr<rq_vqe_batch> b(new rq_vqe_batch());
+    b->prec = precision;
+    b->n = num_qubits;
+    b->depth = depth;
+    b->P = num_qubits * depth;
+    cudaGetDevice(&b->device);
+    // Hamiltonian in mask form, grouped by X/Y pattern, chunks of <= 8 terms
+    std::map<uint64_t, std::vector<std::pair<uint64_t, std::pair<uint32_t, double>>>> by_x;   // x -> (pmask, (ny, coeff))
+    for (uint32_t k = 0; k < nterms; ++k) {
+        if (offsets[k + 1] < offsets[k]) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing");
+        uint64_t x = 0, pm = 0;
+        uint32_t ny = 0;
+        for (uint32_t j = offsets[k]; j < offsets[k + 1]; ++j) {
+            const uint32_t q = ops[j].qubit;
+            const int o = ops[j].op;
+            if (o < RQ_PAULI_I || o > RQ_PAULI_Z) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "invalid Pauli operator");
+            if (o == RQ_PAULI_I) continue;
+            if (q >= num_qubits) return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "Pauli factor on qubit " + std::to_string(q));
+            if (o == RQ_PAULI_X || o == RQ_PAULI_Y) x ^= 1ull << q;
+            if (o == RQ_PAULI_Y || o == RQ_PAULI_Z) pm ^= 1ull << q;
+            if (o == RQ_PAULI_Y) ++ny;
+        }
+        by_x[x].push_back({pm, {ny & 3u, coeffs[k]}});
+    }
+    auto re_ip = [](uint32_t k) { k &= 3u; return k == 0 ? 1.0 : (k == 2 ? -1.0 : 0.0); };
+    std::vector<VGroup> groups;
+    std::vector<VTerm> terms;
+    for (auto& kv : by_x) {
+        const uint64_t x = kv.first;
+        const auto& list = kv.second;
+        for (size_t c0 = 0; c0 < list.size(); c0 += 8) {
+            VGroup G{};
+            G.x = x;
+            G.h = x ? 63 - __builtin_clzll(x) : 0;
+            G.t0 = (uint32_t)terms.size();
+            G.nt = (uint32_t)std::min<size_t>(8, list.size() - c0);
+            for (uint32_t k = 0; k < G.nt; ++k) {
+                const auto& t = list[c0 + k];
+                VTerm vt{};
+                vt.pmask = t.first;
+                const uint32_t ny = t.second.first;
+                const bool odd = x && (__builtin_popcountll(x & t.first) & 1);
+                vt.odd = odd ? 1u : 0u;
+                const double f = x == 0 ? re_ip(ny) : (odd ? 2.0 * re_ip(ny + 1) : 2.0 * re_ip(ny));
+                vt.factor = t.second.second * f;
+                terms.push_back(vt);
+            }
+            groups.push_back(G);
+        }
+    }
+    b->ngroups = (uint32_t)groups.size();
+    if (groups.empty()) groups.push_back(VGroup{});
+    if (terms.empty()) terms.push_back(VTerm{});
+    RQ_CUDA(cudaMalloc((void**)&b->d_groups, groups.size() * sizeof(VGroup)));
+    RQ_CUDA(cudaMemcpy(b->d_groups, groups.data(), groups.size() * sizeof(VGroup), cudaMemcpyHostToDevice));
+    RQ_CUDA(cudaMalloc((void**)&b->d_terms, terms.size() * sizeof(VTerm)));
+    RQ_CUDA(cudaMemcpy(b->d_terms, terms.data(), terms.size() * sizeof(VTerm), cudaMemcpyHostToDevice));
+    // the ansatz program
+    b->m = std::min(num_qubits, precision == RQ_F32 ? 13u : 12u);
+    const uint32_t c = std::min<uint32_t>(b->m, 5);
+    b->ntiles = 1ull << (num_qubits - b->m);
+    b->smem = ((size_t)1 << b->m) * elem_size(precision);
+    std::vector<PGate> g;
+    for (uint32_t l = 0; l < depth; ++l) {
+        for (uint32_t q = 0; q < num_qubits; ++q) {
+            PGate r{};
+            r.type = OP_RYP;
+            r.q0 = q;
+            r.param = (uint16_t)(l * num_qubits + q);
+            g.push_back(r);
+        }
+        for (uint32_t q = 0; q + 1 < num_qubits; ++q) {
+            PGate z{};
+            z.type = OP_CZ;
+            z.q0 = q;
+            z.q1 = q + 1;
+            g.push_back(z);
+        }
+    }
+    auto sweeps = plan_sweeps(g, num_qubits, b->m, c);
+    std::vector<PhaseDesc> phases;
+    std::vector<SwOp> opsv;
+    std::vector<double> mats;
+    build_program(sweeps, num_qubits, b->m, c, rb, precision == RQ_F32 ? 2 : 1, b->descs, phases, opsv, mats);
+    b->descs.front().flags |= SWEEP_INIT_ZERO;
+    b->off_ops = (phases.size() * sizeof(PhaseDesc) + 255) & ~size_t(255);
+    const size_t total = b->off_ops + opsv.size() * sizeof(SwOp);
+    std::vector<unsigned char> host(total);
+    std::memcpy(host.data(), phases.data(), phases.size() * sizeof(PhaseDesc));
+    std::memcpy(host.data() + b->off_ops, opsv.data(), opsv.size() * sizeof(SwOp));
+    RQ_CUDA(cudaMalloc((void**)&b->prog, total));
+    RQ_CUDA(cudaMemcpy(b->prog, host.data(), total, cudaMemcpyHostToDevice));
+    RQ_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    RQ_CUDA(cudaEventCreate(&b->ev0));
+    RQ_CUDA(cudaEventCreate(&b->ev1));
+    *out = b.release();
+    return RQ_OK;
+}
+
+int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* params, int32_t with_gradient, double* energies,
+                     double* gradients) {
+    if (!b || !params || !energies || (with_gradient && !gradients))
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (nsets == 0) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "nsets must be >= 1");
+    RQ_CUDA(cudaSetDevice(b->device));
+    const uint32_t P = b->P;
+    const uint32_t V = with_gradient ? 1 + 2 * P : 1;
+    const uint64_t ncirc = (uint64_t)nsets * V;
+    const size_t es = b->prec == RQ_F32 ? sizeof(float) : sizeof(double);
+    RQ_TRY(grow(&b->d_params, &b->params_cap, (size_t)nsets * P));
+    RQ_TRY(grow_bytes(&b->d_rot, &b->rot_cap, ncirc * P * 2 * es));
+    RQ_TRY(grow(&b->d_energy, &b->energy_cap, ncirc));
+    const size_t state_bytes = ((size_t)1 << b->n) * elem_size(b->prec);
+    const uint64_t wave = std::max<uint64_t>(1, std::min<uint64_t>(ncirc, b->wave_bytes / state_bytes));
+    RQ_TRY(grow_bytes(&b->d_states, &b->states_cap, wave * state_bytes));
+    RQ_CUDA(cudaMemcpyAsync(b->d_params, params, (size_t)nsets * P * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    const int sms = rq::num_sms(b->device);
+    RQ_CUDA(cudaEventRecord(b->ev0, b->stream));
+    if (b->prec == RQ_F32)
+        k_vqe_rot<float><<<rq::grid_for(ncirc * P, TPB, sms), TPB, 0, b->stream>>>(b->d_params, ncirc, P, V, (float*)b->d_rot);
+    else
+        k_vqe_rot<double><<<rq::grid_for(ncirc * P, TPB, sms), TPB, 0, b->stream>>>(b->d_params, ncirc, P, V, (double*)b->d_rot);
+    RQ_CUDA(cudaGetLastError());
+    for (uint64_t w0 = 0; w0 < ncirc; w0 += wave) {
+        const uint64_t wn = std::min<uint64_t>(wave, ncirc - w0);
+        if (b->prec == RQ_F32) RQ_TRY(vqe_wave<float>(b, wn, w0));
+        else RQ_TRY(vqe_wave<double>(b, wn, w0));
+    }
+    RQ_CUDA(cudaEventRecord(b->ev1, b->stream));
+    std::vector<double> e(ncirc);
+    RQ_CUDA(cudaMemcpyAsync(e.data(), b->d_energy, ncirc * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    RQ_CUDA(cudaStreamSynchronize(b->stream));
+    RQ_CUDA(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+    for (uint32_t s = 0; s < nsets; ++s) {
+        energies[s] = e[(uint64_t)s * V];
+        if (with_gradient)
+            for (uint32_t k = 0; k < P; ++k)
+                gradients[(uint64_t)s * P + k] = (e[(uint64_t)s * V + 1 + 2 * k] - e[(uint64_t)s * V + 2 + 2 * k]) / 2.0;
+    }
+    return RQ_OK;
+}
+
+int rq_vqe_batch_last_ms(const rq_vqe_batch* b, float* ms) {
+    if (!b || !ms) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    *ms = b->last_ms;
+    return RQ_OK;
+}
+
+int rq_vqe_batch_destroy(rq_vqe_batch* b) {
+    if (!b) return RQ_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    void* ptrs[] = {b->prog, b->d_groups, b->d_terms, b->d_params, b->d_rot, b->d_states, b->d_energy};
+    for (void* q : ptrs) if (q) cudaFree(q);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
     return RQ_OK;
 }
 

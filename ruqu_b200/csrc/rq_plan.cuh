@@ -27,21 +27,23 @@ enum OpType : uint8_t { OP_U1 = 0, OP_D1 = 1, OP_CX = 2, OP_CZ = 3, OP_ZZ = 4, O
 constexpr int RBMAX = 5;
 constexpr int MMAX = 14;
 
-struct SwOp {
+struct __align__(16) SwOp {
     uint8_t type;
     int8_t k0, k1;   // register slot of q0 / q1 in this phase, -1 if not a slot
     uint8_t q0, q1;  // global qubits
     uint8_t pad;
     uint16_t param;  // layer / parameter index of CPH, RXP, RYP
     uint32_t mat;    // first complex entry in the matrix table
+    uint32_t pad2;
 };
 
-struct PhaseDesc {
+struct __align__(16) PhaseDesc {
+    uint32_t slut[1 << RBMAX];   // swz(lut[i]) for the state's element size
     uint32_t op_begin, op_end;
-    uint32_t nt;              // number of thread bits
-    uint8_t tbit_local[16];   // thread bit b -> local bit index
-    uint8_t tbit_global[16];  // thread bit b -> global qubit
-    uint16_t lut[1 << RBMAX]; // register index -> local offset
+    uint32_t nt;                 // number of thread bits
+    uint8_t tbit_local[16];      // thread bit b -> local bit index
+    uint8_t tbit_global[16];     // thread bit b -> global qubit
+    uint16_t lut[1 << RBMAX];    // register index -> local offset
     uint8_t slot_global[RBMAX];  // register slot -> global qubit
 };
 
@@ -53,10 +55,12 @@ struct SweepDesc {
     uint32_t phase_begin, phase_end;
     uint32_t flags;             // SWEEP_INIT_UNIFORM | SWEEP_ENERGY (batched sweeps)
     uint64_t gj[1 << RBMAX];    // deposit of the per-thread vector offsets
+    uint32_t sgj[1 << RBMAX];   // swz((tid-independent part of) the vector's first element)
 };
 
 constexpr uint32_t SWEEP_INIT_UNIFORM = 1u;   // synthesise |+>^n instead of loading the tile
 constexpr uint32_t SWEEP_ENERGY = 2u;         // reduce sum |a|^2 cut(x) after the last phase
+constexpr uint32_t SWEEP_INIT_ZERO = 4u;      // synthesise |0...0> instead of loading the tile
 
 
 struct PGate {
@@ -270,6 +274,16 @@ inline bool to_pgates(const rq_gate* gates, uint64_t n, std::vector<PGate>& out)
 }
 
 
+// Shared-memory swizzle of a tile element index: XOR the element's column
+// inside its 128-byte row with a fold of the row index.  Linear over GF(2),
+// so swz(a | b) = swz(a) ^ swz(b) for disjoint bit sets; the kernels combine
+// host-swizzled table entries with one per-thread term by XOR.
+inline uint32_t swz_host(uint32_t e, uint32_t cb) {
+    uint32_t r = e >> cb;
+    uint32_t f = r ^ (r >> cb) ^ (r >> (2 * cb)) ^ (r >> (3 * cb));
+    return e ^ (f & ((1u << cb) - 1));
+}
+
 // Flatten sweeps into kernel tables: one SweepDesc per sweep, PhaseDescs,
 // op records and the f64 matrix entries (narrowed later for f32 states).
 inline void build_program(std::vector<Sweep>& sweeps, uint32_t nq, uint32_t m, uint32_t c, uint32_t rb,
@@ -292,11 +306,13 @@ inline void build_program(std::vector<Sweep>& sweeps, uint32_t nq, uint32_t m, u
         d.nonlocal_count = ni;
         const uint32_t t = m - rb;
         const uint32_t VPT = (1u << rb) / epv;
+        const uint32_t cb = epv == 2 ? 4 : 3;
         for (uint32_t j = 0; j < VPT; ++j) {
             uint64_t x = (uint64_t)j * (1ull << t) * epv, gsum = 0;
             for (uint32_t b = 0; b < m; ++b)
                 if ((x >> b) & 1) gsum |= 1ull << d.local_global[b];
             d.gj[j] = gsum;
+            d.sgj[j] = swz_host((uint32_t)x, cb);
         }
         d.phase_begin = (uint32_t)phases.size();
         auto pplan = plan_phases(sw, rb);
@@ -319,6 +335,7 @@ inline void build_program(std::vector<Sweep>& sweeps, uint32_t nq, uint32_t m, u
                 for (uint32_t sidx = 0; sidx < ns; ++sidx)
                     if ((i >> sidx) & 1) off |= 1u << local_index[slots[sidx]];
                 Ph.lut[i] = (uint16_t)off;
+                Ph.slut[i] = swz_host(off, cb);
             }
             for (uint32_t sidx = 0; sidx < ns; ++sidx) Ph.slot_global[sidx] = (uint8_t)slots[sidx];
             for (int oi : pp.ops) {

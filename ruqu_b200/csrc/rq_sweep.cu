@@ -136,6 +136,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep(typename C2<T>::t* __restrict_
         for (uint32_t b = d.c; b < d.m; ++b)
             if ((x >> b) & 1ull) dep_tid |= 1ull << d.local_global[b];
     }
+    const uint32_t stid = swz<T>(tid * EPV);   // swz(e) = stid ^ sgj[j] (the swizzle is XOR-linear)
 
     for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         uint64_t base = 0;
@@ -151,12 +152,12 @@ __global__ void __launch_bounds__(256, 2) k_sweep(typename C2<T>::t* __restrict_
                 v[jj] = __ldcs(reinterpret_cast<const VV*>(amps + (base | dep_tid | d.gj[j0 + jj])));
 #pragma unroll
             for (int jj = 0; jj < 8; ++jj) {
-                const uint32_t e = (tid + T_ * (j0 + jj)) * EPV;
+                const uint32_t se = stid ^ d.sgj[j0 + jj];
                 if constexpr (EPV == 2) {
-                    sm[swz<T>(e)] = make_float2(v[jj].x, v[jj].y);
-                    sm[swz<T>(e + 1)] = make_float2(v[jj].z, v[jj].w);
+                    sm[se] = make_float2(v[jj].x, v[jj].y);
+                    sm[se ^ 1u] = make_float2(v[jj].z, v[jj].w);
                 } else {
-                    sm[swz<T>(e)] = *reinterpret_cast<V*>(&v[jj]);
+                    sm[se] = *reinterpret_cast<V*>(&v[jj]);
                 }
             }
         }
@@ -172,9 +173,10 @@ __global__ void __launch_bounds__(256, 2) k_sweep(typename C2<T>::t* __restrict_
                     ebase |= 1u << ph.tbit_local[b];
                     U |= 1ull << ph.tbit_global[b];
                 }
+            const uint32_t sb = swz<T>(ebase);
             V reg[NR];
 #pragma unroll
-            for (int i = 0; i < NR; ++i) reg[i] = sm[swz<T>(ebase | ph.lut[i])];
+            for (int i = 0; i < NR; ++i) reg[i] = sm[sb ^ ph.slut[i]];
 
             for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
                 const SwOp op = ops[o];
@@ -225,21 +227,21 @@ __global__ void __launch_bounds__(256, 2) k_sweep(typename C2<T>::t* __restrict_
                 }
             }
 #pragma unroll
-            for (int i = 0; i < NR; ++i) sm[swz<T>(ebase | ph.lut[i])] = reg[i];
+            for (int i = 0; i < NR; ++i) sm[sb ^ ph.slut[i]] = reg[i];
             __syncthreads();
         }
 
         // ---- store tile ----
 #pragma unroll
         for (int j = 0; j < VPT; ++j) {
-            const uint32_t e = (tid + T_ * j) * EPV;
+            const uint32_t se = stid ^ d.sgj[j];
             const uint64_t g = base | dep_tid | d.gj[j];
             VV v;
             if constexpr (EPV == 2) {
-                float2 a = sm[swz<T>(e)], b = sm[swz<T>(e + 1)];
+                float2 a = sm[se], b = sm[se ^ 1u];
                 v = make_float4(a.x, a.y, b.x, b.y);
             } else {
-                V a = sm[swz<T>(e)];
+                V a = sm[se];
                 v = *reinterpret_cast<VV*>(&a);
             }
             __stcs(reinterpret_cast<VV*>(amps + g), v);
