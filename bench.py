@@ -54,6 +54,8 @@ def _args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-qaoa", action="store_true", help="skip the batched QAOA leg")
     ap.add_argument("--qaoa-instances", type=int, default=2048)
+    ap.add_argument("--no-vqe", action="store_true", help="skip the batched VQE leg")
+    ap.add_argument("--vqe-sets", type=int, default=512)
     return ap.parse_args()
 
 
@@ -191,6 +193,44 @@ def qaoa_batch_leg(a, ws, rank, with_cpu):
                                "sample": "one evaluate_qaoa_cost (reference f64 engine, energy only, no shots) "
                                          "per n in {12,14,16,18} timed; n = 20, 22, 24 scaled by 4(n+2)/n per +2 "
                                          "qubits; summed over the 2048 instances"}
+    return res
+
+
+def vqe_batch_leg(a, ws, rank, with_cpu):
+    """Batched VQE energies + parameter-shift gradients: 16 qubits, H = 200 random
+    Pauli strings (seed 3), depth-8 Ry + CZ-ladder ansatz (128 parameters), 512
+    parameter sets ~ U[-pi, pi) (seed 4), each with 256 shifted evaluations:
+    131,584 circuits, f32 states, energies in FP64.  Sets are sharded over ranks."""
+    import numpy as np
+
+    from ruqu_b200 import workloads
+    from ruqu_b200.batch import VqeBatch
+    n, depth = 16, 8
+    coeffs, strings = workloads.pauli_hamiltonian(n, 200, 3)
+    params = workloads.vqe_parameter_sets(a.vqe_sets, n * depth, 4)[rank::ws]
+    vb = VqeBatch(n, depth, coeffs, strings, "f32")
+    vb.run(params[:2], gradient=True)           # warm-up
+    ms, wall = [], []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        e, g = vb.run(params, gradient=True)
+        wall.append(time.perf_counter() - t0)
+        ms.append(vb.last_ms())
+    circuits = len(params) * (1 + 2 * n * depth)
+    res = {"workload": "batched VQE, 16 qubits, 200-term Pauli Hamiltonian, depth-8 Ry+CZ ansatz, %d parameter "
+                       "sets x 257 parameter-shift circuits, f32 states" % a.vqe_sets,
+           "circuits_per_rank": circuits, "device_ms": min(ms), "wall_ms": 1e3 * min(wall),
+           "circuits_per_s": circuits * ws / (min(ms) / 1e3), "mean_energy": float(np.mean(e))}
+    if with_cpu:
+        import oracle
+        t0 = time.perf_counter()
+        k = 2
+        for s in range(k):
+            oracle.circuit_energy(n, workloads.hea_ry_cz(n, depth, params[s]), coeffs, strings)
+        dt = (time.perf_counter() - t0) / k
+        res["cpu_baseline"] = {"value": 1.0 / dt, "unit": "circuits/s", "cores": 1, "kind": "port",
+                               "sample": "evaluate_energy of 2 ansatz circuits on the reference f64 engine "
+                                         "(gate by gate, one pass per Pauli term), averaged"}
     return res
 
 
@@ -334,6 +374,15 @@ def run_ours(a):
             qaoa["device_ms_max_over_ranks"] = float(t.item())
             qaoa["evals_per_s"] = a.qaoa_instances / (qaoa["device_ms_max_over_ranks"] / 1e3)
 
+    vqe = None
+    if not a.no_vqe:
+        vqe = vqe_batch_leg(a, ws, rank, with_cpu=(rank == 0 and ws == 1 and not a.no_cpu_baseline))
+        if dist:
+            t = torch.tensor([vqe["device_ms"]], device="cuda")
+            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+            vqe["device_ms_max_over_ranks"] = float(t.item())
+            vqe["circuits_per_s"] = a.vqe_sets * 257 / (vqe["device_ms_max_over_ranks"] / 1e3)
+
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         v, secs, cores, desc = cpu_baseline_sample(a, parallel=False)
@@ -360,6 +409,7 @@ def run_ours(a):
             "e2e": e2e,
             "gpu_launches": a.steps * (1 + stats["launches"]),
             "qaoa_batch": qaoa,
+            "vqe_batch": vqe,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

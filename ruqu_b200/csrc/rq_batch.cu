@@ -23,6 +23,7 @@
 #include "rq_internal.cuh"
 #include "rq_plan.cuh"
 
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -581,6 +582,154 @@ __global__ void k_vqe_energy(const typename C2<T>::t* __restrict__ states, uint3
     }
 }
 
+
+// One Pauli group of a tile pass: NT strings (NT = 8 for 5..8), per-warp sums
+// into wsum.  Products of amplitudes in the state's precision, every product
+// added to an FP64 accumulator; indices fit 32 bits (at most 30 qubits).
+// need: 1 = only Re of conj(a_j) a_i is used, 2 = only Im, 3 = both.
+template <typename T, int NT>
+__device__ __forceinline__ void tile_group(const VGroup& G, const VTerm* __restrict__ terms,
+                                           const typename C2<T>::t* own, const typename C2<T>::t* src, uint32_t r,
+                                           uint32_t rp, uint32_t t, uint32_t M, double* wsum, uint32_t nterms,
+                                           uint32_t lane, uint32_t warp) {
+    using V = typename C2<T>::t;
+    const uint32_t L = 1u << M;
+    uint32_t pm[NT];
+    bool od[NT];
+    double acc[NT];
+    int need = 0;
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        pm[k] = k < (int)G.nt ? (uint32_t)terms[G.t0 + k].pmask : 0u;
+        od[k] = k < (int)G.nt ? terms[G.t0 + k].odd != 0 : false;
+        if (k < (int)G.nt) need |= od[k] ? 2 : 1;
+        acc[k] = 0.0;
+    }
+    const uint32_t x = (uint32_t)G.x;
+    const uint32_t xl = x & (L - 1);
+    const uint32_t count = x == 0 ? L : L >> 1;
+    const uint32_t sel = r < rp ? 0u : (1u ^ ((xl >> (M - 1)) & 1u));
+    const uint32_t rbase = r << M, pbase = rp << M;
+    for (uint32_t q = threadIdx.x; q < count; q += blockDim.x) {
+        T re = 0, im = 0;
+        uint32_t i;
+        if (x == 0) {
+            i = rbase | q;
+            const V v = own[q];
+            re = v.x * v.x + v.y * v.y;
+        } else {
+            V af, as;
+            if (t == 0) {
+                const uint32_t e = (uint32_t)rqd::insert0(q, G.h);
+                i = rbase | e;
+                af = own[e];
+                as = own[e ^ xl];
+            } else {
+                const uint32_t e = (uint32_t)rqd::insert0(q, M - 1) | (sel << (M - 1));
+                const uint32_t ep = e ^ xl;
+                const uint32_t im_ = rbase | e;
+                const V ao = own[e], ap = src[ep];
+                const bool first_is_mine = !((im_ >> G.h) & 1u);
+                i = first_is_mine ? im_ : (pbase | ep);
+                af = first_is_mine ? ao : ap;
+                as = first_is_mine ? ap : ao;
+            }
+            if (need & 1) re = as.x * af.x + as.y * af.y;
+            if (need & 2) im = as.x * af.y - as.y * af.x;
+        }
+        const double dre = (need & 1) ? (double)re : 0.0;
+        const double dim = (need & 2) ? (double)im : 0.0;
+#pragma unroll
+        for (int k = 0; k < NT; ++k) {
+            const double v = od[k] ? dim : dre;
+            acc[k] += (__popc(i & pm[k]) & 1) ? -v : v;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+        const double v = warp_sum_d(acc[k]);
+        if (lane == 0 && k < (int)G.nt) wsum[warp * nterms + G.t0 + k] = v;
+    }
+}
+
+// Tiled form: the state of a circuit is split into ntile tiles of 2^M
+// amplitudes; the CTA of (circuit, tile r) keeps tile r in shared memory and
+// loads every partner tile r ^ t once, evaluating all Pauli groups whose X/Y
+// pattern has top part x >> M == t from on-chip memory.  Pairs inside tile r
+// (t = 0) are all counted by that CTA; pairs between tiles lo < hi are split
+// by bit M-1 of their element in tile lo (0: CTA lo, 1: CTA hi), so each pair
+// is counted once.  Per-warp, per-string sums land in shared memory, the CTA
+// writes one partial per string, and k_vqe_finalize adds the tiles and the
+// strings in a fixed order.
+template <typename T>
+__global__ void __launch_bounds__(512, 1) k_vqe_energy_tiles(const typename C2<T>::t* __restrict__ states, uint32_t n,
+                                                             uint32_t M, uint64_t ncirc,
+                                                             const VGroup* __restrict__ groups,
+                                                             const uint32_t* __restrict__ gofs, uint32_t nterms,
+                                                             const VTerm* __restrict__ terms,
+                                                             double* __restrict__ part) {
+    using V = typename C2<T>::t;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint64_t L = 1ull << M;
+    V* own = reinterpret_cast<V*>(smem_raw);
+    V* par = own + L;
+    double* wsum = reinterpret_cast<double*>(par + L);   // [warps][nterms]
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t ntile = 1u << (n - M);
+    const uint64_t N = 1ull << n;
+    const uint64_t nwork = ncirc * ntile;
+    for (uint64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const uint64_t c = w / ntile;
+        const uint32_t r = (uint32_t)(w - c * ntile);
+        const V* a = states + c * N;
+        for (uint32_t k = threadIdx.x; k < nw * nterms; k += blockDim.x) wsum[k] = 0.0;
+        for (uint64_t e = threadIdx.x; e < L; e += blockDim.x) own[e] = a[((uint64_t)r << M) | e];
+        __syncthreads();
+        for (uint32_t t = 0; t < ntile; ++t) {
+            if (gofs[t] == gofs[t + 1]) continue;
+            const uint32_t rp = r ^ t;
+            const V* src = own;
+            if (t) {
+                for (uint64_t e = threadIdx.x; e < L; e += blockDim.x) par[e] = a[((uint64_t)rp << M) | e];
+                __syncthreads();
+                src = par;
+            }
+            const bool r_is_lo = r < rp;
+            for (uint32_t g = gofs[t]; g < gofs[t + 1]; ++g) {
+                const VGroup G = groups[g];
+                switch (G.nt) {
+                    case 1: tile_group<T, 1>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp); break;
+                    case 2: tile_group<T, 2>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp); break;
+                    case 3: tile_group<T, 3>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp); break;
+                    case 4: tile_group<T, 4>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp); break;
+                    default: tile_group<T, 8>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp); break;
+                }
+            }
+            __syncthreads();
+        }
+        for (uint32_t k = threadIdx.x; k < nterms; k += blockDim.x) {
+            double sum = 0.0;
+            for (uint32_t wv = 0; wv < nw; ++wv) sum += wsum[wv * nterms + k];
+            part[w * nterms + k] = sum;
+        }
+        __syncthreads();
+    }
+}
+
+// energies[circ0 + c] = sum over strings (in order) of factor * sum over tiles
+__global__ void k_vqe_finalize(const double* __restrict__ part, uint64_t ncirc, uint32_t ntile, uint32_t nterms,
+                               const VTerm* __restrict__ terms, uint64_t circ0, double* __restrict__ energies) {
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncirc; c += (uint64_t)gridDim.x * blockDim.x) {
+        double E = 0.0;
+        for (uint32_t k = 0; k < nterms; ++k) {
+            double s = 0.0;
+            for (uint32_t r = 0; r < ntile; ++r) s += part[(c * ntile + r) * nterms + k];
+            E += terms[k].factor * s;
+        }
+        energies[circ0 + c] = E;
+    }
+}
+
 // (cos, sin) of theta/2 for every (circuit, parameter): circuit = set * V + v;
 // v = 0 is the set's parameters, v = 1 + 2k / 2 + 2k shift parameter k by +pi/2 / -pi/2
 template <typename T>
@@ -1035,7 +1184,10 @@ struct rq_vqe_batch {
     uint32_t m = 0;
     VGroup* d_groups = nullptr;
     VTerm* d_terms = nullptr;
-    uint32_t ngroups = 0;
+    uint32_t* d_gofs = nullptr;   // groups of top pattern t: [gofs[t], gofs[t+1])
+    uint32_t ngroups = 0, nterms = 0;
+    double* d_part = nullptr;
+    size_t part_cap = 0;
     double* d_params = nullptr;
     size_t params_cap = 0;
     void* d_rot = nullptr;
@@ -1049,6 +1201,33 @@ struct rq_vqe_batch {
 };
 
 namespace {
+
+// energy of every circuit of a wave through the tiled kernel
+template <typename T>
+int vqe_energy(rq_vqe_batch* b, uint64_t ncirc, uint64_t circ0) {
+    using V = typename C2<T>::t;
+    const uint32_t n = b->n;
+    const uint32_t M = std::min<uint32_t>(n, 13);
+    const uint32_t ntile = 1u << (n - M);
+    const uint32_t threads = 512;
+    const size_t smem = 2 * ((size_t)1 << M) * sizeof(V) + (size_t)(threads / 32) * b->nterms * sizeof(double);
+    if (smem > 227 * 1024) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "Hamiltonian has too many strings for the energy kernel");
+    auto kern = k_vqe_energy_tiles<T>;
+    RQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RQ_TRY(grow(&b->d_part, &b->part_cap, ncirc * ntile * std::max<uint32_t>(1, b->nterms)));
+    int per_sm = 0;
+    RQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)threads, smem));
+    if (per_sm < 1) return rq::fail(RQ_ERR_CUDA, "energy kernel does not fit on an SM");
+    const int sms = rq::num_sms(b->device);
+    const unsigned grid = (unsigned)std::min<uint64_t>(ncirc * ntile, (uint64_t)sms * per_sm);
+    kern<<<grid, threads, smem, b->stream>>>((const V*)b->d_states, n, M, ncirc, b->d_groups, b->d_gofs, b->nterms,
+                                             b->d_terms, b->d_part);
+    RQ_CUDA(cudaGetLastError());
+    k_vqe_finalize<<<rq::grid_for(ncirc, TPB, sms), TPB, 0, b->stream>>>(b->d_part, ncirc, ntile, b->nterms, b->d_terms,
+                                                                         circ0, b->d_energy);
+    RQ_CUDA(cudaGetLastError());
+    return RQ_OK;
+}
 
 template <typename T>
 int vqe_wave(rq_vqe_batch* b, uint64_t ncirc, uint64_t circ0) {
@@ -1075,11 +1254,7 @@ int vqe_wave(rq_vqe_batch* b, uint64_t ncirc, uint64_t circ0) {
         kern<<<grid, threads, b->smem, b->stream>>>(d, ph, op, a);
         RQ_CUDA(cudaGetLastError());
     }
-    const unsigned ge = (unsigned)std::min<uint64_t>(ncirc, (uint64_t)sms * 8);
-    k_vqe_energy<T><<<ge, 256, 0, b->stream>>>((const V*)b->d_states, b->n, ncirc, circ0, b->d_groups, b->ngroups,
-                                                 b->d_terms, b->d_energy);
-    RQ_CUDA(cudaGetLastError());
-    return RQ_OK;
+    return vqe_energy<T>(b, ncirc, circ0);
 }
 
 }  // namespace
@@ -1120,34 +1295,45 @@ int rq_vqe_batch_create(uint32_t num_qubits, uint32_t depth, const double* coeff
         by_x[x].push_back({pm, {ny & 3u, coeffs[k]}});
     }
     auto re_ip = [](uint32_t k) { k &= 3u; return k == 0 ? 1.0 : (k == 2 ? -1.0 : 0.0); };
+    const uint32_t Mt = std::min<uint32_t>(num_qubits, 13);
+    const uint32_t ntile = 1u << (num_qubits - Mt);
     std::vector<VGroup> groups;
     std::vector<VTerm> terms;
-    for (auto& kv : by_x) {
-        const uint64_t x = kv.first;
-        const auto& list = kv.second;
-        for (size_t c0 = 0; c0 < list.size(); c0 += 8) {
-            VGroup G{};
-            G.x = x;
-            G.h = x ? 63 - __builtin_clzll(x) : 0;
-            G.t0 = (uint32_t)terms.size();
-            G.nt = (uint32_t)std::min<size_t>(8, list.size() - c0);
-            for (uint32_t k = 0; k < G.nt; ++k) {
-                const auto& t = list[c0 + k];
-                VTerm vt{};
-                vt.pmask = t.first;
-                const uint32_t ny = t.second.first;
-                const bool odd = x && (__builtin_popcountll(x & t.first) & 1);
-                vt.odd = odd ? 1u : 0u;
-                const double f = x == 0 ? re_ip(ny) : (odd ? 2.0 * re_ip(ny + 1) : 2.0 * re_ip(ny));
-                vt.factor = t.second.second * f;
-                terms.push_back(vt);
+    std::vector<uint32_t> gofs(ntile + 1, 0);
+    for (uint32_t t = 0; t < ntile; ++t) {
+        gofs[t] = (uint32_t)groups.size();
+        for (auto& kv : by_x) {
+            const uint64_t x = kv.first;
+            if ((uint32_t)(x >> Mt) != t) continue;
+            const auto& list = kv.second;
+            for (size_t c0 = 0; c0 < list.size(); c0 += 8) {
+                VGroup G{};
+                G.x = x;
+                G.h = x ? 63 - __builtin_clzll(x) : 0;
+                G.t0 = (uint32_t)terms.size();
+                G.nt = (uint32_t)std::min<size_t>(8, list.size() - c0);
+                for (uint32_t k = 0; k < G.nt; ++k) {
+                    const auto& tt = list[c0 + k];
+                    VTerm vt{};
+                    vt.pmask = tt.first;
+                    const uint32_t ny = tt.second.first;
+                    const bool odd = x && (__builtin_popcountll(x & tt.first) & 1);
+                    vt.odd = odd ? 1u : 0u;
+                    const double f = x == 0 ? re_ip(ny) : (odd ? 2.0 * re_ip(ny + 1) : 2.0 * re_ip(ny));
+                    vt.factor = tt.second.second * f;
+                    terms.push_back(vt);
+                }
+                groups.push_back(G);
             }
-            groups.push_back(G);
         }
     }
+    gofs[ntile] = (uint32_t)groups.size();
     b->ngroups = (uint32_t)groups.size();
+    b->nterms = (uint32_t)terms.size();
     if (groups.empty()) groups.push_back(VGroup{});
     if (terms.empty()) terms.push_back(VTerm{});
+    RQ_CUDA(cudaMalloc((void**)&b->d_gofs, gofs.size() * sizeof(uint32_t)));
+    RQ_CUDA(cudaMemcpy(b->d_gofs, gofs.data(), gofs.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
     RQ_CUDA(cudaMalloc((void**)&b->d_groups, groups.size() * sizeof(VGroup)));
     RQ_CUDA(cudaMemcpy(b->d_groups, groups.data(), groups.size() * sizeof(VGroup), cudaMemcpyHostToDevice));
     RQ_CUDA(cudaMalloc((void**)&b->d_terms, terms.size() * sizeof(VTerm)));
@@ -1247,7 +1433,8 @@ int rq_vqe_batch_destroy(rq_vqe_batch* b) {
     if (!b) return RQ_OK;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
-    void* ptrs[] = {b->prog, b->d_groups, b->d_terms, b->d_params, b->d_rot, b->d_states, b->d_energy};
+    void* ptrs[] = {b->prog, b->d_groups, b->d_terms, b->d_gofs, b->d_part, b->d_params, b->d_rot, b->d_states,
+                    b->d_energy};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
