@@ -353,6 +353,39 @@ RQ_API int rq_vqe_batch_last_ms(const rq_vqe_batch* b, float* ms);
 RQ_API int rq_vqe_batch_destroy(rq_vqe_batch* b);
 
 /* ------------------------------------------------------------------------ */
+/* BF16 tensor-core GEMM and the QAOA warm-start MLP (no reference            */
+/* counterpart: the reference starts QAOA from gamma = beta = 0.5,            */
+/* qaoa.rs:221-222)                                                           */
+/* ------------------------------------------------------------------------ */
+
+/* C (f32, M x N, row-major) = A (bf16 bits, M x K) * B (bf16 bits, N x K)^T on
+ * the tcgen05 tensor cores, FP32 accumulation.  Any M, N >= 1; K a positive
+ * multiple of 16. */
+RQ_API int rq_gemm_bf16(const uint16_t* A, const uint16_t* B, int32_t M, int32_t N, int32_t K, float* C);
+
+typedef struct rq_mlp rq_mlp;
+
+/* MLP in -> h1 -> h2 -> out with ReLU after both hidden layers; FP32 master
+ * parameters laid out flat as W1 [h1 x in], b1 [h1], W2 [h2 x h1], b2 [h2],
+ * W3 [out x h2], b3 [out] (weights row-major, one row per output unit);
+ * BF16 copies feed the tensor-core GEMMs; He-uniform init from Philox stream 6
+ * under `seed`.  h1, h2 multiples of 16. */
+RQ_API int rq_mlp_create(int32_t in, int32_t h1, int32_t h2, int32_t out, uint64_t seed, rq_mlp** res);
+RQ_API int rq_mlp_destroy(rq_mlp* m);
+RQ_API int rq_mlp_num_params(const rq_mlp* m, int64_t* n);
+RQ_API int rq_mlp_get_params(rq_mlp* m, float* params);
+RQ_API int rq_mlp_set_params(rq_mlp* m, const float* params);   /* also resets Adam */
+/* y (B x out) = MLP(x (B x in)), host buffers. */
+RQ_API int rq_mlp_forward(rq_mlp* m, const float* x, int32_t B, float* y);
+/* Mean-squared-error loss against t (B x out) and its gradient w.r.t. every
+ * parameter (flat, parameter layout). */
+RQ_API int rq_mlp_gradients(rq_mlp* m, const float* x, const float* t, int32_t B, float* loss, float* grads);
+/* `steps` Adam steps (lr, 0.9, 0.999, 1e-8) on minibatches of B rows taken in
+ * order (wrapping) from x (n x in), t (n x out); last step's loss out. */
+RQ_API int rq_mlp_train(rq_mlp* m, const float* x, const float* t, int32_t n, int32_t B, int32_t steps, float lr,
+                        float* last_loss);
+
+/* ------------------------------------------------------------------------ */
 /* host transfer (state_vector / amplitudes_mut / from_amplitudes)           */
 /* ------------------------------------------------------------------------ */
 

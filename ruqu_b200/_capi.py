@@ -81,6 +81,15 @@ SIGNATURES = {
     "rq_vqe_batch_run": (C.c_int, [_vp, _u32, _P(_dbl), _i32, _P(_dbl), _P(_dbl)]),
     "rq_vqe_batch_last_ms": (C.c_int, [_vp, _P(C.c_float)]),
     "rq_vqe_batch_destroy": (C.c_int, [_vp]),
+    "rq_gemm_bf16": (C.c_int, [_P(C.c_uint16), _P(C.c_uint16), _i32, _i32, _i32, _P(C.c_float)]),
+    "rq_mlp_create": (C.c_int, [_i32, _i32, _i32, _i32, _u64, _P(_vp)]),
+    "rq_mlp_destroy": (C.c_int, [_vp]),
+    "rq_mlp_num_params": (C.c_int, [_vp, _P(C.c_int64)]),
+    "rq_mlp_get_params": (C.c_int, [_vp, _P(C.c_float)]),
+    "rq_mlp_set_params": (C.c_int, [_vp, _P(C.c_float)]),
+    "rq_mlp_forward": (C.c_int, [_vp, _P(C.c_float), _i32, _P(C.c_float)]),
+    "rq_mlp_gradients": (C.c_int, [_vp, _P(C.c_float), _P(C.c_float), _i32, _P(C.c_float), _P(C.c_float)]),
+    "rq_mlp_train": (C.c_int, [_vp, _P(C.c_float), _P(C.c_float), _i32, _i32, _i32, C.c_float, _P(C.c_float)]),
     "rq_expectation_batch_noalloc": (C.c_int, [_vp, _u32, _i32, _P(RqPauliOp), _P(_u32), _u32, _P(_dbl), _vp]),
     "rq_state_normalize": (C.c_int, [_vp]),
     "rq_state_fidelity": (C.c_int, [_vp, _vp, _P(_dbl)]),

@@ -108,6 +108,9 @@ rq_plan_stats plan_stats(const rq_plan* p);
 bool plan_fits(const rq_plan* p, const rq_state* s);
 int apply_one_gate(rq_state* s, const rq_gate& g);   // per-gate kernels (rq_capi.cu)
 
+// ---- tensor-core GEMM (rq_mlp.cu) -------------------------------------------
+int mma_timeout_flag(int* out);
+
 }  // namespace rq
 
 // ---- device helpers -----------------------------------------------------------
