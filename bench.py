@@ -56,6 +56,9 @@ def _args():
     ap.add_argument("--qaoa-instances", type=int, default=2048)
     ap.add_argument("--no-vqe", action="store_true", help="skip the batched VQE leg")
     ap.add_argument("--vqe-sets", type=int, default=512)
+    ap.add_argument("--no-warm", action="store_true", help="skip the warm-start leg")
+    ap.add_argument("--warm-train", type=int, default=2048, help="training graphs for the warm start")
+    ap.add_argument("--warm-eval", type=int, default=256, help="held-out graphs for the warm start")
     return ap.parse_args()
 
 
@@ -234,6 +237,58 @@ def vqe_batch_leg(a, ws, rank, with_cpu):
     return res
 
 
+def warmstart_leg(a, ws, rank):
+    """Learned warm start vs linear ramp for QAOA p = 4 (scaled down from 200k training
+    pairs / 4096 held-out graphs to keep the default bench within minutes):
+    training: a.warm_train random 3-regular graphs, n in {12, 14, 16}, angles from the
+    plain batched optimizer (linear ramp + 200 Adam steps, parameter-shift gradients);
+    MLP 325 -> 256 -> 256 -> 8 trained on the tensor cores; evaluation: a.warm_eval
+    held-out graphs, n in {16, 18, 20}: plain = ramp + 200 steps (its final energy is
+    the target), warm = MLP angles + Adam until the target is met within 1e-5
+    relative (at most 200 steps).  solves/s = graphs / device time of each method."""
+    import numpy as np
+
+    from ruqu_b200 import rng, workloads
+    from ruqu_b200.batch import QaoaBatch
+    from ruqu_b200.warmstart import Mlp, features, linear_ramp
+    p, steps, lr = 4, 200, 0.05
+
+    def graphs(count, sizes, seed):
+        st = rng.Stream(seed, 2)
+        sel = rng.Stream(seed, 3)
+        return [(n, workloads.random_3regular_graph(n, st)) for n in
+                (sizes[sel.randint(len(sizes))] for _ in range(count))]
+
+    g0, b0 = linear_ramp(p)
+    t0 = time.perf_counter()
+    train = graphs(a.warm_train, (12, 14, 16), 21)
+    qb = QaoaBatch(train, p, "f32")
+    g, b, _, _ = qb.optimize(np.tile(g0, (len(train), 1)), np.tile(b0, (len(train), 1)), steps, lr)
+    gen_ms = qb.last_ms()
+    net = Mlp(seed=5)
+    x = features(train)
+    y = np.concatenate([g, b], axis=1).astype(np.float32)
+    loss = net.train(x, y, batch=256, steps=3000, lr=1e-3)
+    held = graphs(a.warm_eval, (16, 18, 20), 22)[rank::ws]
+    hb = QaoaBatch(held, p, "f32")
+    _, _, e_plain, _ = hb.optimize(np.tile(g0, (len(held), 1)), np.tile(b0, (len(held), 1)), steps, lr)
+    plain_ms = hb.last_ms()
+    pred = net.forward(features(held)).astype(np.float64)
+    _, _, e_warm, st = hb.optimize(pred[:, :p], pred[:, p:], steps, lr, target=e_plain, rtol=1e-5)
+    warm_ms = hb.last_ms()
+    reached = e_warm >= e_plain * (1 - 1e-5)
+    return {"workload": "QAOA p=4 warm start vs linear ramp: train %d graphs n in {12,14,16}, evaluate %d held-out "
+                        "graphs n in {16,18,20}; Adam 200 steps, parameter-shift gradients, f32 states"
+                        % (a.warm_train, a.warm_eval),
+            "train_data_device_ms": gen_ms, "mlp_final_loss": loss, "setup_s": time.perf_counter() - t0,
+            "plain_ms": plain_ms, "warm_ms": warm_ms,
+            "solves_per_s_plain": len(held) * ws / (plain_ms / 1e3),
+            "solves_per_s_warm": len(held) * ws / (warm_ms / 1e3),
+            "speedup": plain_ms / warm_ms, "reached_fraction": float(reached.mean()),
+            "mean_steps_warm": float(np.mean(st)), "steps_plain": steps,
+            "mean_rel_gap": float(np.mean((e_plain - e_warm) / e_plain))}
+
+
 def run_reference(a):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -383,6 +438,10 @@ def run_ours(a):
             vqe["device_ms_max_over_ranks"] = float(t.item())
             vqe["circuits_per_s"] = a.vqe_sets * 257 / (vqe["device_ms_max_over_ranks"] / 1e3)
 
+    warm = None
+    if not a.no_warm:
+        warm = warmstart_leg(a, ws, rank)
+
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         v, secs, cores, desc = cpu_baseline_sample(a, parallel=False)
@@ -410,6 +469,7 @@ def run_ours(a):
             "gpu_launches": a.steps * (1 + stats["launches"]),
             "qaoa_batch": qaoa,
             "vqe_batch": vqe,
+            "warm_start": warm,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

@@ -315,6 +315,18 @@ RQ_API int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gam
                              const double* betas, double* energies, uint32_t shots,
                              uint64_t base_seed, uint64_t* best_bits, uint32_t* best_cut);
 
+/* Batched run_qaoa (qaoa.rs:217-308) with Adam: for up to `steps` steps, every
+ * instance evaluates its energy and the 4p shifted energies of the
+ * parameter-shift rule of qaoa.rs:275-297 (theta_k +- pi/2), and Adam
+ * (0.9, 0.999, 1e-8, learning rate lr) climbs the expected cut; parameters,
+ * moments and updates are FP64 on the device.  gammas / betas (ninst x p) are
+ * the start and receive the result.  With a target (ninst values) an instance
+ * stops once its energy reaches target * (1 - rtol); steps_taken[i] = the
+ * step at which it did (or `steps`).  energies[i] = energy at the returned
+ * angles (at the stop). */
+RQ_API int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, double* betas,
+                                  const double* target, double rtol, double* energies, uint32_t* steps_taken);
+
 /* Final amplitudes of one circuit of the last run (2^n interleaved doubles);
  * only circuits of the last memory wave of that run are still held. */
 RQ_API int rq_qaoa_batch_state(rq_qaoa_batch* b, uint64_t circuit, double* interleaved);

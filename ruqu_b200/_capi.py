@@ -74,6 +74,7 @@ SIGNATURES = {
     "rq_qaoa_batch_create": (C.c_int, [_u32, _P(_u32), _P(_u32), _P(_u32), _u32, _i32, _P(_vp)]),
     "rq_qaoa_batch_run": (C.c_int, [_vp, _u32, _P(_dbl), _P(_dbl), _P(_dbl), _u32, _u64, _P(_u64), _P(_u32)]),
     "rq_qaoa_batch_state": (C.c_int, [_vp, _u64, _P(_dbl)]),
+    "rq_qaoa_batch_optimize": (C.c_int, [_vp, _u32, _dbl, _P(_dbl), _P(_dbl), _P(_dbl), _dbl, _P(_dbl), _P(_u32)]),
     "rq_qaoa_batch_last_ms": (C.c_int, [_vp, _P(C.c_float)]),
     "rq_qaoa_batch_set_state_budget": (C.c_int, [_vp, _u64]),
     "rq_qaoa_batch_destroy": (C.c_int, [_vp]),

@@ -70,6 +70,22 @@ class QaoaBatch:
             out["best_cut"] = bc.reshape(shape)
         return out
 
+    def optimize(self, gammas, betas, steps: int, lr: float = 0.05, target=None, rtol: float = 1e-5):
+        """Adam with the reference's parameter-shift gradients (qaoa.rs:275-297) on the GPU.
+        Returns (gammas, betas, energies, steps_taken)."""
+        g = np.ascontiguousarray(np.array(gammas, dtype=np.float64).reshape(len(self.graphs), self.p))
+        b = np.ascontiguousarray(np.array(betas, dtype=np.float64).reshape(len(self.graphs), self.p))
+        e = np.empty(len(self.graphs))
+        st = np.empty(len(self.graphs), dtype=np.uint32)
+        tp = None
+        if target is not None:
+            t = np.ascontiguousarray(target, dtype=np.float64)
+            tp = _dp(t)
+        check(lib.rq_qaoa_batch_optimize(self._h, int(steps), float(lr), _dp(g), _dp(b), tp, float(rtol), _dp(e),
+                                         _u32p(st)))
+        self.nsets = 1 + 4 * self.p
+        return g, b, e, st
+
     def state(self, circuit: int) -> np.ndarray:
         n = self.graphs[circuit // self.nsets][0]
         out = np.empty(2 << n)

@@ -824,6 +824,16 @@ int grow(P** ptr, size_t* cap, size_t need_elems) {
     return RQ_OK;
 }
 
+template <typename P>
+int dalloc_b(P** p, size_t n) {
+    cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(1, n) * sizeof(P));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return rq::fail(RQ_ERR_MEMORY_ALLOCATION, "memory allocation failed: need " + std::to_string(n * sizeof(P)) + " bytes");
+    }
+    return RQ_OK;
+}
+
 int grow_bytes(void** ptr, size_t* cap, size_t bytes) {
     if (*cap >= bytes) return RQ_OK;
     if (*ptr) cudaFree(*ptr);
@@ -1028,18 +1038,19 @@ int rq_qaoa_batch_destroy(rq_qaoa_batch* b) {
     return RQ_OK;
 }
 
-int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, const double* betas, double* energies,
-                      uint32_t shots, uint64_t base_seed, uint64_t* best_bits, uint32_t* best_cut) {
-    if (!b || !gammas || !betas || !energies) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
-    if (shots && (!best_bits || !best_cut)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null shot outputs");
-    if (nsets == 0) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "nsets must be >= 1");
-    RQ_CUDA(cudaSetDevice(b->device));
+}  // extern "C"
+
+namespace {
+
+// Run order of circuits: class-major, then instance, then parameter set.
+// Fills order / circ_inst, grows the per-run buffers, and (when gammas is not
+// null) uploads the angles in run order.
+int qaoa_prepare(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, const double* betas) {
     const uint64_t ncirc = (uint64_t)b->ninst * nsets;
     const uint32_t p = b->p;
-    // run order: class-major, within a class instance-major then set
     b->order.clear();
     std::vector<uint32_t> circ_inst;
-    std::vector<double> ang(2 * ncirc * p);
+    std::vector<double> ang(gammas ? 2 * ncirc * p : 0);
     for (auto& K : b->classes)
         for (uint32_t inst : K.insts)
             for (uint32_t s = 0; s < nsets; ++s) {
@@ -1047,10 +1058,11 @@ int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, co
                 const uint64_t pos = b->order.size();
                 b->order.push_back(user);
                 circ_inst.push_back(inst);
-                for (uint32_t l = 0; l < p; ++l) {
-                    ang[pos * p + l] = gammas[user * p + l];
-                    ang[ncirc * p + pos * p + l] = betas[user * p + l];
-                }
+                if (gammas)
+                    for (uint32_t l = 0; l < p; ++l) {
+                        ang[pos * p + l] = gammas[user * p + l];
+                        ang[ncirc * p + pos * p + l] = betas[user * p + l];
+                    }
             }
     size_t cap_ci = b->circ_cap;
     RQ_TRY(grow(&b->d_circ_inst, &cap_ci, ncirc));
@@ -1072,9 +1084,18 @@ int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, co
     b->circ_cap = std::max<size_t>(b->circ_cap, ncirc);
     RQ_CUDA(cudaMemcpyAsync(b->d_circ_inst, circ_inst.data(), ncirc * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
     RQ_CUDA(cudaMemcpyAsync(b->d_user, b->order.data(), ncirc * sizeof(uint64_t), cudaMemcpyHostToDevice, b->stream));
-    RQ_CUDA(cudaMemcpyAsync(b->d_ang, ang.data(), ang.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    if (gammas)
+        RQ_CUDA(cudaMemcpyAsync(b->d_ang, ang.data(), ang.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    // the pageable sources must outlive the copies
+    RQ_CUDA(cudaStreamSynchronize(b->stream));
+    return RQ_OK;
+}
+
+// tables + every class's sweeps (+ shots) for the angles in d_ang; energies land in d_energy (run order)
+int qaoa_launch(rq_qaoa_batch* b, uint32_t nsets, uint32_t shots, uint64_t base_seed) {
+    const uint64_t ncirc = (uint64_t)b->ninst * nsets;
+    const uint32_t p = b->p;
     const int sms = rq::num_sms(b->device);
-    RQ_CUDA(cudaEventRecord(b->ev0, b->stream));
     if (b->prec == RQ_F32)
         k_qaoa_tables<float><<<rq::grid_for(ncirc * p, TPB, sms), TPB, 0, b->stream>>>(
             b->d_ang, b->d_ang + ncirc * p, b->d_circ_inst, b->d_ne, ncirc, p, b->phs, (float*)b->d_rx, (float*)b->d_ph);
@@ -1104,6 +1125,87 @@ int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, co
         }
         pos += kc;
     }
+    return RQ_OK;
+}
+
+// parameter sets of one optimizer step: set 0 = theta, set 1+2k / 2+2k = theta_k +- pi/2
+// (the shift rule of run_qaoa, qaoa.rs:275-297); theta = (gamma_1..p, beta_1..p) per instance
+__global__ void k_qaoa_shift(const double* __restrict__ theta, uint32_t ninst, uint32_t p, uint32_t nsets,
+                             double* __restrict__ ang) {
+    const uint64_t ncirc = (uint64_t)ninst * nsets;
+    const uint64_t total = ncirc * p;
+    const double hp = 1.57079632679489661923;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = w / p;
+        const uint32_t l = (uint32_t)(w - c * p);
+        const uint64_t i = c / nsets;
+        const uint32_t s = (uint32_t)(c - i * nsets);
+        double g = theta[i * 2 * p + l], b = theta[i * 2 * p + p + l];
+        if (s > 0) {
+            const uint32_t k = (s - 1) / 2;
+            const double d = (s & 1) ? hp : -hp;
+            if (k == l) g += d;
+            if (k == p + l) b += d;
+        }
+        ang[w] = g;
+        ang[ncirc * p + w] = b;
+    }
+}
+
+// one Adam step (gradient ascent on the expected cut) per instance, FP64 on the device;
+// frozen once the target is met.  done[i] = 1 + the step at which the target was met.
+__global__ void k_qaoa_adam(const double* __restrict__ energy, uint32_t ninst, uint32_t p, uint32_t nsets,
+                            double* __restrict__ theta, double* __restrict__ m, double* __restrict__ v, double lr,
+                            uint32_t step, const double* __restrict__ target, double rtol, uint32_t* __restrict__ done,
+                            double* __restrict__ elast, int final_eval) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ninst; i += gridDim.x * blockDim.x) {
+        if (done[i]) continue;
+        const double* e = energy + (uint64_t)i * nsets;
+        elast[i] = e[0];
+        if (target && e[0] >= target[i] * (1.0 - rtol)) {
+            done[i] = step + 1;
+            continue;
+        }
+        if (final_eval) continue;
+        const double b1 = 0.9, b2 = 0.999, eps = 1e-8;
+        const double c1 = 1.0 - pow(b1, (double)(step + 1)), c2 = 1.0 - pow(b2, (double)(step + 1));
+        for (uint32_t k = 0; k < 2 * p; ++k) {
+            const double g = (e[1 + 2 * k] - e[2 + 2 * k]) / 2.0;
+            const uint64_t j = (uint64_t)i * 2 * p + k;
+            const double mm = b1 * m[j] + (1.0 - b1) * g;
+            const double vv = b2 * v[j] + (1.0 - b2) * g * g;
+            m[j] = mm;
+            v[j] = vv;
+            theta[j] += lr * (mm / c1) / (sqrt(vv / c2) + eps);
+        }
+    }
+}
+
+__global__ void k_count_active(const uint32_t* __restrict__ done, uint32_t n, uint32_t* __restrict__ out) {
+    __shared__ uint32_t s;
+    if (threadIdx.x == 0) s = 0;
+    __syncthreads();
+    uint32_t c = 0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) c += done[i] == 0;
+    atomicAdd(&s, c);
+    __syncthreads();
+    if (threadIdx.x == 0) *out = s;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, const double* betas, double* energies,
+                      uint32_t shots, uint64_t base_seed, uint64_t* best_bits, uint32_t* best_cut) {
+    if (!b || !gammas || !betas || !energies) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (shots && (!best_bits || !best_cut)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null shot outputs");
+    if (nsets == 0) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "nsets must be >= 1");
+    RQ_CUDA(cudaSetDevice(b->device));
+    const uint64_t ncirc = (uint64_t)b->ninst * nsets;
+    RQ_TRY(qaoa_prepare(b, nsets, gammas, betas));
+    RQ_CUDA(cudaEventRecord(b->ev0, b->stream));
+    RQ_TRY(qaoa_launch(b, nsets, shots, base_seed));
     RQ_CUDA(cudaEventRecord(b->ev1, b->stream));
     std::vector<double> e(ncirc);
     RQ_CUDA(cudaMemcpyAsync(e.data(), b->d_energy, ncirc * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
@@ -1126,6 +1228,90 @@ int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, co
         }
     }
     b->last_nsets = nsets;
+    return RQ_OK;
+}
+
+int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, double* betas,
+                           const double* target, double rtol, double* energies, uint32_t* steps_taken) {
+    if (!b || !gammas || !betas || !energies || !steps_taken) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    RQ_CUDA(cudaSetDevice(b->device));
+    const uint32_t p = b->p, P2 = 2 * p, nsets = 1 + 2 * P2, ninst = b->ninst;
+    RQ_TRY(qaoa_prepare(b, nsets, nullptr, nullptr));
+    // instances in run order (class-major), angles as theta = (gammas, betas) per instance
+    std::vector<uint32_t> inst_order;
+    for (auto& K : b->classes)
+        for (uint32_t inst : K.insts) inst_order.push_back(inst);
+    std::vector<double> th((size_t)ninst * P2), tg(ninst);
+    for (uint32_t r = 0; r < ninst; ++r) {
+        const uint32_t i = inst_order[r];
+        for (uint32_t l = 0; l < p; ++l) {
+            th[(size_t)r * P2 + l] = gammas[(size_t)i * p + l];
+            th[(size_t)r * P2 + p + l] = betas[(size_t)i * p + l];
+        }
+        if (target) tg[r] = target[i];
+    }
+    double *d_th = nullptr, *d_m = nullptr, *d_v = nullptr, *d_tg = nullptr, *d_el = nullptr;
+    uint32_t *d_done = nullptr, *d_active = nullptr;
+    auto cleanup = [&]() {
+        void* q[] = {d_th, d_m, d_v, d_tg, d_el, d_done, d_active};
+        for (void* x : q) if (x) cudaFree(x);
+    };
+    int rc = RQ_OK;
+    if (rc == RQ_OK) rc = dalloc_b(&d_th, th.size());
+    if (rc == RQ_OK) rc = dalloc_b(&d_m, th.size());
+    if (rc == RQ_OK) rc = dalloc_b(&d_v, th.size());
+    if (rc == RQ_OK) rc = dalloc_b(&d_tg, ninst);
+    if (rc == RQ_OK) rc = dalloc_b(&d_el, ninst);
+    if (rc == RQ_OK) rc = dalloc_b(&d_done, ninst);
+    if (rc == RQ_OK) rc = dalloc_b(&d_active, 1);
+    if (rc != RQ_OK) { cleanup(); return rc; }
+    cudaMemcpyAsync(d_th, th.data(), th.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+    cudaMemsetAsync(d_m, 0, th.size() * sizeof(double), b->stream);
+    cudaMemsetAsync(d_v, 0, th.size() * sizeof(double), b->stream);
+    cudaMemsetAsync(d_done, 0, ninst * sizeof(uint32_t), b->stream);
+    if (target) cudaMemcpyAsync(d_tg, tg.data(), ninst * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+    const int sms = rq::num_sms(b->device);
+    const uint64_t ncirc = (uint64_t)ninst * nsets;
+    cudaEventRecord(b->ev0, b->stream);
+    for (uint32_t step = 0; step <= steps && rc == RQ_OK; ++step) {
+        k_qaoa_shift<<<rq::grid_for(ncirc * p, TPB, sms), TPB, 0, b->stream>>>(d_th, ninst, p, nsets, b->d_ang);
+        rc = qaoa_launch(b, nsets, 0, 0);
+        if (rc != RQ_OK) break;
+        k_qaoa_adam<<<rq::grid_for(ninst, TPB, sms), TPB, 0, b->stream>>>(b->d_energy, ninst, p, nsets, d_th, d_m, d_v, lr,
+                                                                       step, target ? d_tg : nullptr, rtol, d_done, d_el,
+                                                                       step == steps ? 1 : 0);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { rc = rq::cuda_fail(e, "optimizer kernels"); break; }
+        if (target && (step % 5 == 4)) {   // stop once every instance has met its target
+            uint32_t active = 1;
+            k_count_active<<<1, 256, 0, b->stream>>>(d_done, ninst, d_active);
+            cudaMemcpyAsync(&active, d_active, sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
+            cudaStreamSynchronize(b->stream);
+            if (active == 0) break;
+        }
+    }
+    cudaEventRecord(b->ev1, b->stream);
+    std::vector<double> el(ninst);
+    std::vector<uint32_t> dn(ninst);
+    if (rc == RQ_OK) {
+        cudaMemcpyAsync(th.data(), d_th, th.size() * sizeof(double), cudaMemcpyDeviceToHost, b->stream);
+        cudaMemcpyAsync(el.data(), d_el, ninst * sizeof(double), cudaMemcpyDeviceToHost, b->stream);
+        cudaMemcpyAsync(dn.data(), d_done, ninst * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
+        cudaError_t e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) rc = rq::cuda_fail(e, "optimizer");
+        cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
+    }
+    cleanup();
+    RQ_TRY(rc);
+    for (uint32_t r = 0; r < ninst; ++r) {
+        const uint32_t i = inst_order[r];
+        for (uint32_t l = 0; l < p; ++l) {
+            gammas[(size_t)i * p + l] = th[(size_t)r * P2 + l];
+            betas[(size_t)i * p + l] = th[(size_t)r * P2 + p + l];
+        }
+        energies[i] = el[r];
+        steps_taken[i] = dn[r] ? dn[r] - 1 : steps;
+    }
     return RQ_OK;
 }
 

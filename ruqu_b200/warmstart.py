@@ -82,3 +82,13 @@ class Mlp:
         if h is not None:
             lib.rq_mlp_destroy(h)
             self._h = None
+
+
+def linear_ramp(p: int, delta: float = 0.75):
+    """Plain start: gamma_l = (l - 1/2)/p * delta, beta_l = (1 - (l - 1/2)/p) * delta, l = 1..p."""
+    f = (np.arange(1, p + 1) - 0.5) / p
+    return f * delta, (1.0 - f) * delta
+
+
+def features(graphs) -> np.ndarray:
+    return np.stack([graph_features(n, e) for n, e in graphs]).astype(np.float32)
