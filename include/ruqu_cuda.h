@@ -315,17 +315,37 @@ RQ_API int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gam
                              const double* betas, double* energies, uint32_t shots,
                              uint64_t base_seed, uint64_t* best_bits, uint32_t* best_cut);
 
-/* Batched run_qaoa (qaoa.rs:217-308) with Adam: for up to `steps` steps, every
- * instance evaluates its energy and the 4p shifted energies of the
- * parameter-shift rule of qaoa.rs:275-297 (theta_k +- pi/2), and Adam
+/* Gradient rules of rq_qaoa_batch_optimize.
+ * RQ_QAOA_GRAD_ADJOINT: exact dE/dgamma_l, dE/dbeta_l by one backward pass
+ *   (2 Im <lambda|G|psi> per gate generator G, lambda = C psi carried back).
+ * RQ_QAOA_GRAD_SHIFT: the rule of run_qaoa (qaoa.rs:275-297), (E(theta_k +
+ *   pi/2) - E(theta_k - pi/2)) / 2 with the shift applied to a whole layer's
+ *   angle.  For unit edge weights it is zero up to rounding: shifting every
+ *   Rzz(2 gamma) of a layer by pi/2 multiplies the state by a Pauli string
+ *   (up to phase) that cancels between the two evaluations, and likewise for
+ *   the Rx(2 beta) of a layer.  Kept to reproduce the reference's rule. */
+#define RQ_QAOA_GRAD_ADJOINT 0
+#define RQ_QAOA_GRAD_SHIFT 1
+
+/* Energies and exact gradients of ninst circuits (one per graph):
+ * gammas / betas are ninst x p; energies[i] as rq_qaoa_batch_run;
+ * gradients[i*2p + l] = dE/dgamma_l, gradients[i*2p + p + l] = dE/dbeta_l,
+ * reduced in FP64.  No reference counterpart (run_qaoa only has the shift
+ * rule). */
+RQ_API int rq_qaoa_batch_gradient(rq_qaoa_batch* b, const double* gammas, const double* betas,
+                                  double* energies, double* gradients);
+
+/* Batched run_qaoa (qaoa.rs:217-308) with Adam: for up to `steps` steps every
+ * instance takes its gradient by `gradient` (RQ_QAOA_GRAD_*) and Adam
  * (0.9, 0.999, 1e-8, learning rate lr) climbs the expected cut; parameters,
  * moments and updates are FP64 on the device.  gammas / betas (ninst x p) are
  * the start and receive the result.  With a target (ninst values) an instance
- * stops once its energy reaches target * (1 - rtol); steps_taken[i] = the
- * step at which it did (or `steps`).  energies[i] = energy at the returned
- * angles (at the stop). */
+ * stops once its energy reaches target * (1 - rtol) and leaves the following
+ * steps' launches; steps_taken[i] = the step at which it did (or `steps`).
+ * energies[i] = energy at the returned angles (at the stop). */
 RQ_API int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, double* betas,
-                                  const double* target, double rtol, double* energies, uint32_t* steps_taken);
+                                  const double* target, double rtol, int32_t gradient, double* energies,
+                                  uint32_t* steps_taken);
 
 /* Final amplitudes of one circuit of the last run (2^n interleaved doubles);
  * only circuits of the last memory wave of that run are still held. */

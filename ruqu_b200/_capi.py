@@ -12,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libruqu_cuda.so")
 
 RQ_F32, RQ_F64 = 0, 1
+RQ_QAOA_GRAD_ADJOINT, RQ_QAOA_GRAD_SHIFT = 0, 1
 RQ_EXEC_AUTO, RQ_EXEC_PER_GATE, RQ_EXEC_SWEEP = 0, 1, 2
 
 (RQ_OK, RQ_ERR_QUBIT_LIMIT_EXCEEDED, RQ_ERR_INVALID_QUBIT_INDEX, RQ_ERR_MEMORY_ALLOCATION,
@@ -74,7 +75,9 @@ SIGNATURES = {
     "rq_qaoa_batch_create": (C.c_int, [_u32, _P(_u32), _P(_u32), _P(_u32), _u32, _i32, _P(_vp)]),
     "rq_qaoa_batch_run": (C.c_int, [_vp, _u32, _P(_dbl), _P(_dbl), _P(_dbl), _u32, _u64, _P(_u64), _P(_u32)]),
     "rq_qaoa_batch_state": (C.c_int, [_vp, _u64, _P(_dbl)]),
-    "rq_qaoa_batch_optimize": (C.c_int, [_vp, _u32, _dbl, _P(_dbl), _P(_dbl), _P(_dbl), _dbl, _P(_dbl), _P(_u32)]),
+    "rq_qaoa_batch_optimize": (C.c_int, [_vp, _u32, _dbl, _P(_dbl), _P(_dbl), _P(_dbl), _dbl, C.c_int32, _P(_dbl),
+                                         _P(_u32)]),
+    "rq_qaoa_batch_gradient": (C.c_int, [_vp, _P(_dbl), _P(_dbl), _P(_dbl), _P(_dbl)]),
     "rq_qaoa_batch_last_ms": (C.c_int, [_vp, _P(C.c_float)]),
     "rq_qaoa_batch_set_state_budget": (C.c_int, [_vp, _u64]),
     "rq_qaoa_batch_destroy": (C.c_int, [_vp]),

@@ -11,6 +11,7 @@ import ctypes as C
 
 import numpy as np
 
+from . import _capi
 from ._capi import RQ_F32, RQ_F64, lib
 from .error import check
 
@@ -70,9 +71,23 @@ class QaoaBatch:
             out["best_cut"] = bc.reshape(shape)
         return out
 
-    def optimize(self, gammas, betas, steps: int, lr: float = 0.05, target=None, rtol: float = 1e-5):
-        """Adam with the reference's parameter-shift gradients (qaoa.rs:275-297) on the GPU.
+    def gradient(self, gammas, betas):
+        """Energies and exact gradients (ninst x 2p: d/dgamma_1..p, then d/dbeta_1..p) of one
+        circuit per graph, by the adjoint pass on the GPU."""
+        g = np.ascontiguousarray(np.array(gammas, dtype=np.float64).reshape(len(self.graphs), self.p))
+        b = np.ascontiguousarray(np.array(betas, dtype=np.float64).reshape(len(self.graphs), self.p))
+        e = np.empty(len(self.graphs))
+        grad = np.empty((len(self.graphs), 2 * self.p))
+        check(lib.rq_qaoa_batch_gradient(self._h, _dp(g), _dp(b), _dp(e), _dp(grad)))
+        self.nsets = 1
+        return e, grad
+
+    def optimize(self, gammas, betas, steps: int, lr: float = 0.05, target=None, rtol: float = 1e-5,
+                 gradient: str = "adjoint"):
+        """Adam on the GPU.  gradient = "adjoint" (exact gradients) or "shift" (the rule of
+        run_qaoa, qaoa.rs:275-297, zero up to rounding for unit edge weights).
         Returns (gammas, betas, energies, steps_taken)."""
+        mode = {"adjoint": _capi.RQ_QAOA_GRAD_ADJOINT, "shift": _capi.RQ_QAOA_GRAD_SHIFT}[gradient]
         g = np.ascontiguousarray(np.array(gammas, dtype=np.float64).reshape(len(self.graphs), self.p))
         b = np.ascontiguousarray(np.array(betas, dtype=np.float64).reshape(len(self.graphs), self.p))
         e = np.empty(len(self.graphs))
@@ -81,9 +96,9 @@ class QaoaBatch:
         if target is not None:
             t = np.ascontiguousarray(target, dtype=np.float64)
             tp = _dp(t)
-        check(lib.rq_qaoa_batch_optimize(self._h, int(steps), float(lr), _dp(g), _dp(b), tp, float(rtol), _dp(e),
-                                         _u32p(st)))
-        self.nsets = 1 + 4 * self.p
+        check(lib.rq_qaoa_batch_optimize(self._h, int(steps), float(lr), _dp(g), _dp(b), tp, float(rtol), mode,
+                                         _dp(e), _u32p(st)))
+        self.nsets = 1 if gradient == "adjoint" else 1 + 4 * self.p
         return g, b, e, st
 
     def state(self, circuit: int) -> np.ndarray:

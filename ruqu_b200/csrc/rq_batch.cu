@@ -66,6 +66,8 @@ struct QArgs {
     uint32_t p, phs;
     double* epart;                 // [wave circuit][ntiles]
     T amp0;                        // 2^(-n/2)
+    typename C2<T>::t* lam;        // adjoint sweeps: lambda of circuit c at lam + c * 2^n
+    double* gpart;                 // adjoint sweeps: [wave circuit][ntiles][2p] gradient partials
 };
 
 // cut(x) for the register amplitudes of one thread: x = U | deposit(i).
@@ -375,6 +377,231 @@ __global__ void k_energy_finalize(const double* __restrict__ epart, uint64_t nci
         double s = 0.0;
         for (uint64_t t = 0; t < ntiles; ++t) s += epart[c * ntiles + t];
         energies[circ0 + c] = s;
+    }
+}
+
+// ---- exact gradients: one adjoint sweep pass per circuit ------------------
+//
+// With psi = the final state and lambda = C psi (C = diag(cut(x))), the
+// derivative of E = <psi|C|psi> by a parameter theta of a gate exp(-i theta G)
+// is 2 Im <lambda_k|G|psi_k>, both vectors taken at that gate and carried
+// backwards by applying each gate's inverse to both.  Per QAOA layer l (in
+// reverse): dE/dbeta_l = sum_q 2 Im <lambda|X_q|psi> (Rx(2 beta) =
+// exp(-i beta X); X_q commutes with every Rx of the layer, so the term is
+// taken when Rx_q is undone), then dE/dgamma_l = 2 Im <lambda|G|psi> with
+// G = diag(|E| - 2 cut(x)) (the product of the layer's Rzz(2 gamma) is
+// exp(-i gamma G)).  Each thread holds the same 2^RB indices of psi and
+// lambda; the per-op partial sums are FP64, reduced per warp by shuffles
+// (fixed order) into per-warp rows of shared memory, and per tile into
+// gpart -- deterministic for a given launch shape.
+template <int K, int NR, typename V>
+__device__ __forceinline__ double im_x_overlap(const V* p, const V* l) {
+    double acc = 0.0;
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+        if (i & (1 << K)) continue;
+        const int j = i | (1 << K);
+        // Im(conj(l_i) p_j + conj(l_j) p_i)
+        acc += (double)(l[i].x * p[j].y - l[i].y * p[j].x) + (double)(l[j].x * p[i].y - l[j].y * p[i].x);
+    }
+    return acc;
+}
+
+template <int NR, typename V>
+__device__ __forceinline__ double dispatch_im_x(int k, const V* p, const V* l) {
+    switch (k) {
+        case 0: return im_x_overlap<0, NR>(p, l);
+        case 1: return im_x_overlap<1, NR>(p, l);
+        case 2: return im_x_overlap<2, NR>(p, l);
+        case 3: if constexpr (NR > 8) return im_x_overlap<3, NR>(p, l); break;
+        case 4: if constexpr (NR > 16) return im_x_overlap<4, NR>(p, l); break;
+        default: break;
+    }
+    return 0.0;
+}
+
+template <typename T, int RB>
+__global__ void __launch_bounds__(512, 1) k_batch_adjoint(const SweepDesc d, const PhaseDesc* __restrict__ phases,
+                                                        const SwOp* __restrict__ ops, QArgs<T> a) {
+    using V = typename C2<T>::t;
+    using VV = typename Vec16b<T>::t;
+    constexpr int NR = 1 << RB;
+    constexpr int EPV = Vec16b<T>::EPV;
+    constexpr int VPT = NR / EPV;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t tile_elems = 1u << d.m;
+    V* smp = reinterpret_cast<V*>(smem_raw);
+    V* sml = smp + tile_elems;
+    double* gw = reinterpret_cast<double*>(sml + tile_elems);   // [group][2p]
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t T_ = blockDim.x;
+    const bool small = T_ < 32;                  // tiny blocks: one row per thread, no shuffles
+    const uint32_t ngroup = small ? T_ : (T_ >> 5);
+    const uint32_t grp = small ? tid : (tid >> 5);
+    const uint32_t lane = tid & 31u;
+    const uint32_t P2 = 2 * a.p;
+    const uint64_t cmask = (1ull << d.c) - 1;
+    uint64_t dep_tid = 0;
+    {
+        uint64_t x = (uint64_t)tid * EPV;
+        dep_tid = x & cmask;
+        for (uint32_t b = d.c; b < d.m; ++b)
+            if ((x >> b) & 1ull) dep_tid |= 1ull << d.local_global[b];
+    }
+    const uint32_t stid = swzb<T>(tid * EPV);
+    const uint64_t nwork = a.ncirc * a.ntiles;
+    const uint64_t nstate = 1ull << d.n;
+    const bool initl = (d.flags & SWEEP_INIT_LAMBDA) != 0;
+
+    auto flush = [&](double v, uint32_t idx) {
+        if (!small) {
+            v = warp_sum_d(v);
+            if (lane == 0) gw[grp * P2 + idx] += v;
+        } else {
+            gw[grp * P2 + idx] += v;
+        }
+    };
+
+    for (uint64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const uint64_t circ = w / a.ntiles, tile = w - circ * a.ntiles;
+        const uint64_t gcirc = a.circ0 + circ;
+        V* psi = a.amps + circ * nstate;
+        V* lam = a.lam + circ * nstate;
+        const uint32_t inst = a.circ_inst[gcirc];
+        const uint8_t* edges = a.edges + 2 * (size_t)a.eoff[inst];
+        const uint32_t ne = a.ne[inst];
+        uint64_t base = 0;
+        for (uint32_t b = 0; b < d.nonlocal_count; ++b)
+            if ((tile >> b) & 1ull) base |= 1ull << d.nonlocal[b];
+        for (uint32_t k = tid; k < ngroup * P2; k += T_) gw[k] = 0.0;
+
+#pragma unroll 1
+        for (int j0 = 0; j0 < VPT; j0 += 4) {
+            VV v[4], u[4];
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                const uint64_t g = base | dep_tid | d.gj[j0 + jj];
+                v[jj] = __ldcs(reinterpret_cast<const VV*>(psi + g));
+                if (!initl) u[jj] = __ldcs(reinterpret_cast<const VV*>(lam + g));
+            }
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                const uint32_t se = stid ^ d.sgj[j0 + jj];
+                if constexpr (EPV == 2) {
+                    smp[se] = make_float2(v[jj].x, v[jj].y);
+                    smp[se ^ 1u] = make_float2(v[jj].z, v[jj].w);
+                    if (!initl) {
+                        sml[se] = make_float2(u[jj].x, u[jj].y);
+                        sml[se ^ 1u] = make_float2(u[jj].z, u[jj].w);
+                    }
+                } else {
+                    smp[se] = *reinterpret_cast<V*>(&v[jj]);
+                    if (!initl) sml[se] = *reinterpret_cast<V*>(&u[jj]);
+                }
+            }
+        }
+        __syncthreads();
+
+        for (uint32_t p = d.phase_begin; p < d.phase_end; ++p) {
+            const PhaseDesc& ph = phases[p];
+            uint32_t ebase = 0;
+            uint64_t U = base;
+            for (uint32_t b = 0; b < ph.nt; ++b)
+                if ((tid >> b) & 1u) {
+                    ebase |= 1u << ph.tbit_local[b];
+                    U |= 1ull << ph.tbit_global[b];
+                }
+            const uint32_t sb = swzb<T>(ebase);
+            uint64_t slotmask = 0;
+#pragma unroll
+            for (int s = 0; s < RB; ++s) slotmask |= 1ull << ph.slot_global[s];
+            V rp[NR], rl[NR];
+#pragma unroll
+            for (int i = 0; i < NR; ++i) rp[i] = smp[sb ^ ph.slut[i]];
+            if (initl && p == d.phase_begin) {
+                CutPlan<RB> cp;
+                cut_plan<RB>(cp, edges, ne, U, slotmask);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) {
+                    const T c = (T)cut_of<RB>(cp, i);
+                    rl[i].x = c * rp[i].x;
+                    rl[i].y = c * rp[i].y;
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < NR; ++i) rl[i] = sml[sb ^ ph.slut[i]];
+            }
+            for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
+                const SwOp op = ops[o];
+                if (op.type == OP_RXP) {
+                    const T* r = a.rot + ((size_t)gcirc * a.nparam + op.param) * 2;
+                    flush(2.0 * dispatch_im_x<NR>(op.k0, rp, rl), a.p + op.param);
+                    dispatch_rx<NR>(op.k0, rp, r[0], -r[1]);
+                    dispatch_rx<NR>(op.k0, rl, r[0], -r[1]);
+                } else if (op.type == OP_CPH) {
+                    CutPlan<RB> cp;
+                    cut_plan<RB>(cp, edges, ne, U, slotmask);
+                    const T* tab = a.ph + ((size_t)gcirc * a.p + op.param) * a.phs * 2;
+                    double acc = 0.0;
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) {
+                        const int c = cut_of<RB>(cp, i);
+                        const T gdiag = (T)((int)ne - 2 * c);
+                        acc += (double)(gdiag * (rl[i].x * rp[i].y - rl[i].y * rp[i].x));
+                        rp[i] = cmulv(rp[i], tab[2 * c], -tab[2 * c + 1]);
+                        rl[i] = cmulv(rl[i], tab[2 * c], -tab[2 * c + 1]);
+                    }
+                    flush(2.0 * acc, op.param);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < NR; ++i) {
+                smp[sb ^ ph.slut[i]] = rp[i];
+                sml[sb ^ ph.slut[i]] = rl[i];
+            }
+            __syncthreads();
+        }
+
+        for (uint32_t k = tid; k < P2; k += T_) {
+            double s = 0.0;
+            for (uint32_t g = 0; g < ngroup; ++g) s += gw[g * P2 + k];
+            a.gpart[(circ * a.ntiles + tile) * P2 + k] = s;
+        }
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) {
+            const uint32_t se = stid ^ d.sgj[j];
+            const uint64_t g = base | dep_tid | d.gj[j];
+            VV v, u;
+            if constexpr (EPV == 2) {
+                float2 x = smp[se], y = smp[se ^ 1u];
+                v = make_float4(x.x, x.y, y.x, y.y);
+                x = sml[se];
+                y = sml[se ^ 1u];
+                u = make_float4(x.x, x.y, y.x, y.y);
+            } else {
+                V x = smp[se];
+                v = *reinterpret_cast<VV*>(&x);
+                x = sml[se];
+                u = *reinterpret_cast<VV*>(&x);
+            }
+            __stcs(reinterpret_cast<VV*>(psi + g), v);
+            __stcs(reinterpret_cast<VV*>(lam + g), u);
+        }
+        __syncthreads();
+    }
+}
+
+// grad[(circ0 + c) * P2 + k] += sum over the circuit's tile partials (fixed order)
+__global__ void k_grad_finalize(const double* __restrict__ gpart, uint64_t ncirc, uint64_t ntiles, uint32_t P2,
+                                uint64_t circ0, double* __restrict__ grad) {
+    const uint64_t total = ncirc * P2;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = w / P2;
+        const uint32_t k = (uint32_t)(w - c * P2);
+        double s = 0.0;
+        for (uint64_t t = 0; t < ntiles; ++t) s += gpart[(c * ntiles + t) * P2 + k];
+        grad[(circ0 + c) * P2 + k] += s;
     }
 }
 
@@ -765,6 +992,12 @@ struct QClass {
     size_t off_ops = 0;
     size_t smem = 0;
     uint64_t ntiles = 0;
+    // the adjoint program (exact gradients): both states' tiles in shared memory
+    uint32_t am = 0;
+    std::vector<SweepDesc> adescs;
+    unsigned char* aprog = nullptr;
+    size_t aoff_ops = 0;
+    uint64_t antiles = 0;
 };
 
 struct rq_qaoa_batch {
@@ -795,6 +1028,12 @@ struct rq_qaoa_batch {
     size_t epart_cap = 0;                  // doubles
     double* d_tree = nullptr;
     size_t tree_cap = 0;                   // doubles
+    void* d_lam = nullptr;                 // adjoint wave buffer (lambda)
+    size_t lam_cap = 0;                    // bytes
+    double* d_gpart = nullptr;             // adjoint per-tile gradient partials
+    size_t gpart_cap = 0;                  // doubles
+    double* d_grad = nullptr;              // [circuit][2p] gradients of the last adjoint run
+    size_t grad_cap = 0;                   // doubles
     std::vector<uint64_t> order;           // run-order position -> user circuit index
     // last run: which wave holds which circuits (for rq_qaoa_batch_state)
     uint32_t last_nsets = 0;
@@ -886,6 +1125,52 @@ int launch_class(rq_qaoa_batch* b, QClass& K, uint64_t ncirc, uint64_t circ0, vo
     k_energy_finalize<<<rq::grid_for(ncirc, TPB, rq::num_sms(b->device)), TPB, 0, b->stream>>>(
         b->d_epart, ncirc, K.ntiles, circ0, b->d_energy);
     RQ_CUDA(cudaGetLastError());
+    return RQ_OK;
+}
+
+// backward pass of one wave: psi (left by the forward sweeps) and lambda through the
+// adjoint program; per-circuit gradients accumulate into d_grad (zeroed by the caller)
+template <typename T>
+int adjoint_class(rq_qaoa_batch* b, QClass& K, uint64_t ncirc, uint64_t circ0, void* states, void* lam) {
+    using V = typename C2<T>::t;
+    constexpr int RBc = std::is_same<T, float>::value ? 4 : 3;
+    const uint32_t P2 = 2 * b->p;
+    QArgs<T> a{};
+    a.amps = (V*)states;
+    a.lam = (V*)lam;
+    a.ncirc = ncirc;
+    a.ntiles = K.antiles;
+    a.circ0 = circ0;
+    a.circ_inst = b->d_circ_inst;
+    a.edges = b->d_edges;
+    a.eoff = b->d_eoff;
+    a.ne = b->d_ne;
+    a.rot = (const T*)b->d_rx;
+    a.nparam = b->p;
+    a.ph = (const T*)b->d_ph;
+    a.p = b->p;
+    a.phs = b->phs;
+    a.gpart = b->d_gpart;
+    const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(K.aprog);
+    const SwOp* op = reinterpret_cast<const SwOp*>(K.aprog + K.aoff_ops);
+    auto kern = k_batch_adjoint<T, RBc>;
+    const unsigned threads = 1u << (K.am - RBc);
+    const unsigned ngroup = threads < 32 ? threads : threads / 32;
+    const size_t smem = 2 * ((size_t)1 << K.am) * sizeof(V) + (size_t)ngroup * P2 * sizeof(double);
+    RQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    RQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)threads, smem));
+    if (per_sm < 1) return rq::fail(RQ_ERR_CUDA, "adjoint sweep kernel does not fit on an SM");
+    const uint64_t work = ncirc * K.antiles;
+    const unsigned grid = (unsigned)std::min<uint64_t>(work, (uint64_t)rq::num_sms(b->device) * per_sm);
+    const int sms = rq::num_sms(b->device);
+    for (const auto& d : K.adescs) {
+        kern<<<grid, threads, smem, b->stream>>>(d, ph, op, a);
+        RQ_CUDA(cudaGetLastError());
+        k_grad_finalize<<<rq::grid_for(ncirc * P2, TPB, sms), TPB, 0, b->stream>>>(b->d_gpart, ncirc, K.antiles, P2,
+                                                                                 circ0, b->d_grad);
+        RQ_CUDA(cudaGetLastError());
+    }
     return RQ_OK;
 }
 
@@ -1007,6 +1292,41 @@ int rq_qaoa_batch_create(uint32_t ninst, const uint32_t* num_nodes, const uint32
         std::memcpy(host.data() + K.off_ops, ops.data(), ops.size() * sizeof(SwOp));
         RQ_CUDA(cudaMalloc((void**)&K.prog, total));
         RQ_CUDA(cudaMemcpy(K.prog, host.data(), total, cudaMemcpyHostToDevice));
+        {
+            // adjoint: per layer in reverse, Rx^-1 on every qubit, then the inverse cost phase
+            const uint32_t arb = precision == RQ_F32 ? 4 : 3;
+            K.am = std::min(K.n, mloc);
+            K.antiles = 1ull << (K.n - K.am);
+            const uint32_t ac = std::min<uint32_t>(K.am, 5);
+            std::vector<PGate> ga;
+            for (uint32_t l = p; l-- > 0;) {
+                for (uint32_t q = 0; q < K.n; ++q) {
+                    PGate rx{};
+                    rx.type = OP_RXP;
+                    rx.q0 = q;
+                    rx.param = (uint16_t)l;
+                    ga.push_back(rx);
+                }
+                PGate ph{};
+                ph.type = OP_CPH;
+                ph.param = (uint16_t)l;
+                ph.span = (K.n >= 64) ? ~0ull : ((1ull << K.n) - 1);
+                ga.push_back(ph);
+            }
+            auto asw = plan_sweeps(ga, K.n, K.am, ac);
+            std::vector<PhaseDesc> aph;
+            std::vector<SwOp> aops;
+            std::vector<double> amats;
+            build_program(asw, K.n, K.am, ac, arb, precision == RQ_F32 ? 2 : 1, K.adescs, aph, aops, amats);
+            K.adescs.front().flags |= SWEEP_INIT_LAMBDA;
+            K.aoff_ops = (aph.size() * sizeof(PhaseDesc) + 255) & ~size_t(255);
+            const size_t atotal = K.aoff_ops + aops.size() * sizeof(SwOp);
+            std::vector<unsigned char> ah(atotal);
+            std::memcpy(ah.data(), aph.data(), aph.size() * sizeof(PhaseDesc));
+            std::memcpy(ah.data() + K.aoff_ops, aops.data(), aops.size() * sizeof(SwOp));
+            RQ_CUDA(cudaMalloc((void**)&K.aprog, atotal));
+            RQ_CUDA(cudaMemcpy(K.aprog, ah.data(), atotal, cudaMemcpyHostToDevice));
+        }
         b->classes.push_back(std::move(K));
     }
     // graph data
@@ -1027,9 +1347,13 @@ int rq_qaoa_batch_destroy(rq_qaoa_batch* b) {
     if (!b) return RQ_OK;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
-    for (auto& K : b->classes) if (K.prog) cudaFree(K.prog);
+    for (auto& K : b->classes) {
+        if (K.prog) cudaFree(K.prog);
+        if (K.aprog) cudaFree(K.aprog);
+    }
     void* ptrs[] = {b->d_edges, b->d_eoff, b->d_ne, b->d_circ_inst, b->d_user, b->d_ang, b->d_rx, b->d_ph, b->d_energy,
-                    b->d_best_bits, b->d_best_cut, b->d_states, b->d_epart, b->d_tree};
+                    b->d_best_bits, b->d_best_cut, b->d_states, b->d_epart, b->d_tree, b->d_lam, b->d_gpart,
+                    b->d_grad};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
@@ -1091,9 +1415,16 @@ int qaoa_prepare(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, const d
     return RQ_OK;
 }
 
-// tables + every class's sweeps (+ shots) for the angles in d_ang; energies land in d_energy (run order)
-int qaoa_launch(rq_qaoa_batch* b, uint32_t nsets, uint32_t shots, uint64_t base_seed) {
-    const uint64_t ncirc = (uint64_t)b->ninst * nsets;
+// tables + every class's sweeps (+ shots) for the angles in d_ang; energies land in d_energy (run order).
+// per_class (optional) gives how many instances of each size class the run holds, when the run is a
+// compacted subset (the optimizer's still-active instances); d_circ_inst then lists only those.
+// With adjoint set, every wave also runs the backward pass and d_grad receives the
+// exact gradients ([run position][2p]: gammas, then betas).
+int qaoa_launch(rq_qaoa_batch* b, uint32_t nsets, uint32_t shots, uint64_t base_seed,
+                const std::vector<uint64_t>* per_class = nullptr, bool adjoint = false) {
+    uint64_t nrun = 0;
+    for (size_t k = 0; k < b->classes.size(); ++k) nrun += per_class ? (*per_class)[k] : b->classes[k].insts.size();
+    const uint64_t ncirc = nrun * nsets;
     const uint32_t p = b->p;
     const int sms = rq::num_sms(b->device);
     if (b->prec == RQ_F32)
@@ -1103,24 +1434,38 @@ int qaoa_launch(rq_qaoa_batch* b, uint32_t nsets, uint32_t shots, uint64_t base_
         k_qaoa_tables<double><<<rq::grid_for(ncirc * p, TPB, sms), TPB, 0, b->stream>>>(
             b->d_ang, b->d_ang + ncirc * p, b->d_circ_inst, b->d_ne, ncirc, p, b->phs, (double*)b->d_rx, (double*)b->d_ph);
     RQ_CUDA(cudaGetLastError());
+    const uint32_t P2 = 2 * p;
+    if (adjoint) {
+        RQ_TRY(grow(&b->d_grad, &b->grad_cap, std::max<uint64_t>(1, ncirc) * P2));
+        RQ_CUDA(cudaMemsetAsync(b->d_grad, 0, ncirc * P2 * sizeof(double), b->stream));
+    }
     uint64_t pos = 0;
-    for (auto& K : b->classes) {
-        const uint64_t kc = (uint64_t)K.insts.size() * nsets;
+    for (size_t ki = 0; ki < b->classes.size(); ++ki) {
+        auto& K = b->classes[ki];
+        const uint64_t kc = (per_class ? (*per_class)[ki] : (uint64_t)K.insts.size()) * nsets;
+        if (kc == 0) continue;
         const size_t state_bytes = ((size_t)1 << K.n) * elem_size(b->prec);
-        const uint64_t wave = std::max<uint64_t>(1, std::min<uint64_t>(kc, b->state_budget / state_bytes));
+        const size_t per_circ = adjoint ? 2 * state_bytes : state_bytes;
+        const uint64_t wave = std::max<uint64_t>(1, std::min<uint64_t>(kc, b->state_budget / per_circ));
         RQ_TRY(grow_bytes(&b->d_states, &b->states_cap, wave * state_bytes));
         RQ_TRY(grow(&b->d_epart, &b->epart_cap, wave * K.ntiles));
+        if (adjoint) {
+            RQ_TRY(grow_bytes(&b->d_lam, &b->lam_cap, wave * state_bytes));
+            RQ_TRY(grow(&b->d_gpart, &b->gpart_cap, wave * K.antiles * P2));
+        }
         for (uint64_t w0 = 0; w0 < kc; w0 += wave) {
             const uint64_t wn = std::min<uint64_t>(wave, kc - w0);
             if (b->prec == RQ_F32) {
                 RQ_TRY(launch_class<float>(b, K, wn, pos + w0, b->d_states));
                 if (shots) RQ_TRY(sample_class<float>(b, K, wn, pos + w0, b->d_states, shots, base_seed));
+                if (adjoint) RQ_TRY(adjoint_class<float>(b, K, wn, pos + w0, b->d_states, b->d_lam));
             } else {
                 RQ_TRY(launch_class<double>(b, K, wn, pos + w0, b->d_states));
                 if (shots) RQ_TRY(sample_class<double>(b, K, wn, pos + w0, b->d_states, shots, base_seed));
+                if (adjoint) RQ_TRY(adjoint_class<double>(b, K, wn, pos + w0, b->d_states, b->d_lam));
             }
             b->last_wave_first = pos + w0;
-            b->last_wave_count = wn;
+            b->last_wave_count = adjoint ? 0 : wn;   // the backward pass overwrites the final states
             b->last_wave_n = K.n;
         }
         pos += kc;
@@ -1130,16 +1475,18 @@ int qaoa_launch(rq_qaoa_batch* b, uint32_t nsets, uint32_t shots, uint64_t base_
 
 // parameter sets of one optimizer step: set 0 = theta, set 1+2k / 2+2k = theta_k +- pi/2
 // (the shift rule of run_qaoa, qaoa.rs:275-297); theta = (gamma_1..p, beta_1..p) per instance
-__global__ void k_qaoa_shift(const double* __restrict__ theta, uint32_t ninst, uint32_t p, uint32_t nsets,
-                             double* __restrict__ ang) {
-    const uint64_t ncirc = (uint64_t)ninst * nsets;
+// act lists the run-order instances still optimising; slot a of the run holds instance act[a].
+__global__ void k_qaoa_shift(const double* __restrict__ theta, const uint32_t* __restrict__ act, uint32_t nact,
+                             uint32_t p, uint32_t nsets, double* __restrict__ ang) {
+    const uint64_t ncirc = (uint64_t)nact * nsets;
     const uint64_t total = ncirc * p;
     const double hp = 1.57079632679489661923;
     for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t c = w / p;
         const uint32_t l = (uint32_t)(w - c * p);
-        const uint64_t i = c / nsets;
-        const uint32_t s = (uint32_t)(c - i * nsets);
+        const uint64_t a = c / nsets;
+        const uint32_t s = (uint32_t)(c - a * nsets);
+        const uint64_t i = act[a];
         double g = theta[i * 2 * p + l], b = theta[i * 2 * p + p + l];
         if (s > 0) {
             const uint32_t k = (s - 1) / 2;
@@ -1154,13 +1501,15 @@ __global__ void k_qaoa_shift(const double* __restrict__ theta, uint32_t ninst, u
 
 // one Adam step (gradient ascent on the expected cut) per instance, FP64 on the device;
 // frozen once the target is met.  done[i] = 1 + the step at which the target was met.
-__global__ void k_qaoa_adam(const double* __restrict__ energy, uint32_t ninst, uint32_t p, uint32_t nsets,
-                            double* __restrict__ theta, double* __restrict__ m, double* __restrict__ v, double lr,
-                            uint32_t step, const double* __restrict__ target, double rtol, uint32_t* __restrict__ done,
-                            double* __restrict__ elast, int final_eval) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ninst; i += gridDim.x * blockDim.x) {
+__global__ void k_qaoa_adam(const double* __restrict__ energy, const uint32_t* __restrict__ act, uint32_t nact,
+                            uint32_t p, uint32_t nsets, double* __restrict__ theta, double* __restrict__ m,
+                            double* __restrict__ v, double lr, uint32_t step, const double* __restrict__ target,
+                            double rtol, uint32_t* __restrict__ done, double* __restrict__ elast, int final_eval,
+                            const double* __restrict__ grad) {
+    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < nact; a += gridDim.x * blockDim.x) {
+        const uint32_t i = act[a];
         if (done[i]) continue;
-        const double* e = energy + (uint64_t)i * nsets;
+        const double* e = energy + (uint64_t)a * nsets;
         elast[i] = e[0];
         if (target && e[0] >= target[i] * (1.0 - rtol)) {
             done[i] = step + 1;
@@ -1170,7 +1519,8 @@ __global__ void k_qaoa_adam(const double* __restrict__ energy, uint32_t ninst, u
         const double b1 = 0.9, b2 = 0.999, eps = 1e-8;
         const double c1 = 1.0 - pow(b1, (double)(step + 1)), c2 = 1.0 - pow(b2, (double)(step + 1));
         for (uint32_t k = 0; k < 2 * p; ++k) {
-            const double g = (e[1 + 2 * k] - e[2 + 2 * k]) / 2.0;
+            // exact (adjoint) gradient when given, else the shift rule of qaoa.rs:275-297
+            const double g = grad ? grad[(uint64_t)a * 2 * p + k] : (e[1 + 2 * k] - e[2 + 2 * k]) / 2.0;
             const uint64_t j = (uint64_t)i * 2 * p + k;
             const double mm = b1 * m[j] + (1.0 - b1) * g;
             const double vv = b2 * v[j] + (1.0 - b2) * g * g;
@@ -1179,17 +1529,6 @@ __global__ void k_qaoa_adam(const double* __restrict__ energy, uint32_t ninst, u
             theta[j] += lr * (mm / c1) / (sqrt(vv / c2) + eps);
         }
     }
-}
-
-__global__ void k_count_active(const uint32_t* __restrict__ done, uint32_t n, uint32_t* __restrict__ out) {
-    __shared__ uint32_t s;
-    if (threadIdx.x == 0) s = 0;
-    __syncthreads();
-    uint32_t c = 0;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) c += done[i] == 0;
-    atomicAdd(&s, c);
-    __syncthreads();
-    if (threadIdx.x == 0) *out = s;
 }
 
 }  // namespace
@@ -1231,11 +1570,38 @@ int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, co
     return RQ_OK;
 }
 
-int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, double* betas,
-                           const double* target, double rtol, double* energies, uint32_t* steps_taken) {
-    if (!b || !gammas || !betas || !energies || !steps_taken) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+int rq_qaoa_batch_gradient(rq_qaoa_batch* b, const double* gammas, const double* betas, double* energies,
+                           double* gradients) {
+    if (!b || !gammas || !betas || !energies || !gradients) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
     RQ_CUDA(cudaSetDevice(b->device));
-    const uint32_t p = b->p, P2 = 2 * p, nsets = 1 + 2 * P2, ninst = b->ninst;
+    const uint32_t p = b->p, P2 = 2 * p, ninst = b->ninst;
+    RQ_TRY(qaoa_prepare(b, 1, gammas, betas));
+    RQ_CUDA(cudaEventRecord(b->ev0, b->stream));
+    RQ_TRY(qaoa_launch(b, 1, 0, 0, nullptr, true));
+    RQ_CUDA(cudaEventRecord(b->ev1, b->stream));
+    std::vector<double> e(ninst), g((size_t)ninst * P2);
+    RQ_CUDA(cudaMemcpyAsync(e.data(), b->d_energy, ninst * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    RQ_CUDA(cudaMemcpyAsync(g.data(), b->d_grad, g.size() * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    RQ_CUDA(cudaStreamSynchronize(b->stream));
+    RQ_CUDA(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+    for (uint32_t k = 0; k < ninst; ++k) {
+        const uint64_t user = b->order[k];
+        energies[user] = e[k];
+        for (uint32_t j = 0; j < P2; ++j) gradients[user * P2 + j] = g[(size_t)k * P2 + j];
+    }
+    b->last_nsets = 1;
+    return RQ_OK;
+}
+
+int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, double* betas,
+                           const double* target, double rtol, int32_t gradient, double* energies,
+                           uint32_t* steps_taken) {
+    if (!b || !gammas || !betas || !energies || !steps_taken) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (gradient != RQ_QAOA_GRAD_ADJOINT && gradient != RQ_QAOA_GRAD_SHIFT)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "gradient must be RQ_QAOA_GRAD_ADJOINT or RQ_QAOA_GRAD_SHIFT");
+    RQ_CUDA(cudaSetDevice(b->device));
+    const bool adj = gradient == RQ_QAOA_GRAD_ADJOINT;
+    const uint32_t p = b->p, P2 = 2 * p, nsets = adj ? 1 : 1 + 2 * P2, ninst = b->ninst;
     RQ_TRY(qaoa_prepare(b, nsets, nullptr, nullptr));
     // instances in run order (class-major), angles as theta = (gammas, betas) per instance
     std::vector<uint32_t> inst_order;
@@ -1250,10 +1616,17 @@ int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* 
         }
         if (target) tg[r] = target[i];
     }
+    // run-order position of each size class's first instance
+    std::vector<uint32_t> cls_of(ninst);
+    {
+        uint32_t r = 0;
+        for (size_t k = 0; k < b->classes.size(); ++k)
+            for (size_t j = 0; j < b->classes[k].insts.size(); ++j) cls_of[r++] = (uint32_t)k;
+    }
     double *d_th = nullptr, *d_m = nullptr, *d_v = nullptr, *d_tg = nullptr, *d_el = nullptr;
-    uint32_t *d_done = nullptr, *d_active = nullptr;
+    uint32_t *d_done = nullptr, *d_act = nullptr;
     auto cleanup = [&]() {
-        void* q[] = {d_th, d_m, d_v, d_tg, d_el, d_done, d_active};
+        void* q[] = {d_th, d_m, d_v, d_tg, d_el, d_done, d_act};
         for (void* x : q) if (x) cudaFree(x);
     };
     int rc = RQ_OK;
@@ -1263,36 +1636,65 @@ int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* 
     if (rc == RQ_OK) rc = dalloc_b(&d_tg, ninst);
     if (rc == RQ_OK) rc = dalloc_b(&d_el, ninst);
     if (rc == RQ_OK) rc = dalloc_b(&d_done, ninst);
-    if (rc == RQ_OK) rc = dalloc_b(&d_active, 1);
+    if (rc == RQ_OK) rc = dalloc_b(&d_act, ninst);
     if (rc != RQ_OK) { cleanup(); return rc; }
+    // active set: run-order instances still optimising, their circuits' instance map, and per-class counts
+    std::vector<uint32_t> act(ninst), ci;
+    for (uint32_t r = 0; r < ninst; ++r) act[r] = r;
+    std::vector<uint64_t> per_class(b->classes.size());
+    std::vector<uint32_t> dn(ninst, 0);
+    auto upload_active = [&]() -> int {
+        std::fill(per_class.begin(), per_class.end(), 0);
+        ci.clear();
+        for (uint32_t r : act) {
+            ++per_class[cls_of[r]];
+            for (uint32_t s2 = 0; s2 < nsets; ++s2) ci.push_back(inst_order[r]);
+        }
+        RQ_CUDA(cudaMemcpyAsync(d_act, act.data(), act.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream));
+        RQ_CUDA(cudaMemcpyAsync(b->d_circ_inst, ci.data(), ci.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                b->stream));
+        // the pageable sources must outlive the copies
+        RQ_CUDA(cudaStreamSynchronize(b->stream));
+        return RQ_OK;
+    };
     cudaMemcpyAsync(d_th, th.data(), th.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream);
     cudaMemsetAsync(d_m, 0, th.size() * sizeof(double), b->stream);
     cudaMemsetAsync(d_v, 0, th.size() * sizeof(double), b->stream);
     cudaMemsetAsync(d_done, 0, ninst * sizeof(uint32_t), b->stream);
     if (target) cudaMemcpyAsync(d_tg, tg.data(), ninst * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+    rc = upload_active();
     const int sms = rq::num_sms(b->device);
-    const uint64_t ncirc = (uint64_t)ninst * nsets;
     cudaEventRecord(b->ev0, b->stream);
     for (uint32_t step = 0; step <= steps && rc == RQ_OK; ++step) {
-        k_qaoa_shift<<<rq::grid_for(ncirc * p, TPB, sms), TPB, 0, b->stream>>>(d_th, ninst, p, nsets, b->d_ang);
-        rc = qaoa_launch(b, nsets, 0, 0);
+        const uint32_t nact = (uint32_t)act.size();
+        const uint64_t ncirc = (uint64_t)nact * nsets;
+        k_qaoa_shift<<<rq::grid_for(ncirc * p, TPB, sms), TPB, 0, b->stream>>>(d_th, d_act, nact, p, nsets, b->d_ang);
+        rc = qaoa_launch(b, nsets, 0, 0, &per_class, adj && step < steps);
         if (rc != RQ_OK) break;
-        k_qaoa_adam<<<rq::grid_for(ninst, TPB, sms), TPB, 0, b->stream>>>(b->d_energy, ninst, p, nsets, d_th, d_m, d_v, lr,
-                                                                       step, target ? d_tg : nullptr, rtol, d_done, d_el,
-                                                                       step == steps ? 1 : 0);
+        k_qaoa_adam<<<rq::grid_for(nact, TPB, sms), TPB, 0, b->stream>>>(b->d_energy, d_act, nact, p, nsets, d_th, d_m,
+                                                                      d_v, lr, step, target ? d_tg : nullptr, rtol,
+                                                                      d_done, d_el, step == steps ? 1 : 0,
+                                                                      adj ? b->d_grad : nullptr);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) { rc = rq::cuda_fail(e, "optimizer kernels"); break; }
-        if (target && (step % 5 == 4)) {   // stop once every instance has met its target
-            uint32_t active = 1;
-            k_count_active<<<1, 256, 0, b->stream>>>(d_done, ninst, d_active);
-            cudaMemcpyAsync(&active, d_active, sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
-            cudaStreamSynchronize(b->stream);
-            if (active == 0) break;
+        if (target && step < steps && (step % 5 == 4)) {
+            // drop the instances that met their target from the next steps' launches; the
+            // rest keep their slots' math (every circuit's energy is independent of the batch)
+            e = cudaMemcpyAsync(dn.data(), d_done, ninst * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+            if (e != cudaSuccess) { rc = rq::cuda_fail(e, "optimizer poll"); break; }
+            std::vector<uint32_t> still;
+            for (uint32_t r : act)
+                if (dn[r] == 0) still.push_back(r);
+            if (still.empty()) break;
+            if (still.size() < act.size()) {
+                act.swap(still);
+                rc = upload_active();
+            }
         }
     }
     cudaEventRecord(b->ev1, b->stream);
     std::vector<double> el(ninst);
-    std::vector<uint32_t> dn(ninst);
     if (rc == RQ_OK) {
         cudaMemcpyAsync(th.data(), d_th, th.size() * sizeof(double), cudaMemcpyDeviceToHost, b->stream);
         cudaMemcpyAsync(el.data(), d_el, ninst * sizeof(double), cudaMemcpyDeviceToHost, b->stream);
@@ -1302,6 +1704,8 @@ int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* 
         cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
     }
     cleanup();
+    // the wave buffer holds shifted-angle circuits of a compacted run: nothing there for state()
+    b->last_wave_count = 0;
     RQ_TRY(rc);
     for (uint32_t r = 0; r < ninst; ++r) {
         const uint32_t i = inst_order[r];

@@ -61,6 +61,7 @@ struct SweepDesc {
 constexpr uint32_t SWEEP_INIT_UNIFORM = 1u;   // synthesise |+>^n instead of loading the tile
 constexpr uint32_t SWEEP_ENERGY = 2u;         // reduce sum |a|^2 cut(x) after the last phase
 constexpr uint32_t SWEEP_INIT_ZERO = 4u;      // synthesise |0...0> instead of loading the tile
+constexpr uint32_t SWEEP_INIT_LAMBDA = 8u;    // adjoint sweeps: build lambda = C psi instead of loading it
 
 
 struct PGate {

@@ -21,13 +21,15 @@ PAD_NODES = 26
 FEATURES = PAD_NODES * (PAD_NODES - 1) // 2      # 325
 
 
-def graph_features(n: int, edges) -> np.ndarray:
-    """Upper triangle (i < j, row-major) of the adjacency matrix padded to PAD_NODES nodes."""
+def graph_features(n: int, edges, slots=None) -> np.ndarray:
+    """Upper triangle (i < j, row-major) of the adjacency matrix padded to PAD_NODES nodes.
+    slots (optional, n distinct values below PAD_NODES) places node v at row slots[v]."""
     if n > PAD_NODES:
         raise ValueError(f"graphs up to {PAD_NODES} nodes")
+    pos = np.arange(n) if slots is None else np.asarray(slots)
     a = np.zeros((PAD_NODES, PAD_NODES), dtype=np.float32)
     for u, v in edges:
-        a[u, v] = a[v, u] = 1.0
+        a[pos[u], pos[v]] = a[pos[v], pos[u]] = 1.0
     iu = np.triu_indices(PAD_NODES, 1)
     return a[iu]
 
@@ -85,10 +87,73 @@ class Mlp:
 
 
 def linear_ramp(p: int, delta: float = 0.75):
-    """Plain start: gamma_l = (l - 1/2)/p * delta, beta_l = (1 - (l - 1/2)/p) * delta, l = 1..p."""
+    """Plain start: gamma_l = -(l - 1/2)/p * delta, beta_l = (1 - (l - 1/2)/p) * delta, l = 1..p.
+
+    The circuit of build_qaoa_circuit (qaoa.rs:125-153) applies Rzz(2 gamma) = exp(-i gamma ZZ)
+    per edge, i.e. exp(+2i gamma cut(x)) up to a global phase, and Rx(2 beta) = exp(-i beta X):
+    the expected cut rises from the random-guess |E|/2 for gamma < 0 with beta > 0, so the
+    annealing-style ramp takes negative gammas."""
     f = (np.arange(1, p + 1) - 0.5) / p
-    return f * delta, (1.0 - f) * delta
+    return -f * delta, (1.0 - f) * delta
 
 
-def features(graphs) -> np.ndarray:
-    return np.stack([graph_features(n, e) for n, e in graphs]).astype(np.float32)
+def features(graphs, copies: int = 1, seed=None) -> np.ndarray:
+    """Feature rows of the graphs.  With a seed, each graph gives `copies` rows, each
+    with its nodes placed at random distinct rows of the padded matrix (graph-major
+    order): the angles do not depend on node labels, and every input position is
+    exercised during training whatever the graph sizes."""
+    if seed is None:
+        return np.stack([graph_features(n, e) for n, e in graphs]).astype(np.float32)
+    r = np.random.default_rng(seed)
+    rows = [graph_features(n, e, r.permutation(PAD_NODES)[:n]) for n, e in graphs for _ in range(copies)]
+    return np.stack(rows).astype(np.float32)
+
+
+class WarmStart:
+    """Learned QAOA warm start: an Mlp from padded adjacency features to the 2p angles.
+
+    Targets are normalised per angle (mean / standard deviation of the training set),
+    so an untrained network predicts the mean angles -- optimal QAOA angles of graphs
+    from one family concentrate, and the network learns the per-graph correction.
+    Training rows place each graph's nodes at random rows of the padded matrix
+    (`copies` placements per graph); a held-out slice of the graphs picks the
+    parameters with the lowest validation error; predictions average `tta` random
+    placements."""
+
+    def __init__(self, p: int, hidden: int = 256, seed: int = 5):
+        self.p = p
+        self.net = Mlp(h1=hidden, h2=hidden, n_out=2 * p, seed=seed)
+        self.mu = np.zeros(2 * p)
+        self.sd = np.ones(2 * p)
+
+    def fit(self, graphs, gammas, betas, copies: int = 4, val_fraction: float = 0.125, chunks: int = 12,
+            chunk_steps: int = 500, lr: float = 1e-3, batch: int = 256, seed: int = 3) -> list:
+        y = np.concatenate([np.asarray(gammas, dtype=np.float64), np.asarray(betas, dtype=np.float64)], axis=1)
+        nval = max(1, int(len(graphs) * val_fraction))
+        ntr = len(graphs) - nval
+        self.mu = y[:ntr].mean(axis=0)
+        self.sd = np.maximum(y[:ntr].std(axis=0), 1e-6)
+        z = (y - self.mu) / self.sd
+        x = features(graphs[:ntr], copies, seed=seed)
+        t = np.repeat(z[:ntr], copies, axis=0).astype(np.float32)
+        xv = features(graphs[ntr:], copies, seed=seed + 1)
+        tv = np.repeat(z[ntr:], copies, axis=0).astype(np.float32)
+        best, best_p, hist = float(np.mean(tv.astype(np.float64) ** 2)), None, []
+        for c in range(chunks):
+            self.net.train(x, t, batch=batch, steps=chunk_steps, lr=lr if c < (2 * chunks) // 3 else lr / 3)
+            vl = float(np.mean((self.net.forward(xv) - tv) ** 2))
+            hist.append(vl)
+            if vl < best:
+                best, best_p = vl, self.net.get_params()
+        if best_p is None:     # never better than the mean: predict the mean
+            self.net.set_params(np.zeros(self.net.nparam, dtype=np.float32))
+        else:
+            self.net.set_params(best_p)
+        return hist
+
+    def predict(self, graphs, tta: int = 8, seed: int = 9):
+        x = features(graphs, tta, seed=seed)
+        z = self.net.forward(x).reshape(len(graphs), tta, -1).mean(axis=1).astype(np.float64)
+        y = self.mu + self.sd * z
+        return y[:, :self.p], y[:, self.p:]
+
