@@ -125,10 +125,8 @@ class Clocks:
 
 
 def _dist():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from ruqu_b200.dist import world
+    return world()
 
 
 def cpu_baseline_sample(a, parallel: bool, gates_in_sample: int = 4):
@@ -161,8 +159,9 @@ def qaoa_batch_leg(a, ws, rank, with_cpu):
 
     from ruqu_b200 import workloads
     from ruqu_b200.batch import QaoaBatch
+    from ruqu_b200.dist import shard
     inst = workloads.qaoa_instances(a.qaoa_instances, 2)
-    mine = inst[rank::ws]
+    mine = shard(inst, rank, ws)
     graphs = [(x["n"], [(u, v) for u, v, _ in x["edges"]]) for x in mine]
     gam = np.array([x["gammas"] for x in mine])
     bet = np.array([x["betas"] for x in mine])
@@ -210,7 +209,8 @@ def vqe_batch_leg(a, ws, rank, with_cpu):
     from ruqu_b200.batch import VqeBatch
     n, depth = 16, 8
     coeffs, strings = workloads.pauli_hamiltonian(n, 200, 3)
-    params = workloads.vqe_parameter_sets(a.vqe_sets, n * depth, 4)[rank::ws]
+    from ruqu_b200.dist import shard
+    params = shard(workloads.vqe_parameter_sets(a.vqe_sets, n * depth, 4), rank, ws)
     vb = VqeBatch(n, depth, coeffs, strings, "f32")
     vb.run(params[:2], gradient=True)           # warm-up
     ms, wall = [], []
@@ -270,7 +270,8 @@ def warmstart_leg(a, ws, rank):
     gen_ms = qb.last_ms()
     warm = WarmStart(p)
     hist = warm.fit(train, g, b)
-    held = graphs(a.warm_eval, (16, 18, 20), 22)[rank::ws]
+    from ruqu_b200.dist import shard
+    held = shard(graphs(a.warm_eval, (16, 18, 20), 22), rank, ws)
     hb = QaoaBatch(held, p, "f32")
     G0, B0 = np.tile(g0, (len(held), 1)), np.tile(b0, (len(held), 1))
     _, _, target, _ = hb.optimize(G0, B0, 200, lr)
@@ -348,11 +349,9 @@ def run_ours(a):
     ws, rank, local = _dist()
     dist = ws > 1
     if dist:
-        import datetime
-
-        import torch.distributed as tdist
+        from ruqu_b200 import dist as rqdist
         torch.cuda.set_device(local)
-        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        tdist = rqdist.init("nccl", 120.0)
     rq.set_device(local)
     torch.cuda.set_device(local)
 
@@ -398,9 +397,7 @@ def run_ours(a):
     plan_ms = sum(e[1].elapsed_time(e[2]) for e in ev)
     init_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
     if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = rqdist.max_over_ranks(total_ms)
     value = ws * step_bytes * a.steps / (total_ms / 1e3) / 1e9
     peak, peak_kind = _peak()
     sweeps = max(1, stats["sweeps"] or stats["launches"])
@@ -431,18 +428,14 @@ def run_ours(a):
     if not a.no_qaoa:
         qaoa = qaoa_batch_leg(a, ws, rank, with_cpu=(rank == 0 and ws == 1 and not a.no_cpu_baseline))
         if dist:
-            t = torch.tensor([qaoa["device_ms"]], device="cuda")
-            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-            qaoa["device_ms_max_over_ranks"] = float(t.item())
+            qaoa["device_ms_max_over_ranks"] = rqdist.max_over_ranks(qaoa["device_ms"])
             qaoa["evals_per_s"] = a.qaoa_instances / (qaoa["device_ms_max_over_ranks"] / 1e3)
 
     vqe = None
     if not a.no_vqe:
         vqe = vqe_batch_leg(a, ws, rank, with_cpu=(rank == 0 and ws == 1 and not a.no_cpu_baseline))
         if dist:
-            t = torch.tensor([vqe["device_ms"]], device="cuda")
-            tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
-            vqe["device_ms_max_over_ranks"] = float(t.item())
+            vqe["device_ms_max_over_ranks"] = rqdist.max_over_ranks(vqe["device_ms"])
             vqe["circuits_per_s"] = a.vqe_sets * 257 / (vqe["device_ms_max_over_ranks"] / 1e3)
 
     warm = None

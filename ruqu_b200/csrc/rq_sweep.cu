@@ -112,6 +112,81 @@ __device__ __forceinline__ void dispatch_cx(int k, V* reg, int ck, int cu) {
     }
 }
 
+// The phases of one sweep on a tile held in shared memory (all threads of the CTA).
+template <typename T, int RB>
+__device__ __forceinline__ void run_phases(typename C2<T>::t* sm, const SweepDesc& d,
+                                           const PhaseDesc* __restrict__ phases, const SwOp* __restrict__ ops,
+                                           const T* __restrict__ mats, uint64_t base, uint32_t tid) {
+    using V = typename C2<T>::t;
+    constexpr int NR = 1 << RB;
+    for (uint32_t p = d.phase_begin; p < d.phase_end; ++p) {
+        const PhaseDesc& ph = phases[p];
+        uint32_t ebase = 0;
+        uint64_t U = base;
+        for (uint32_t b = 0; b < ph.nt; ++b)
+            if ((tid >> b) & 1u) {
+                ebase |= 1u << ph.tbit_local[b];
+                U |= 1ull << ph.tbit_global[b];
+            }
+        const uint32_t sb = swz<T>(ebase);
+        V reg[NR];
+#pragma unroll
+        for (int i = 0; i < NR; ++i) reg[i] = sm[sb ^ ph.slut[i]];
+
+        for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
+            const SwOp op = ops[o];
+            const T* mm = mats + 2 * op.mat;
+            switch (op.type) {
+                case OP_U1: dispatch_u1<NR>(op.k0, reg, mm); break;
+                case OP_CX: dispatch_cx<NR>(op.k1, reg, op.k0, (int)((U >> op.q0) & 1ull)); break;
+                case OP_D1: {
+                    const T d0r = mm[0], d0i = mm[1], d1r = mm[2], d1i = mm[3];
+                    const int kk = op.k0;
+                    const int ub = (int)((U >> op.q0) & 1ull);
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) {
+                        const int b = kk >= 0 ? ((i >> kk) & 1) : ub;
+                        reg[i] = cmul(reg[i], b ? d1r : d0r, b ? d1i : d0i);
+                    }
+                    break;
+                }
+                case OP_CZ: {
+                    const int k0 = op.k0, k1 = op.k1;
+                    const int u0 = (int)((U >> op.q0) & 1ull), u1 = (int)((U >> op.q1) & 1ull);
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) {
+                        const int b0 = k0 >= 0 ? ((i >> k0) & 1) : u0;
+                        const int b1 = k1 >= 0 ? ((i >> k1) & 1) : u1;
+                        if (b0 & b1) {
+                            reg[i].x = -reg[i].x;
+                            reg[i].y = -reg[i].y;
+                        }
+                    }
+                    break;
+                }
+                case OP_ZZ: {
+                    // diag(en, ep, ep, en): en for equal bits, ep for different bits
+                    const T er = mm[0], ei = mm[1], pr = mm[2], pi = mm[3];
+                    const int k0 = op.k0, k1 = op.k1;
+                    const int u0 = (int)((U >> op.q0) & 1ull), u1 = (int)((U >> op.q1) & 1ull);
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) {
+                        const int b0 = k0 >= 0 ? ((i >> k0) & 1) : u0;
+                        const int b1 = k1 >= 0 ? ((i >> k1) & 1) : u1;
+                        const bool diff = (b0 ^ b1) != 0;
+                        reg[i] = cmul(reg[i], diff ? pr : er, diff ? pi : ei);
+                    }
+                    break;
+                }
+                default: break;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NR; ++i) sm[sb ^ ph.slut[i]] = reg[i];
+        __syncthreads();
+    }
+}
+
 template <typename T, int RB>
 __global__ void __launch_bounds__(256, 2) k_sweep(typename C2<T>::t* __restrict__ amps, const SweepDesc d,
                                                const PhaseDesc* __restrict__ phases, const SwOp* __restrict__ ops,
@@ -164,72 +239,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep(typename C2<T>::t* __restrict_
         __syncthreads();
 
         // ---- phases ----
-        for (uint32_t p = d.phase_begin; p < d.phase_end; ++p) {
-            const PhaseDesc& ph = phases[p];
-            uint32_t ebase = 0;
-            uint64_t U = base;
-            for (uint32_t b = 0; b < ph.nt; ++b)
-                if ((tid >> b) & 1u) {
-                    ebase |= 1u << ph.tbit_local[b];
-                    U |= 1ull << ph.tbit_global[b];
-                }
-            const uint32_t sb = swz<T>(ebase);
-            V reg[NR];
-#pragma unroll
-            for (int i = 0; i < NR; ++i) reg[i] = sm[sb ^ ph.slut[i]];
-
-            for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
-                const SwOp op = ops[o];
-                const T* mm = mats + 2 * op.mat;
-                switch (op.type) {
-                    case OP_U1: dispatch_u1<NR>(op.k0, reg, mm); break;
-                    case OP_CX: dispatch_cx<NR>(op.k1, reg, op.k0, (int)((U >> op.q0) & 1ull)); break;
-                    case OP_D1: {
-                        const T d0r = mm[0], d0i = mm[1], d1r = mm[2], d1i = mm[3];
-                        const int kk = op.k0;
-                        const int ub = (int)((U >> op.q0) & 1ull);
-#pragma unroll
-                        for (int i = 0; i < NR; ++i) {
-                            const int b = kk >= 0 ? ((i >> kk) & 1) : ub;
-                            reg[i] = cmul(reg[i], b ? d1r : d0r, b ? d1i : d0i);
-                        }
-                        break;
-                    }
-                    case OP_CZ: {
-                        const int k0 = op.k0, k1 = op.k1;
-                        const int u0 = (int)((U >> op.q0) & 1ull), u1 = (int)((U >> op.q1) & 1ull);
-#pragma unroll
-                        for (int i = 0; i < NR; ++i) {
-                            const int b0 = k0 >= 0 ? ((i >> k0) & 1) : u0;
-                            const int b1 = k1 >= 0 ? ((i >> k1) & 1) : u1;
-                            if (b0 & b1) {
-                                reg[i].x = -reg[i].x;
-                                reg[i].y = -reg[i].y;
-                            }
-                        }
-                        break;
-                    }
-                    case OP_ZZ: {
-                        // diag(en, ep, ep, en): en for equal bits, ep for different bits
-                        const T er = mm[0], ei = mm[1], pr = mm[2], pi = mm[3];
-                        const int k0 = op.k0, k1 = op.k1;
-                        const int u0 = (int)((U >> op.q0) & 1ull), u1 = (int)((U >> op.q1) & 1ull);
-#pragma unroll
-                        for (int i = 0; i < NR; ++i) {
-                            const int b0 = k0 >= 0 ? ((i >> k0) & 1) : u0;
-                            const int b1 = k1 >= 0 ? ((i >> k1) & 1) : u1;
-                            const bool diff = (b0 ^ b1) != 0;
-                            reg[i] = cmul(reg[i], diff ? pr : er, diff ? pi : ei);
-                        }
-                        break;
-                    }
-                    default: break;
-                }
-            }
-#pragma unroll
-            for (int i = 0; i < NR; ++i) sm[sb ^ ph.slut[i]] = reg[i];
-            __syncthreads();
-        }
+        run_phases<T, RB>(sm, d, phases, ops, mats, base, tid);
 
         // ---- store tile ----
 #pragma unroll
@@ -250,9 +260,121 @@ __global__ void __launch_bounds__(256, 2) k_sweep(typename C2<T>::t* __restrict_
     }
 }
 
+// Asynchronous global -> shared copies (cp.async): the data bypasses registers,
+// so the next tile streams in while the CTA computes on the current one.
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Tile loads of one thread into a swizzled shared-memory buffer: the element
+// granularity of the swizzle is kept (f32: two 8-byte copies per 16-byte vector).
+template <typename T>
+__device__ __forceinline__ void issue_tile(typename C2<T>::t* buf, const typename C2<T>::t* __restrict__ amps,
+                                           const SweepDesc& d, uint64_t base, uint64_t dep_tid, uint32_t stid) {
+    constexpr int EPV = Vec16<T>::EPV;
+    constexpr int VPT = (1 << (std::is_same<T, float>::value ? 5 : 4)) / EPV;
+#pragma unroll
+    for (int j = 0; j < VPT; ++j) {
+        const typename C2<T>::t* g = amps + (base | dep_tid | d.gj[j]);
+        const uint32_t se = stid ^ d.sgj[j];
+        if constexpr (EPV == 2) {
+            cp_async8(buf + se, g);
+            cp_async8(buf + (se ^ 1u), g + 1);
+        } else {
+            cp_async16(buf + se, g);
+        }
+    }
+}
+
+// Persistent, double-buffered sweep: one CTA per SM walks tiles blockIdx.x,
+// blockIdx.x + gridDim.x, ...; the copies of tile k+1 are in flight while the
+// phases of tile k run and its stores drain.
+template <typename T, int RB>
+__global__ void __launch_bounds__(256, 1) k_sweep_pipe(typename C2<T>::t* __restrict__ amps, const SweepDesc d,
+                                                     const PhaseDesc* __restrict__ phases,
+                                                     const SwOp* __restrict__ ops, const T* __restrict__ mats,
+                                                     uint64_t ntiles) {
+    using V = typename C2<T>::t;
+    using VV = typename Vec16<T>::t;
+    constexpr int NR = 1 << RB;
+    constexpr int EPV = Vec16<T>::EPV;
+    constexpr int VPT = NR / EPV;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* buf0 = reinterpret_cast<V*>(smem_raw);
+    V* buf1 = buf0 + (1u << d.m);
+
+    const uint32_t tid = threadIdx.x;
+    const uint64_t cmask = (1ull << d.c) - 1;
+    uint64_t dep_tid = 0;
+    {
+        uint64_t x = (uint64_t)tid * EPV;
+        dep_tid = x & cmask;
+        for (uint32_t b = d.c; b < d.m; ++b)
+            if ((x >> b) & 1ull) dep_tid |= 1ull << d.local_global[b];
+    }
+    const uint32_t stid = swz<T>(tid * EPV);
+    auto tile_base = [&](uint64_t tile) {
+        uint64_t base = 0;
+        for (uint32_t b = 0; b < d.nonlocal_count; ++b)
+            if ((tile >> b) & 1ull) base |= 1ull << d.nonlocal[b];
+        return base;
+    };
+
+    uint64_t tile = blockIdx.x;
+    if (tile < ntiles) issue_tile<T>(buf0, amps, d, tile_base(tile), dep_tid, stid);
+    cp_async_commit();
+    bool cur1 = false;
+    for (; tile < ntiles; tile += gridDim.x) {
+        V* sm = cur1 ? buf1 : buf0;
+        V* nx = cur1 ? buf0 : buf1;
+        const uint64_t next = tile + gridDim.x;
+        if (next < ntiles) issue_tile<T>(nx, amps, d, tile_base(next), dep_tid, stid);
+        cp_async_commit();
+        cp_async_wait1();          // this thread's copies of the current tile have landed
+        __syncthreads();           // ... and everyone else's
+        const uint64_t base = tile_base(tile);
+        run_phases<T, RB>(sm, d, phases, ops, mats, base, tid);
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) {
+            const uint32_t se = stid ^ d.sgj[j];
+            const uint64_t g = base | dep_tid | d.gj[j];
+            VV v;
+            if constexpr (EPV == 2) {
+                float2 a = sm[se], b = sm[se ^ 1u];
+                v = make_float4(a.x, a.y, b.x, b.y);
+            } else {
+                V a = sm[se];
+                v = *reinterpret_cast<VV*>(&a);
+            }
+            __stcs(reinterpret_cast<VV*>(amps + g), v);
+        }
+        __syncthreads();           // the buffer is free for the copies issued next iteration
+        cur1 = !cur1;
+    }
+    cp_async_wait0();
+}
+
 // ---------------------------------------------------------------------------
 // host planner
 // ---------------------------------------------------------------------------
+
+// Double-buffered persistent sweeps (default); RUQU_SWEEP_PIPE=0 selects the
+// single-buffered kernel with two CTAs per SM.
+static bool sweep_pipelined() {
+    static const bool on = [] {
+        const char* e = std::getenv("RUQU_SWEEP_PIPE");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
 
 template <typename T>
 int launch_sweep(rq_state* s, const SweepDesc& d, const PhaseDesc* ph, const SwOp* ops, const void* mats,
@@ -260,6 +382,19 @@ int launch_sweep(rq_state* s, const SweepDesc& d, const PhaseDesc* ph, const SwO
     using V = typename C2<T>::t;
     unsigned threads = 1u << (d.m - rb);
     int sms = rq::num_sms(s->device);
+    if (sweep_pipelined()) {
+        auto kp = k_sweep_pipe<T, std::is_same<T, float>::value ? 5 : 4>;
+        const size_t smem2 = 2 * smem;
+        RQ_CUDA(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+        int per_sm = 0;
+        RQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kp, (int)threads, smem2));
+        if (per_sm >= 1) {
+            unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)sms * per_sm);
+            kp<<<grid, threads, smem2, s->stream>>>((V*)s->amps, d, ph, ops, (const T*)mats, ntiles);
+            RQ_CUDA(cudaGetLastError());
+            return RQ_OK;
+        }
+    }
     auto kern = k_sweep<T, std::is_same<T, float>::value ? 5 : 4>;
     RQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // persistent grid: exactly the CTAs that can be resident at once
