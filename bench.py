@@ -49,7 +49,7 @@ def _args():
     ap.add_argument("--layers", type=int, default=20)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
-    ap.add_argument("--mode", choices=["auto", "per_gate", "sweep"], default="auto")
+    ap.add_argument("--mode", choices=["auto", "per_gate", "sweep", "tc", "tc_fast"], default="auto")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-qaoa", action="store_true", help="skip the batched QAOA leg")
@@ -355,7 +355,8 @@ def run_ours(a):
     rq.set_device(local)
     torch.cuda.set_device(local)
 
-    mode = {"auto": rq.RQ_EXEC_AUTO, "per_gate": rq.RQ_EXEC_PER_GATE, "sweep": rq.RQ_EXEC_SWEEP}[a.mode]
+    mode = {"auto": rq.RQ_EXEC_AUTO, "per_gate": rq.RQ_EXEC_PER_GATE, "sweep": rq.RQ_EXEC_SWEEP,
+            "tc": rq.RQ_EXEC_SWEEP_TC, "tc_fast": rq.RQ_EXEC_SWEEP_TC_FAST}[a.mode]
     gates = workloads.random_layer_circuit(a.qubits, a.layers, a.seed)
     garr = gates_to_array(gates)
     state = rq.QuantumState(a.qubits, 0, a.precision)

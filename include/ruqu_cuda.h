@@ -110,7 +110,12 @@ typedef struct rq_pauli_op {
 typedef enum rq_exec_mode {
     RQ_EXEC_AUTO = 0,      /* autotuned choice (default) */
     RQ_EXEC_PER_GATE = 1,  /* one kernel per gate: the unfused path              */
-    RQ_EXEC_SWEEP = 2      /* register/shared-memory tiled multi-gate sweeps     */
+    RQ_EXEC_SWEEP = 2,     /* register/shared-memory tiled multi-gate sweeps     */
+    RQ_EXEC_SWEEP_TC = 3,  /* sweeps whose per-phase gate runs are fused into dense
+                              32x32 unitaries applied on the tensor cores as
+                              3xTF32 MMAs (complex f32 states, >= 12 qubits)     */
+    RQ_EXEC_SWEEP_TC_FAST = 4  /* as RQ_EXEC_SWEEP_TC with one TF32 MMA pass
+                                  (10-bit operand mantissas)                     */
 } rq_exec_mode;
 
 typedef struct rq_state rq_state;   /* opaque: device-resident amplitudes */
@@ -124,6 +129,7 @@ typedef struct rq_plan_stats {
     uint64_t phases;      /* register phases summed over all sweeps             */
     uint64_t ops;         /* device ops after 1-qubit fusion                    */
     uint64_t hbm_bytes;   /* algorithmic HBM bytes per execution                */
+    uint64_t dense_ops;   /* dense 32x32 unitaries on the tensor cores          */
 } rq_plan_stats;
 
 /* ------------------------------------------------------------------------ */

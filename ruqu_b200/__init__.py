@@ -7,7 +7,8 @@ reference's API: ``QuantumState`` (crates/ruqu-core/src/state.rs),
 (simulator.rs), the types of types.rs and the QAOA / VQE drivers of
 crates/ruqu-algorithms.  Importing it fails if the library is not built.
 """
-from ._capi import RQ_EXEC_AUTO, RQ_EXEC_PER_GATE, RQ_EXEC_SWEEP, RQ_F32, RQ_F64
+from ._capi import (RQ_EXEC_AUTO, RQ_EXEC_PER_GATE, RQ_EXEC_SWEEP, RQ_EXEC_SWEEP_TC, RQ_EXEC_SWEEP_TC_FAST, RQ_F32,
+                    RQ_F64)
 from .circuit import QuantumCircuit
 from .error import (CircuitError, CudaError, DeviceTimeout, InvalidArgument, InvalidQubitIndex, InvalidStateVector,
                     MemoryAllocationFailed, QuantumError, QubitLimitExceeded)
@@ -21,5 +22,6 @@ __all__ = [
     "ShotResult", "PauliOp", "PauliString", "Hamiltonian", "MeasurementOutcome", "SimulationMetrics",
     "QuantumError", "QubitLimitExceeded", "InvalidQubitIndex", "MemoryAllocationFailed", "InvalidStateVector",
     "CircuitError", "CudaError", "DeviceTimeout", "InvalidArgument", "MAX_QUBITS", "MAX_QUBITS_F32",
-    "RQ_F32", "RQ_F64", "RQ_EXEC_AUTO", "RQ_EXEC_PER_GATE", "RQ_EXEC_SWEEP",
+    "RQ_F32", "RQ_F64", "RQ_EXEC_AUTO", "RQ_EXEC_PER_GATE", "RQ_EXEC_SWEEP", "RQ_EXEC_SWEEP_TC",
+    "RQ_EXEC_SWEEP_TC_FAST",
 ]

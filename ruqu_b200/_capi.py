@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libruqu_cuda.so")
 
 RQ_F32, RQ_F64 = 0, 1
 RQ_QAOA_GRAD_ADJOINT, RQ_QAOA_GRAD_SHIFT = 0, 1
-RQ_EXEC_AUTO, RQ_EXEC_PER_GATE, RQ_EXEC_SWEEP = 0, 1, 2
+RQ_EXEC_AUTO, RQ_EXEC_PER_GATE, RQ_EXEC_SWEEP, RQ_EXEC_SWEEP_TC, RQ_EXEC_SWEEP_TC_FAST = 0, 1, 2, 3, 4
 
 (RQ_OK, RQ_ERR_QUBIT_LIMIT_EXCEEDED, RQ_ERR_INVALID_QUBIT_INDEX, RQ_ERR_MEMORY_ALLOCATION,
  RQ_ERR_INVALID_STATE_VECTOR, RQ_ERR_CIRCUIT, RQ_ERR_CUDA, RQ_ERR_TIMEOUT, RQ_ERR_INVALID_ARGUMENT) = range(9)
@@ -34,7 +34,7 @@ class RqPauliOp(C.Structure):
 
 class RqPlanStats(C.Structure):
     _fields_ = [("gates", C.c_uint64), ("launches", C.c_uint64), ("sweeps", C.c_uint64), ("phases", C.c_uint64),
-                ("ops", C.c_uint64), ("hbm_bytes", C.c_uint64)]
+                ("ops", C.c_uint64), ("hbm_bytes", C.c_uint64), ("dense_ops", C.c_uint64)]
 
 
 # name -> (restype, argtypes); every symbol here is declared in include/ruqu_cuda.h

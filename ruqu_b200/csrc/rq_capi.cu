@@ -351,15 +351,16 @@ int rq_device_count(int32_t* out) {
 
 int rq_plan_create(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out) {
     if (!s || !out || (!gates && n)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
-    if (mode < RQ_EXEC_AUTO || mode > RQ_EXEC_SWEEP) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "bad execution mode");
+    if (mode < RQ_EXEC_AUTO || mode > RQ_EXEC_SWEEP_TC_FAST)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "bad execution mode");
     for (uint64_t k = 0; k < n; ++k) {
         RQ_TRY(validate_gate(s, gates[k]));
         if (gates[k].kind == RQ_GATE_MEASURE || gates[k].kind == RQ_GATE_RESET)
             return rq::fail(RQ_ERR_CIRCUIT, "circuit error: a plan holds unitary gates only");
     }
     RQ_TRY(set_device(s));
-    int use_sweep = (mode == RQ_EXEC_SWEEP || (mode == RQ_EXEC_AUTO && s->nq >= 12)) && s->nq >= 7;
-    return rq::plan_build(s, gates, n, use_sweep ? RQ_EXEC_SWEEP : RQ_EXEC_PER_GATE, out);
+    int use_sweep = (mode != RQ_EXEC_PER_GATE && (mode != RQ_EXEC_AUTO || s->nq >= 12)) && s->nq >= 7;
+    return rq::plan_build(s, gates, n, use_sweep ? RQ_EXEC_SWEEP : RQ_EXEC_PER_GATE, out, rq::tc_passes_of(mode));
 }
 
 int rq_plan_execute(rq_state* s, const rq_plan* p) {
@@ -430,11 +431,12 @@ int rq_state_synchronize(rq_state* s) {
 int rq_state_apply_mode(rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_measurement* out,
                         uint64_t cap, uint64_t* nout) {
     if (!s || (!gates && n)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
-    if (mode < RQ_EXEC_AUTO || mode > RQ_EXEC_SWEEP) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "bad execution mode");
+    if (mode < RQ_EXEC_AUTO || mode > RQ_EXEC_SWEEP_TC_FAST)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "bad execution mode");
     RQ_TRY(set_device(s));
     for (uint64_t k = 0; k < n; ++k) RQ_TRY(validate_gate(s, gates[k]));
     // states below 7 qubits are smaller than one sweep tile: per-gate kernels
-    int use_sweep = (mode == RQ_EXEC_SWEEP || (mode == RQ_EXEC_AUTO && s->nq >= 12)) && s->nq >= 7;
+    int use_sweep = (mode != RQ_EXEC_PER_GATE && (mode != RQ_EXEC_AUTO || s->nq >= 12)) && s->nq >= 7;
     uint64_t nm = 0;
     uint64_t k = 0;
     while (k < n) {
@@ -460,7 +462,7 @@ int rq_state_apply_mode(rq_state* s, const rq_gate* gates, uint64_t n, int32_t m
             run.reserve(e - k);
             for (uint64_t j = k; j < e; ++j)
                 if (gates[j].kind != RQ_GATE_BARRIER) run.push_back(gates[j]);
-            RQ_TRY(rq::apply_sweeps(s, run.data(), run.size()));
+            RQ_TRY(rq::apply_sweeps(s, run.data(), run.size(), rq::tc_passes_of(mode)));
         } else {
             for (uint64_t j = k; j < e; ++j)
                 if (gates[j].kind != RQ_GATE_BARRIER) RQ_TRY(rq::apply_one_gate(s, gates[j]));

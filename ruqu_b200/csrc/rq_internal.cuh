@@ -100,8 +100,13 @@ int sample(rq_state* s, const uint32_t* qubits, uint32_t nq, uint64_t base_seed,
            uint64_t shots, uint64_t* host_out);
 
 // ---- fused sweeps and prepared plans (rq_sweep.cu) ---------------------------
-int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n);
-int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out);
+// tc_passes > 0: fuse each phase's slot-local gate runs into dense 32x32 unitaries
+// on the tensor cores (3 = 3xTF32, 1 = one TF32 pass); complex f32, m in {12, 13}
+int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n, int tc_passes = 0);
+int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out, int tc_passes = 0,
+               uint32_t tc_min_ops = 2);
+// the tensor-core passes a mode asks for (0: none)
+inline int tc_passes_of(int32_t mode) { return mode == RQ_EXEC_SWEEP_TC ? 3 : mode == RQ_EXEC_SWEEP_TC_FAST ? 1 : 0; }
 int plan_launch(rq_state* s, const rq_plan* p);
 void plan_free(rq_plan* p);
 rq_plan_stats plan_stats(const rq_plan* p);

@@ -8,9 +8,11 @@
 // earlier untaken gate (gates on disjoint qubits commute).
 #pragma once
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "rq_internal.cuh"
@@ -22,7 +24,10 @@ namespace rqp {
 // exp(-i*gamma_l*(|E| - 2 cut(x))) over all qubits (param = layer l);
 // RXP / RYP: Rx / Ry whose angle comes from the circuit's parameter table
 // (param = its index there).
-enum OpType : uint8_t { OP_U1 = 0, OP_D1 = 1, OP_CX = 2, OP_CZ = 3, OP_ZZ = 4, OP_CPH = 5, OP_RXP = 6, OP_RYP = 7 };
+// DENSE: a 32x32 complex unitary on the phase's five register slots, applied
+// on the tensor cores (param = index of its operand image).
+enum OpType : uint8_t { OP_U1 = 0, OP_D1 = 1, OP_CX = 2, OP_CZ = 3, OP_ZZ = 4, OP_CPH = 5, OP_RXP = 6, OP_RYP = 7,
+                        OP_DENSE = 8 };
 
 constexpr int RBMAX = 5;
 constexpr int MMAX = 14;
@@ -56,6 +61,7 @@ struct SweepDesc {
     uint32_t flags;             // SWEEP_INIT_UNIFORM | SWEEP_ENERGY (batched sweeps)
     uint64_t gj[1 << RBMAX];    // deposit of the per-thread vector offsets
     uint32_t sgj[1 << RBMAX];   // swz((tid-independent part of) the vector's first element)
+    uint32_t img_begin, img_count;   // dense operand images of this sweep (tensor-core sweeps)
 };
 
 constexpr uint32_t SWEEP_INIT_UNIFORM = 1u;   // synthesise |+>^n instead of loading the tile
@@ -79,9 +85,15 @@ inline uint64_t qmask(const PGate& g) {
     return m;
 }
 
-// qubits that must be register slots (and therefore local)
-inline uint64_t needs(const PGate& g) {
+// qubits that must be register slots (and therefore local).  With all_slots
+// (plans for dense tensor-core phases) every qubit a 1- or 2-qubit gate touches
+// is a slot, so whole gate runs stay inside the phase's 32-dimensional space.
+inline uint64_t needs(const PGate& g, bool all_slots = false) {
     if (g.type == OP_U1 || g.type == OP_RXP || g.type == OP_RYP) return 1ull << g.q0;
+    if (all_slots) {
+        if (g.type == OP_D1) return 1ull << g.q0;
+        if (g.type == OP_CX || g.type == OP_CZ || g.type == OP_ZZ) return (1ull << g.q0) | (1ull << g.q1);
+    }
     if (g.type == OP_CX) return 1ull << g.q1;
     return 0;
 }
@@ -139,7 +151,8 @@ struct Sweep {
     std::vector<PGate> ops;   // in execution order (after fusion)
 };
 
-inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c) {
+inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c,
+                                      bool all_slots = false) {
     std::vector<Sweep> out;
     std::vector<char> taken(gates.size(), 0);
     size_t first = 0;
@@ -157,7 +170,7 @@ inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t 
                 blocked |= qm;
                 continue;
             }
-            uint64_t L2 = sw.L | needs(g);
+            uint64_t L2 = sw.L | needs(g, all_slots);
             if ((uint32_t)__builtin_popcountll(L2) > m) {
                 blocked |= qm;
                 continue;
@@ -184,7 +197,7 @@ struct PhasePlan {
     std::vector<int> ops;     // indices into the sweep's op list
 };
 
-inline std::vector<PhasePlan> plan_phases(const Sweep& sw, uint32_t rb) {
+inline std::vector<PhasePlan> plan_phases(const Sweep& sw, uint32_t rb, bool all_slots = false) {
     std::vector<PhasePlan> out;
     std::vector<char> taken(sw.ops.size(), 0);
     size_t first = 0;
@@ -200,7 +213,7 @@ inline std::vector<PhasePlan> plan_phases(const Sweep& sw, uint32_t rb) {
                 blocked |= qm;
                 continue;
             }
-            uint64_t R2 = ph.R | needs(g);
+            uint64_t R2 = ph.R | needs(g, all_slots);
             if ((uint32_t)__builtin_popcountll(R2) > rb) {
                 blocked |= qm;
                 continue;
@@ -289,7 +302,7 @@ inline uint32_t swz_host(uint32_t e, uint32_t cb) {
 // op records and the f64 matrix entries (narrowed later for f32 states).
 inline void build_program(std::vector<Sweep>& sweeps, uint32_t nq, uint32_t m, uint32_t c, uint32_t rb,
                           uint32_t epv, std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& phases,
-                          std::vector<SwOp>& ops, std::vector<double>& mats) {
+                          std::vector<SwOp>& ops, std::vector<double>& mats, bool all_slots = false) {
     for (auto& sw : sweeps) {
         uint64_t L = sw.L;
         for (uint32_t q = 0; q < nq && (uint32_t)__builtin_popcountll(L) < m; ++q) L |= 1ull << q;
@@ -316,7 +329,7 @@ inline void build_program(std::vector<Sweep>& sweeps, uint32_t nq, uint32_t m, u
             d.sgj[j] = swz_host((uint32_t)x, cb);
         }
         d.phase_begin = (uint32_t)phases.size();
-        auto pplan = plan_phases(sw, rb);
+        auto pplan = plan_phases(sw, rb, all_slots);
         for (auto& pp : pplan) {
             PhaseDesc Ph{};
             Ph.op_begin = (uint32_t)ops.size();
@@ -364,4 +377,177 @@ inline void build_program(std::vector<Sweep>& sweeps, uint32_t nq, uint32_t m, u
     if (phases.empty()) phases.push_back(PhaseDesc{});
 }
 
+// ---- dense fusion for the tensor cores ----------------------------------
+//
+// In a phase every thread holds the 32 amplitudes spanned by the five register
+// slots, so any run of ops that only reads and writes slot bits is one 32x32
+// complex matrix, the same for every thread.  fuse_dense rewrites each phase:
+// ops touching a non-slot bit (a CNOT controlled by a thread bit, a diagonal
+// on a thread bit) are deferred past the slot-local ops that do not share a
+// qubit with them (gates on disjoint qubits commute), the slot-local ops
+// become one OP_DENSE when there are at least `min_ops` of them, and the
+// deferred ops follow in their original order.
+//
+// Operand image of a dense op, as the MMA's B operand: B[c][k] (c = output
+// 2i'+r', k = input 2i+r, r = 0 real / 1 imaginary part) is the real form of
+// U: B[2i'][2i] = Re U, B[2i'][2i+1] = -Im U, B[2i'+1][2i] = Im U,
+// B[2i'+1][2i+1] = Re U, stored in the no-swizzle K-major core-matrix layout
+// (element (c, k) at byte (c/8)*2048 + (k/4)*128 + (c%8)*16 + (k%4)*4), as a
+// TF32 high part followed by the FP32 remainder (16 KB each).
+constexpr int DENSE_FLOATS = 64 * 64;          // one 64x64 operand image
+constexpr int DENSE_IMAGE_FLOATS = 2 * DENSE_FLOATS;
+
+inline bool slot_local(const SwOp& o) {
+    switch (o.type) {
+        case OP_U1: case OP_D1: return o.k0 >= 0;
+        case OP_CX: case OP_CZ: case OP_ZZ: return o.k0 >= 0 && o.k1 >= 0;
+        default: return false;
+    }
+}
+
+inline uint64_t op_qubits(const SwOp& o) {
+    uint64_t m = 1ull << o.q0;
+    if (o.type == OP_CX || o.type == OP_CZ || o.type == OP_ZZ) m |= 1ull << o.q1;
+    return m;
+}
+
+// v <- op(v) on a 32-vector of register amplitudes (the kernel's op semantics)
+inline void apply_op32(const SwOp& o, const double* mt, double* v /* 64: re, im interleaved */) {
+    auto re = [&](int i) -> double& { return v[2 * i]; };
+    auto im = [&](int i) -> double& { return v[2 * i + 1]; };
+    if (o.type == OP_U1) {
+        const int b = 1 << o.k0;
+        for (int i = 0; i < 32; ++i) {
+            if (i & b) continue;
+            const int j = i | b;
+            const double xr = re(i), xi = im(i), yr = re(j), yi = im(j);
+            re(i) = mt[0] * xr - mt[1] * xi + mt[2] * yr - mt[3] * yi;
+            im(i) = mt[0] * xi + mt[1] * xr + mt[2] * yi + mt[3] * yr;
+            re(j) = mt[4] * xr - mt[5] * xi + mt[6] * yr - mt[7] * yi;
+            im(j) = mt[4] * xi + mt[5] * xr + mt[6] * yi + mt[7] * yr;
+        }
+    } else if (o.type == OP_D1) {
+        for (int i = 0; i < 32; ++i) {
+            const int bit = (i >> o.k0) & 1;
+            const double dr = bit ? mt[2] : mt[0], di = bit ? mt[3] : mt[1];
+            const double xr = re(i), xi = im(i);
+            re(i) = xr * dr - xi * di;
+            im(i) = xr * di + xi * dr;
+        }
+    } else if (o.type == OP_CX) {
+        const int t = 1 << o.k1;
+        for (int i = 0; i < 32; ++i)
+            if (!(i & t) && ((i >> o.k0) & 1)) {
+                std::swap(re(i), re(i | t));
+                std::swap(im(i), im(i | t));
+            }
+    } else if (o.type == OP_CZ) {
+        for (int i = 0; i < 32; ++i)
+            if (((i >> o.k0) & 1) && ((i >> o.k1) & 1)) { re(i) = -re(i); im(i) = -im(i); }
+    } else if (o.type == OP_ZZ) {
+        for (int i = 0; i < 32; ++i) {
+            const bool diff = (((i >> o.k0) ^ (i >> o.k1)) & 1) != 0;
+            const double dr = diff ? mt[2] : mt[0], di = diff ? mt[3] : mt[1];
+            const double xr = re(i), xi = im(i);
+            re(i) = xr * dr - xi * di;
+            im(i) = xr * di + xi * dr;
+        }
+    }
+}
+
+inline float tf32_round(float x) {
+    uint32_t b;
+    std::memcpy(&b, &x, 4);
+    if ((b & 0x7F800000u) != 0x7F800000u) {   // finite: round to nearest, ties away, at 10 mantissa bits
+        b += 0x1000u;
+        b &= 0xFFFFE000u;
+    }
+    float r;
+    std::memcpy(&r, &b, 4);
+    return r;
+}
+
+inline size_t dense_offset(int c, int k) {   // in floats
+    return (size_t)(c / 8) * 512 + (size_t)(k / 4) * 32 + (size_t)(c % 8) * 4 + (size_t)(k % 4);
+}
+
+// U (column-major over inputs: U[i][col] = amplitude i of the image of basis col) -> operand image
+inline void dense_image(const std::vector<double>& U /* 32 x 32 complex, [col][i] re/im */, float* out) {
+    for (int col = 0; col < 32; ++col)
+        for (int i = 0; i < 32; ++i) {
+            const double ur = U[(size_t)col * 64 + 2 * i], ui = U[(size_t)col * 64 + 2 * i + 1];
+            // output i, input col
+            const double vals[2][2] = {{ur, -ui}, {ui, ur}};
+            for (int rp = 0; rp < 2; ++rp)
+                for (int r = 0; r < 2; ++r) {
+                    const double x = vals[rp][r];
+                    const float f = (float)x;
+                    const float hi = tf32_round(f);
+                    const float lo = (float)(x - (double)hi);
+                    const size_t off = dense_offset(2 * i + rp, 2 * col + r);
+                    out[off] = hi;
+                    out[DENSE_FLOATS + off] = lo;
+                }
+        }
+}
+
+// Rewrites ops/phases in place; appends the operand images of the new dense ops
+// (in phase order, so a sweep's images are consecutive) and records each sweep's
+// image range; at most max_per_sweep dense ops per sweep (they stay resident in
+// shared memory during the sweep's launch).
+inline void fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& phases, std::vector<SwOp>& ops,
+                       const std::vector<double>& mats, uint32_t min_ops, uint32_t max_per_sweep,
+                       std::vector<float>& images, uint64_t* ndense) {
+    std::vector<SwOp> out;
+    std::vector<uint32_t> sweep_of(phases.size(), 0);
+    for (size_t d = 0; d < descs.size(); ++d) {
+        for (uint32_t p = descs[d].phase_begin; p < descs[d].phase_end; ++p) sweep_of[p] = (uint32_t)d;
+        descs[d].img_begin = 0;
+        descs[d].img_count = 0;
+    }
+    for (size_t pi = 0; pi < phases.size(); ++pi) {
+        auto& ph = phases[pi];
+        SweepDesc& sd = descs[sweep_of[pi]];
+        std::vector<SwOp> dense, deferred;
+        uint64_t held = 0;
+        for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
+            const SwOp& op = ops[o];
+            if (slot_local(op) && !(op_qubits(op) & held)) {
+                dense.push_back(op);
+            } else {
+                deferred.push_back(op);
+                held |= op_qubits(op);
+            }
+        }
+        const uint32_t begin = (uint32_t)out.size();
+        if (dense.size() >= min_ops && min_ops > 0 && sd.img_count < max_per_sweep) {
+            std::vector<double> U(32 * 64, 0.0);
+            for (int col = 0; col < 32; ++col) {
+                double* v = &U[(size_t)col * 64];
+                v[2 * col] = 1.0;
+                for (const auto& op : dense) apply_op32(op, mats.data() + 2 * (size_t)op.mat, v);
+            }
+            const size_t idx = images.size() / DENSE_IMAGE_FLOATS;
+            if (sd.img_count == 0) sd.img_begin = (uint32_t)idx;
+            ++sd.img_count;
+            images.resize(images.size() + DENSE_IMAGE_FLOATS);
+            dense_image(U, images.data() + idx * DENSE_IMAGE_FLOATS);
+            SwOp d{};
+            d.type = OP_DENSE;
+            d.k0 = d.k1 = -1;
+            d.mat = (uint32_t)idx;
+            out.push_back(d);
+            for (const auto& op : deferred) out.push_back(op);
+            ++*ndense;
+        } else {
+            for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) out.push_back(ops[o]);
+        }
+        ph.op_begin = begin;
+        ph.op_end = (uint32_t)out.size();
+    }
+    if (out.empty()) out.push_back(SwOp{});
+    ops.swap(out);
+}
+
 }  // namespace rqp
+

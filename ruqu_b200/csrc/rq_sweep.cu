@@ -187,7 +187,105 @@ __device__ __forceinline__ void run_phases(typename C2<T>::t* sm, const SweepDes
     }
 }
 
+// Variant of run_phases: register addresses composed by XOR from the five slot
+// offsets (no table loads), and the next op and its matrix fetched while the
+// current op runs.
 template <typename T, int RB>
+__device__ __forceinline__ void run_phases_v1(typename C2<T>::t* sm, const SweepDesc& d,
+                                           const PhaseDesc* __restrict__ phases, const SwOp* __restrict__ ops,
+                                           const T* __restrict__ mats, uint64_t base, uint32_t tid) {
+    using V = typename C2<T>::t;
+    constexpr int NR = 1 << RB;
+    for (uint32_t p = d.phase_begin; p < d.phase_end; ++p) {
+        const PhaseDesc& ph = phases[p];
+        uint32_t ebase = 0;
+        uint64_t U = base;
+        for (uint32_t b = 0; b < ph.nt; ++b)
+            if ((tid >> b) & 1u) {
+                ebase |= 1u << ph.tbit_local[b];
+                U |= 1ull << ph.tbit_global[b];
+            }
+        const uint32_t sb = swz<T>(ebase);
+        uint32_t S[RB];
+#pragma unroll
+        for (int k = 0; k < RB; ++k) S[k] = ph.slut[1 << k];
+        auto addr = [&](int i) {
+            uint32_t a = sb;
+#pragma unroll
+            for (int k = 0; k < RB; ++k)
+                if ((i >> k) & 1) a ^= S[k];
+            return a;
+        };
+        V reg[NR];
+#pragma unroll
+        for (int i = 0; i < NR; ++i) reg[i] = sm[addr(i)];
+
+        SwOp nop = ops[ph.op_begin];
+        T nm[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) nm[k] = mats[2 * nop.mat + k];
+        for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
+            const SwOp op = nop;
+            T mm[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) mm[k] = nm[k];
+            if (o + 1 < ph.op_end) {
+                nop = ops[o + 1];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) nm[k] = mats[2 * nop.mat + k];
+            }
+            switch (op.type) {
+                case OP_U1: dispatch_u1<NR>(op.k0, reg, mm); break;
+                case OP_CX: dispatch_cx<NR>(op.k1, reg, op.k0, (int)((U >> op.q0) & 1ull)); break;
+                case OP_D1: {
+                    const T d0r = mm[0], d0i = mm[1], d1r = mm[2], d1i = mm[3];
+                    const int kk = op.k0;
+                    const int ub = (int)((U >> op.q0) & 1ull);
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) {
+                        const int b = kk >= 0 ? ((i >> kk) & 1) : ub;
+                        reg[i] = cmul(reg[i], b ? d1r : d0r, b ? d1i : d0i);
+                    }
+                    break;
+                }
+                case OP_CZ: {
+                    const int k0 = op.k0, k1 = op.k1;
+                    const int u0 = (int)((U >> op.q0) & 1ull), u1 = (int)((U >> op.q1) & 1ull);
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) {
+                        const int b0 = k0 >= 0 ? ((i >> k0) & 1) : u0;
+                        const int b1 = k1 >= 0 ? ((i >> k1) & 1) : u1;
+                        if (b0 & b1) {
+                            reg[i].x = -reg[i].x;
+                            reg[i].y = -reg[i].y;
+                        }
+                    }
+                    break;
+                }
+                case OP_ZZ: {
+                    // diag(en, ep, ep, en): en for equal bits, ep for different bits
+                    const T er = mm[0], ei = mm[1], pr = mm[2], pi = mm[3];
+                    const int k0 = op.k0, k1 = op.k1;
+                    const int u0 = (int)((U >> op.q0) & 1ull), u1 = (int)((U >> op.q1) & 1ull);
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) {
+                        const int b0 = k0 >= 0 ? ((i >> k0) & 1) : u0;
+                        const int b1 = k1 >= 0 ? ((i >> k1) & 1) : u1;
+                        const bool diff = (b0 ^ b1) != 0;
+                        reg[i] = cmul(reg[i], diff ? pr : er, diff ? pi : ei);
+                    }
+                    break;
+                }
+                default: break;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NR; ++i) sm[addr(i)] = reg[i];
+        __syncthreads();
+    }
+}
+
+template <typename T, int RB, bool PV>
 __global__ void __launch_bounds__(256, 2) k_sweep(typename C2<T>::t* __restrict__ amps, const SweepDesc d,
                                                const PhaseDesc* __restrict__ phases, const SwOp* __restrict__ ops,
                                                const T* __restrict__ mats, uint64_t ntiles) {
@@ -239,7 +337,8 @@ __global__ void __launch_bounds__(256, 2) k_sweep(typename C2<T>::t* __restrict_
         __syncthreads();
 
         // ---- phases ----
-        run_phases<T, RB>(sm, d, phases, ops, mats, base, tid);
+        if (PV) run_phases_v1<T, RB>(sm, d, phases, ops, mats, base, tid);
+        else run_phases<T, RB>(sm, d, phases, ops, mats, base, tid);
 
         // ---- store tile ----
 #pragma unroll
@@ -297,7 +396,7 @@ __device__ __forceinline__ void issue_tile(typename C2<T>::t* buf, const typenam
 // Persistent, double-buffered sweep: one CTA per SM walks tiles blockIdx.x,
 // blockIdx.x + gridDim.x, ...; the copies of tile k+1 are in flight while the
 // phases of tile k run and its stores drain.
-template <typename T, int RB>
+template <typename T, int RB, bool PV>
 __global__ void __launch_bounds__(256, 1) k_sweep_pipe(typename C2<T>::t* __restrict__ amps, const SweepDesc d,
                                                      const PhaseDesc* __restrict__ phases,
                                                      const SwOp* __restrict__ ops, const T* __restrict__ mats,
@@ -341,7 +440,8 @@ __global__ void __launch_bounds__(256, 1) k_sweep_pipe(typename C2<T>::t* __rest
         cp_async_wait1();          // this thread's copies of the current tile have landed
         __syncthreads();           // ... and everyone else's
         const uint64_t base = tile_base(tile);
-        run_phases<T, RB>(sm, d, phases, ops, mats, base, tid);
+        if (PV) run_phases_v1<T, RB>(sm, d, phases, ops, mats, base, tid);
+        else run_phases<T, RB>(sm, d, phases, ops, mats, base, tid);
 #pragma unroll
         for (int j = 0; j < VPT; ++j) {
             const uint32_t se = stid ^ d.sgj[j];
@@ -363,15 +463,374 @@ __global__ void __launch_bounds__(256, 1) k_sweep_pipe(typename C2<T>::t* __rest
 }
 
 // ---------------------------------------------------------------------------
+// Tensor-core sweeps: dense 32x32 phase unitaries as TF32 MMAs (tcgen05)
+// ---------------------------------------------------------------------------
+//
+// Complex f32 states, m = 13 local qubits (256 threads x 32 register
+// amplitudes) or m = 12 (128 threads); two CTAs per SM, so one CTA's copies
+// and MMAs overlap the other's CUDA-core work.  The sweep's phase and op
+// descriptors are copied into shared memory at the start.  At the start of a
+// phase whose first op is an OP_DENSE, one thread starts a bulk copy of the
+// op's operand image (B, 64x64 TF32 values, plus the FP32 remainder for 3
+// passes) into shared memory.  The dense op: every thread stores its 32
+// amplitudes (64 floats: re, im of register amplitude 0, 1, ...) into its own
+// tensor-memory lane as row n = tid of the A operand (TF32 high part); one
+// thread issues, per 128-row half, the K = 64 products in steps of 8 into a
+// 128 x 64 FP32 accumulator; for 3xTF32 the same A is multiplied by the
+// image's remainder, then A is overwritten with the FP32 remainder of the
+// amplitudes and multiplied by the high image; tcgen05.commit signals an
+// mbarrier and every thread reads its row of the accumulator back
+// (tcgen05.ld) as its 32 new amplitudes.  Tensor memory (256 columns per CTA):
+// accumulator [0, 128), A [128, 256); half h of the rows uses columns 64h..
+namespace tc {
+
+constexpr uint32_t B_SBO = 2048;   // bytes between 8-row groups of an image (16 core matrices along K)
+constexpr uint32_t B_LBO = 128;    // bytes between core matrices along K
+constexpr uint32_t COL_D = 0, COL_A = 128, NCOLS = 256;
+
+__device__ int g_tc_timeout = 0;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
+    d |= (uint64_t)(B_LBO >> 4) << 16;
+    d |= (uint64_t)(B_SBO >> 4) << 32;
+    d |= (uint64_t)1 << 46;   // sm_100 descriptor version; no swizzle, base offset 0
+    return d;
+}
+
+// TF32 x TF32 -> F32, both operands K-major, M = 128, N = 64
+constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (uint32_t it = 0; it < (1u << 24); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ float to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// 16 accumulator columns of this thread's lane -> 8 complex amplitudes
+__device__ __forceinline__ void ld16(uint32_t taddr, float2* out) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int j = 0; j < 8; ++j) out[j] = make_float2(__uint_as_float(r[2 * j]), __uint_as_float(r[2 * j + 1]));
+}
+
+__device__ __forceinline__ void st16(uint32_t taddr, const float* v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+        ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+        "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+        "r"(__float_as_uint(v[15]))
+        : "memory");
+}
+
+struct TcCtx {
+    float* img;          // shared-memory image buffer
+    uint32_t img_bytes;  // bytes copied per image (1 pass: high part only)
+    uint64_t* bar;       // MMA completion
+    uint64_t* ibar;      // image copy completion
+    uint32_t tmem;
+    uint32_t parity, iparity;
+    int passes;
+    bool failed;
+};
+
+// thread 0: bulk copy of one operand image into shared memory, completion on ibar
+__device__ __forceinline__ void start_image(TcCtx& c, const float* src) {
+    const uint32_t b = smem_u32(c.ibar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(c.img_bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(c.img)),
+                 "l"(src), "r"(c.img_bytes), "r"(b)
+                 : "memory");
+}
+
+__device__ __forceinline__ void store_a(TcCtx& c, const float2* reg, uint32_t taddr, bool low) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float h[16];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const float2 v = reg[8 * q + j];
+            const float hx = to_tf32(v.x), hy = to_tf32(v.y);
+            h[2 * j] = low ? v.x - hx : hx;
+            h[2 * j + 1] = low ? v.y - hy : hy;
+        }
+        st16(taddr + 16 * q, h);
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+// thread 0: the products of A (tensor memory) with one image part, into the accumulator
+__device__ __forceinline__ void issue(TcCtx& c, uint32_t bsmem, uint32_t halves, bool first) {
+    for (uint32_t h = 0; h < halves; ++h)
+        for (int ks = 0; ks < 8; ++ks) {
+            const uint64_t bd = sdesc(bsmem + ks * 2 * B_LBO);
+            const uint32_t acc = (!first || ks > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                ::"r"(c.tmem + COL_D + h * 64), "r"(c.tmem + COL_A + h * 64 + ks * 8), "l"(bd), "r"(IDESC),
+                "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                : "memory");
+        }
+}
+
+// waits on the MMA barrier; a wait that runs out marks the CTA failed (uniformly)
+__device__ __forceinline__ bool commit_wait(TcCtx& c, uint32_t tid) {
+    if (tid == 0)
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(c.bar))
+                     : "memory");
+    const bool late = !mbar_wait(c.bar, c.parity);
+    c.parity ^= 1u;
+    if (__syncthreads_or(late)) {
+        c.failed = true;
+        if (tid == 0) g_tc_timeout = 1;
+        return false;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    return true;
+}
+
+// One OP_DENSE on the CTA's registers.  All threads call it (uniform control flow).
+__device__ __forceinline__ void dense_op(TcCtx& c, float2* reg, uint32_t tid, uint32_t nthreads) {
+    const uint32_t warp = tid >> 5;
+    const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
+    const uint32_t half_col = (warp >> 2) * 64u;
+    const uint32_t halves = nthreads / 128;
+    store_a(c, reg, c.tmem + lane_base + COL_A + half_col, false);
+    // the image copy started at the phase start
+    const bool late = !mbar_wait(c.ibar, c.iparity);
+    c.iparity ^= 1u;
+    if (__syncthreads_or(late)) {
+        c.failed = true;
+        if (tid == 0) g_tc_timeout = 1;
+        return;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t bhi = smem_u32(c.img), blo = smem_u32(c.img + DENSE_FLOATS);
+    if (tid == 0) {
+        issue(c, bhi, halves, true);
+        if (c.passes > 1) issue(c, blo, halves, false);
+    }
+    if (!commit_wait(c, tid)) return;
+    if (c.passes > 1) {
+        store_a(c, reg, c.tmem + lane_base + COL_A + half_col, true);
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) issue(c, bhi, halves, false);
+        if (!commit_wait(c, tid)) return;
+    }
+    const uint32_t taddr = c.tmem + lane_base + COL_D + half_col;
+    ld16(taddr, reg);
+    ld16(taddr + 16, reg + 8);
+    ld16(taddr + 32, reg + 16);
+    ld16(taddr + 48, reg + 24);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+}  // namespace tc
+
+// run_phases for the tensor-core sweep (complex f32, RB = 5).  With every gate
+// qubit planned onto a register slot, each phase of such a plan is exactly
+// one OP_DENSE (the planner checks this).
+__device__ __forceinline__ void run_phases_tc(float2* sm, const SweepDesc& d, const PhaseDesc* phases,
+                                              const SwOp* ops, const float* __restrict__ images, uint32_t tid,
+                                              uint32_t nthreads, tc::TcCtx& c) {
+    using V = float2;
+    constexpr int NR = 32;
+    for (uint32_t p = d.phase_begin; p < d.phase_end; ++p) {
+        const PhaseDesc& ph = phases[p];
+        if (tid == 0) tc::start_image(c, images + (size_t)ops[ph.op_begin].mat * DENSE_IMAGE_FLOATS);
+        uint32_t ebase = 0;
+        for (uint32_t b = 0; b < ph.nt; ++b)
+            if ((tid >> b) & 1u) ebase |= 1u << ph.tbit_local[b];
+        const uint32_t sb = swz<float>(ebase);
+        // register addresses: XOR combinations of the five slot offsets (read again for the store,
+        // after the dense op, so that they are not held across it)
+        auto addr = [&](int i, const uint32_t* S) {
+            uint32_t a = sb;
+#pragma unroll
+            for (int k = 0; k < 5; ++k)
+                if ((i >> k) & 1) a ^= S[k];
+            return a;
+        };
+        V reg[NR];
+        {
+            uint32_t S[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) S[k] = ph.slut[1 << k];
+#pragma unroll
+            for (int i = 0; i < NR; ++i) reg[i] = sm[addr(i, S)];
+        }
+        tc::dense_op(c, reg, tid, nthreads);
+        if (c.failed) return;
+        {
+            uint32_t S[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) S[k] = ph.slut[1 << k];
+#pragma unroll
+            for (int i = 0; i < NR; ++i) sm[addr(i, S)] = reg[i];
+        }
+        __syncthreads();
+    }
+}
+
+// Tensor-core sweep kernel, persistent over tiles, two CTAs per SM.  Shared
+// memory: tile | image buffer | the sweep's phase and op descriptors.  Tensor
+// memory is allocated once per CTA and always freed, also after a timed-out wait.
+__global__ void __launch_bounds__(256, 2) k_sweep_tc(float2* __restrict__ amps, const SweepDesc d,
+                                                   const PhaseDesc* __restrict__ phases, const SwOp* __restrict__ ops,
+                                                   const float* __restrict__ mats, const float* __restrict__ images,
+                                                   uint64_t ntiles, int passes) {
+    using V = float2;
+    using VV = float4;
+    constexpr int EPV = 2;
+    constexpr int VPT = 32 / EPV;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t tile_elems = 1u << d.m;
+    V* sm = reinterpret_cast<V*>(smem_raw);
+    float* img = reinterpret_cast<float*>(sm + tile_elems);
+    const uint32_t img_bytes = (passes > 1 ? DENSE_IMAGE_FLOATS : DENSE_FLOATS) * 4u;
+    PhaseDesc* sph = reinterpret_cast<PhaseDesc*>(reinterpret_cast<unsigned char*>(img) + img_bytes);
+    const uint32_t nph = d.phase_end - d.phase_begin;
+    const uint32_t op0 = phases[d.phase_begin].op_begin, nops = phases[d.phase_end - 1].op_end - op0;
+    SwOp* sop = reinterpret_cast<SwOp*>(sph + nph);
+    __shared__ __align__(8) uint64_t bar, ibar;
+    __shared__ uint32_t tmem_base;
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t T_ = blockDim.x;
+    for (uint32_t k = tid; k < nph * (uint32_t)(sizeof(PhaseDesc) / 16); k += T_)
+        reinterpret_cast<uint4*>(sph)[k] = reinterpret_cast<const uint4*>(phases + d.phase_begin)[k];
+    for (uint32_t k = tid; k < nops; k += T_) sop[k] = ops[op0 + k];
+    tc::TcCtx c;
+    c.img = img;
+    c.img_bytes = img_bytes;
+    c.bar = &bar;
+    c.ibar = &ibar;
+    c.parity = 0;
+    c.iparity = 0;
+    c.passes = passes;
+    c.failed = false;
+    if (tid < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(&tmem_base)),
+                     "r"(tc::NCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc::smem_u32(&bar)), "r"(1u) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc::smem_u32(&ibar)), "r"(1u) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    c.tmem = tmem_base;
+    const PhaseDesc* lph = sph - d.phase_begin;   // indexable by the sweep's global phase numbers
+    const SwOp* lop = sop - op0;
+
+    const uint64_t cmask = (1ull << d.c) - 1;
+    uint64_t dep_tid = 0;
+    {
+        uint64_t x = (uint64_t)tid * EPV;
+        dep_tid = x & cmask;
+        for (uint32_t b = d.c; b < d.m; ++b)
+            if ((x >> b) & 1ull) dep_tid |= 1ull << d.local_global[b];
+    }
+    const uint32_t stid = swz<float>(tid * EPV);
+
+    for (uint64_t tile = blockIdx.x; tile < ntiles && !c.failed; tile += gridDim.x) {
+        uint64_t base = 0;
+        for (uint32_t b = 0; b < d.nonlocal_count; ++b)
+            if ((tile >> b) & 1ull) base |= 1ull << d.nonlocal[b];
+#pragma unroll 1
+        for (int j0 = 0; j0 < VPT; j0 += 4) {
+            VV v[4];
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj)
+                v[jj] = __ldcs(reinterpret_cast<const VV*>(amps + (base | dep_tid | d.gj[j0 + jj])));
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                const uint32_t se = stid ^ d.sgj[j0 + jj];
+                sm[se] = make_float2(v[jj].x, v[jj].y);
+                sm[se ^ 1u] = make_float2(v[jj].z, v[jj].w);
+            }
+        }
+        __syncthreads();
+        run_phases_tc(sm, d, lph, lop, images, tid, T_, c);
+        if (c.failed) break;
+#pragma unroll
+        for (int j = 0; j < VPT; ++j) {
+            const uint32_t se = stid ^ d.sgj[j];
+            const uint64_t g = base | dep_tid | d.gj[j];
+            float2 a = sm[se], b = sm[se ^ 1u];
+            __stcs(reinterpret_cast<VV*>(amps + g), make_float4(a.x, a.y, b.x, b.y));
+        }
+        __syncthreads();
+    }
+    // after a timed-out wait, give the outstanding copy and MMAs a bounded chance to land before freeing
+    if (c.failed) {
+        tc::mbar_wait(&bar, c.parity ^ 1u);
+        tc::mbar_wait(&ibar, c.iparity ^ 1u);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid < 32) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(c.tmem), "r"(tc::NCOLS) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host planner
 // ---------------------------------------------------------------------------
 
-// Double-buffered persistent sweeps (default); RUQU_SWEEP_PIPE=0 selects the
-// single-buffered kernel with two CTAs per SM.
+// RUQU_SWEEP_PIPE=1 selects the double-buffered persistent kernel (one CTA per
+// SM); the default is the single-buffered kernel with two CTAs per SM.
 static bool sweep_pipelined() {
     static const bool on = [] {
         const char* e = std::getenv("RUQU_SWEEP_PIPE");
-        return !(e && e[0] == '0');
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+
+static bool phase_v1() {
+    static const bool on = [] {
+        const char* e = std::getenv("RUQU_PHASE_V");
+        return e && e[0] == '1';
     }();
     return on;
 }
@@ -383,7 +842,8 @@ int launch_sweep(rq_state* s, const SweepDesc& d, const PhaseDesc* ph, const SwO
     unsigned threads = 1u << (d.m - rb);
     int sms = rq::num_sms(s->device);
     if (sweep_pipelined()) {
-        auto kp = k_sweep_pipe<T, std::is_same<T, float>::value ? 5 : 4>;
+        auto kp = phase_v1() ? k_sweep_pipe<T, std::is_same<T, float>::value ? 5 : 4, true>
+                             : k_sweep_pipe<T, std::is_same<T, float>::value ? 5 : 4, false>;
         const size_t smem2 = 2 * smem;
         RQ_CUDA(cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
         int per_sm = 0;
@@ -395,7 +855,8 @@ int launch_sweep(rq_state* s, const SweepDesc& d, const PhaseDesc* ph, const SwO
             return RQ_OK;
         }
     }
-    auto kern = k_sweep<T, std::is_same<T, float>::value ? 5 : 4>;
+    auto kern = phase_v1() ? k_sweep<T, std::is_same<T, float>::value ? 5 : 4, true>
+                           : k_sweep<T, std::is_same<T, float>::value ? 5 : 4, false>;
     RQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     // persistent grid: exactly the CTAs that can be resident at once
     int per_sm = 0;
@@ -418,8 +879,10 @@ struct rq_plan {
     int32_t mode = RQ_EXEC_SWEEP;
     std::vector<rq_gate> gates;          // per-gate mode
     std::vector<SweepDesc> descs;        // sweep mode: one launch each
-    unsigned char* dev = nullptr;        // phases | ops | matrices
-    size_t off_ph = 0, off_ops = 0, off_mat = 0;
+    unsigned char* dev = nullptr;        // phases | ops | matrices | dense operand images
+    size_t off_ph = 0, off_ops = 0, off_mat = 0, off_img = 0;
+    int tc_passes = 0;                   // > 0: tensor-core sweeps (3 = 3xTF32, 1 = TF32)
+    std::vector<PhaseDesc> host_phases;  // tensor-core sweeps: descriptor sizes per launch
     uint64_t ntiles = 0;
     size_t smem = 0;
     uint32_t rb = 0;
@@ -438,7 +901,10 @@ static uint32_t sweep_local_qubits(uint32_t nq, int32_t prec) {
     return std::min(nq, m);
 }
 
-int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out) {
+// tc_passes > 0 fuses each phase's slot-local ops (at least tc_min_ops of them) into one
+// dense 32x32 op applied on the tensor cores (complex f32 states, m in {12, 13} only).
+int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out, int tc_passes,
+               uint32_t tc_min_ops) {
     rq_plan* P = new rq_plan();
     P->nq = s->nq;
     P->prec = s->prec;
@@ -465,6 +931,7 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
     }
     P->mode = RQ_EXEC_SWEEP;
     const uint32_t m = sweep_local_qubits(nq, s->prec);
+    if (s->prec != RQ_F32 || (m != 12 && m != 13)) tc_passes = 0;   // the tensor-core sweep's tile shapes
     const uint32_t c = std::min<uint32_t>(m, 5);
     std::vector<PGate> pg;
     std::vector<rq_gate> filtered;
@@ -474,19 +941,35 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
         delete P;
         return fail(RQ_ERR_CIRCUIT, "circuit error: only unitary gates can be planned");
     }
-    auto sweeps = plan_sweeps(pg, nq, m, c);
+    const bool tcp = tc_passes > 0;
+    auto sweeps = plan_sweeps(pg, nq, m, c, tcp);
 
     std::vector<PhaseDesc> phases;
     std::vector<SwOp> ops;
     std::vector<double> mats;
-    build_program(sweeps, nq, m, c, rb, s->prec == RQ_F32 ? 2 : 1, P->descs, phases, ops, mats);
+    build_program(sweeps, nq, m, c, rb, s->prec == RQ_F32 ? 2 : 1, P->descs, phases, ops, mats, tcp);
+    std::vector<float> images;
+    uint64_t ndense = 0;
+    if (tcp) {
+        // images resident in shared memory next to one tile
+        fuse_dense(P->descs, phases, ops, mats, 1, UINT32_MAX, images, &ndense);
+        for (const auto& ph : phases)
+            if (ph.op_end != ph.op_begin + 1 || ops[ph.op_begin].type != OP_DENSE) {
+                delete P;
+                return fail(RQ_ERR_CIRCUIT, "tensor-core plan: a phase is not one dense op");
+            }
+        P->tc_passes = tc_passes;
+        P->mode = RQ_EXEC_SWEEP_TC;
+    }
 
     size_t mat_elem = s->prec == RQ_F32 ? sizeof(float) : sizeof(double);
     P->off_ph = 0;
     P->off_ops = (P->off_ph + phases.size() * sizeof(PhaseDesc) + 255) & ~size_t(255);
     P->off_mat = (P->off_ops + ops.size() * sizeof(SwOp) + 255) & ~size_t(255);
-    size_t total = P->off_mat + mats.size() * mat_elem;
+    P->off_img = (P->off_mat + mats.size() * mat_elem + 255) & ~size_t(255);
+    size_t total = P->off_img + images.size() * sizeof(float);
     std::vector<unsigned char> host(total);
+    if (!images.empty()) std::memcpy(host.data() + P->off_img, images.data(), images.size() * sizeof(float));
     std::memcpy(host.data() + P->off_ph, phases.data(), phases.size() * sizeof(PhaseDesc));
     std::memcpy(host.data() + P->off_ops, ops.data(), ops.size() * sizeof(SwOp));
     if (s->prec == RQ_F32) {
@@ -503,6 +986,7 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
         return cuda_fail(e, "plan upload");
     }
     P->smem = ((size_t)1 << m) * s->elem_bytes();
+    if (tcp) P->host_phases = phases;
     P->ntiles = 1ull << (nq - m);
     P->rb = rb;
     P->stats.gates = filtered.size();
@@ -510,6 +994,7 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
     P->stats.launches = P->descs.size();
     P->stats.phases = phases.size();
     P->stats.ops = ops.size();
+    P->stats.dense_ops = ndense;
     P->stats.hbm_bytes = 2 * S * P->descs.size();
     *out = P;
     return RQ_OK;
@@ -525,6 +1010,23 @@ int plan_launch(rq_state* s, const rq_plan* P) {
     const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(P->dev + P->off_ph);
     const SwOp* op = reinterpret_cast<const SwOp*>(P->dev + P->off_ops);
     const void* mt = P->dev + P->off_mat;
+    if (P->tc_passes > 0) {
+        const float* img = reinterpret_cast<const float*>(P->dev + P->off_img);
+        const size_t img_bytes = (P->tc_passes > 1 ? DENSE_IMAGE_FLOATS : DENSE_FLOATS) * sizeof(float);
+        const unsigned threads = 1u << (P->descs.front().m - 5);
+        const unsigned grid = (unsigned)std::min<uint64_t>(P->ntiles, 2ull * (uint64_t)rq::num_sms(s->device));
+        const PhaseDesc* hph = P->host_phases.data();
+        for (const auto& d : P->descs) {
+            const size_t nph = d.phase_end - d.phase_begin;
+            const size_t nops = hph[d.phase_end - 1].op_end - hph[d.phase_begin].op_begin;
+            const size_t smem = P->smem + img_bytes + nph * sizeof(PhaseDesc) + nops * sizeof(SwOp);
+            RQ_CUDA(cudaFuncSetAttribute(k_sweep_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_sweep_tc<<<grid, threads, smem, s->stream>>>((float2*)s->amps, d, ph, op, (const float*)mt, img,
+                                                          P->ntiles, P->tc_passes);
+            RQ_CUDA(cudaGetLastError());
+        }
+        return RQ_OK;
+    }
     for (const auto& d : P->descs) {
         if (s->prec == RQ_F32) RQ_TRY(launch_sweep<float>(s, d, ph, op, mt, P->ntiles, P->rb, P->smem));
         else RQ_TRY(launch_sweep<double>(s, d, ph, op, mt, P->ntiles, P->rb, P->smem));
@@ -547,10 +1049,10 @@ bool plan_fits(const rq_plan* p, const rq_state* s) {
     return p->nq == s->nq && p->prec == s->prec && p->device == s->device;
 }
 
-int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n) {
+int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n, int tc_passes) {
     if (n == 0) return RQ_OK;
     rq_plan* P = nullptr;
-    RQ_TRY(plan_build(s, gates, n, RQ_EXEC_SWEEP, &P));
+    RQ_TRY(plan_build(s, gates, n, RQ_EXEC_SWEEP, &P, tc_passes));
     int rc = plan_launch(s, P);
     // cudaFree of the program waits for the launches that read it
     plan_free(P);
