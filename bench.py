@@ -5,15 +5,20 @@ Workload: random-layer circuit on 30 qubits (2^30 amplitudes, complex f32 =
 and a CNOT brickwork (even pairs on even layers, odd pairs on odd layers).
 A step is one full simulation: |0...0> initialisation plus the 20 layers.
 
-value   -- HBM GB/s of the device work with the prepared gate program
-           resident on the GPU: algorithmic bytes (S for the |0> write, 2S per
-           full sweep over the state) / device time (CUDA events on the
-           state's stream), summed over ranks / max time over ranks.
+value   -- per-gate-layer HBM GB/s: (S for the |0> write + 2S per layer, the
+           read and write of the state that one pass per layer needs) / device
+           time of the step (CUDA events on the state's stream), with the
+           prepared plan resident on the GPU; summed over ranks / max time.
 e2e     -- the same bytes through the public API with host buffers: reset,
            apply(host gate list), read <Z_i> for all qubits back to the host;
            wall-clock per step.
-roofline-- the dominant kernel (the multi-gate sweep): 2S per launch / its
-           average launch time, against the measured HBM copy bandwidth.
+roofline-- the dominant kernel (the sweep kernel the plan launches): 2S per
+           launch / its average launch time, against the measured HBM copy
+           bandwidth.
+variants-- one run of each execution mode (unfused per-gate kernels, CUDA-core
+           sweeps, 3xTF32 and one-pass TF32 tensor-core sweeps) with its
+           per-layer GB/s and its max-abs amplitude error against the complex
+           f64 run of the same circuit.
 
 N>1 ranks (torchrun) run independent replicas (the state does not shard on
 one node at this size): weak scaling, no collective on the data path.
@@ -57,6 +62,7 @@ def _args():
     ap.add_argument("--no-vqe", action="store_true", help="skip the batched VQE leg")
     ap.add_argument("--vqe-sets", type=int, default=512)
     ap.add_argument("--no-warm", action="store_true", help="skip the warm-start leg")
+    ap.add_argument("--no-variants", action="store_true", help="skip the per-mode runs and the f64 comparison")
     ap.add_argument("--warm-train", type=int, default=2048, help="training graphs for the warm start")
     ap.add_argument("--warm-eval", type=int, default=256, help="held-out graphs for the warm start")
     return ap.parse_args()
@@ -297,6 +303,66 @@ def warmstart_leg(a, ws, rank):
             "median_steps_ramp": float(np.median(st_ramp)), "median_steps_warm": float(np.median(st_warm))}
 
 
+class _DeviceArray:
+    """A raw device buffer seen by torch (__cuda_array_interface__), for measurements only."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
+def _max_abs_diff(f32_state, f64_state, nq):
+    import torch
+    p32, _ = f32_state.device_pointer()
+    p64, _ = f64_state.device_pointer()
+    f32_state.synchronize()
+    f64_state.synchronize()
+    a = torch.as_tensor(_DeviceArray(p32, 2 << nq, "<f4"), device="cuda")
+    b = torch.as_tensor(_DeviceArray(p64, 2 << nq, "<f8"), device="cuda")
+    worst = 0.0
+    chunk = 1 << 26
+    for k in range(0, 2 << nq, chunk):
+        worst = max(worst, float((a[k:k + chunk].double() - b[k:k + chunk]).abs().max()))
+    return worst
+
+
+def variants_leg(a, garr):
+    """One timed run (after one warm-up run) of every execution mode on the benchmark circuit,
+    and each f32 run's max-abs amplitude error against the complex f64 CUDA-core sweep."""
+    import torch
+
+    import ruqu_b200 as rq
+    S = (1 << a.qubits) * 8
+    layer_bytes = S + 2 * S * a.layers
+    ref = rq.QuantumState(a.qubits, 0, "f64")
+    ref.apply_gates(garr, rq.RQ_EXEC_SWEEP)
+    ref.synchronize()
+    out = {"value_bytes_per_run": layer_bytes, "reference": "complex f64 CUDA-core sweep of the same circuit"}
+    for name, mode in (("unfused_per_gate", rq.RQ_EXEC_PER_GATE), ("sweep_cuda_cores", rq.RQ_EXEC_SWEEP),
+                       ("tensor_core_3xtf32", rq.RQ_EXEC_SWEEP_TC), ("tensor_core_tf32", rq.RQ_EXEC_SWEEP_TC_FAST)):
+        st = rq.QuantumState(a.qubits, 0, "f32")
+        plan = rq.Plan(st, garr, mode)
+        _, sptr = st.device_pointer()
+        stream = torch.cuda.ExternalStream(sptr)
+        st.reset()
+        plan.execute(st)
+        st.reset()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.execute(st)
+        e1.record(stream)
+        st.synchronize()
+        ms = e0.elapsed_time(e1)
+        stats = plan.stats()
+        out[name] = {"ms_per_circuit": ms, "gbs_per_layer": layer_bytes / (ms / 1e3) / 1e9,
+                     "launches": stats["launches"], "sweeps": stats["sweeps"], "dense_ops": stats["dense_ops"],
+                     "max_abs_vs_f64": _max_abs_diff(st, ref, a.qubits)}
+        del plan
+        del st
+    del ref
+    return out
+
+
 def run_reference(a):
     ws, rank, _ = _dist()
     if rank != 0:
@@ -399,7 +465,8 @@ def run_ours(a):
     init_ms = sum(e[0].elapsed_time(e[1]) for e in ev)
     if dist:
         total_ms = rqdist.max_over_ranks(total_ms)
-    value = ws * step_bytes * a.steps / (total_ms / 1e3) / 1e9
+    layer_bytes = S + 2 * S * a.layers          # |0> write + one read and write of the state per layer
+    value = ws * layer_bytes * a.steps / (total_ms / 1e3) / 1e9
     peak, peak_kind = _peak()
     sweeps = max(1, stats["sweeps"] or stats["launches"])
     avg_launch_ms = plan_ms / (a.steps * sweeps)
@@ -420,10 +487,14 @@ def run_ours(a):
             state.apply_gates(garr, mode)
             state.expectation_values(zs)
         dt = (time.perf_counter() - t0) / ksteps
-        e2e = {"value": ws * step_bytes / dt / 1e9, "unit": UNIT,
+        e2e = {"value": ws * layer_bytes / dt / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": len(gates) * C.sizeof(rq._capi.RqGate),
                "d2h_bytes_per_step": 8 * a.qubits, "ms_per_step": dt * 1e3,
                "path": "QuantumState.reset + apply_gates(host list) + expectation_values(<Z_i>) -> host"}
+
+    variants = None
+    if not a.no_variants and rank == 0:
+        variants = variants_leg(a, garr)
 
     qaoa = None
     if not a.no_qaoa:
@@ -458,16 +529,21 @@ def run_ours(a):
                        "l2": "state (%.1f GiB) larger than L2, no flush needed" % (S / 2**30),
                        "sweeps_per_step": stats["sweeps"], "launches_per_step": 1 + stats["launches"],
                        "phases_per_step": stats["phases"], "device_ops_per_step": stats["ops"],
-                       "bytes_per_step": step_bytes, "layers_per_s": ws * a.layers * a.steps / (total_ms / 1e3),
+                       "dense_tensor_core_ops_per_step": stats["dense_ops"],
+                       "executed_as": "tensor-core sweeps (3xTF32)" if stats["dense_ops"] else "CUDA-core sweeps",
+                       "value_bytes_per_step": layer_bytes, "plan_hbm_bytes_per_step": step_bytes,
+                       "layers_per_s": ws * a.layers * a.steps / (total_ms / 1e3),
                        "ms_init": init_ms / a.steps, "ms_gates": plan_ms / a.steps,
                        "unfused_reference_bytes_per_step": ref_layer_bytes},
-            "roofline": {"bound": "hbm", "kernel": "k_sweep (multi-gate sweep)", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": "k_sweep_tc (tensor-core sweep)" if stats["dense_ops"]
+                         else "k_sweep (multi-gate sweep)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg_launch_ms,
                          "traffic": None},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": a.steps * (1 + stats["launches"]),
+            "variants": variants,
             "qaoa_batch": qaoa,
             "vqe_batch": vqe,
             "warm_start": warm,

@@ -105,6 +105,9 @@ int sample(rq_state* s, const uint32_t* qubits, uint32_t nq, uint64_t base_seed,
 int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n, int tc_passes = 0);
 int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out, int tc_passes = 0,
                uint32_t tc_min_ops = 2);
+// RQ_EXEC_AUTO's measured choice between the CUDA-core and the 3xTF32 tensor-core sweep
+// (0 or 3 passes), cached per (device, qubits, gate structure)
+int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes);
 // the tensor-core passes a mode asks for (0: none)
 inline int tc_passes_of(int32_t mode) { return mode == RQ_EXEC_SWEEP_TC ? 3 : mode == RQ_EXEC_SWEEP_TC_FAST ? 1 : 0; }
 int plan_launch(rq_state* s, const rq_plan* p);

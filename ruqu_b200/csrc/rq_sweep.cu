@@ -27,6 +27,9 @@
 #include <type_traits>
 #include <vector>
 #include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 namespace {
 
@@ -775,19 +778,10 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc(float2* __restrict__ amps, 
         uint64_t base = 0;
         for (uint32_t b = 0; b < d.nonlocal_count; ++b)
             if ((tile >> b) & 1ull) base |= 1ull << d.nonlocal[b];
-#pragma unroll 1
-        for (int j0 = 0; j0 < VPT; j0 += 4) {
-            VV v[4];
-#pragma unroll
-            for (int jj = 0; jj < 4; ++jj)
-                v[jj] = __ldcs(reinterpret_cast<const VV*>(amps + (base | dep_tid | d.gj[j0 + jj])));
-#pragma unroll
-            for (int jj = 0; jj < 4; ++jj) {
-                const uint32_t se = stid ^ d.sgj[j0 + jj];
-                sm[se] = make_float2(v[jj].x, v[jj].y);
-                sm[se ^ 1u] = make_float2(v[jj].z, v[jj].w);
-            }
-        }
+        // all of the tile's copies in flight at once (cp.async, element-granular for the swizzle)
+        issue_tile<float>(sm, amps, d, base, dep_tid, stid);
+        cp_async_commit();
+        cp_async_wait0();
         __syncthreads();
         run_phases_tc(sm, d, lph, lop, images, tid, T_, c);
         if (c.failed) break;
@@ -1001,6 +995,96 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
 }
 
 int apply_one_gate(rq_state* s, const rq_gate& g);   // rq_capi.cu
+
+// ---- autotuner ---------------------------------------------------------------
+// For complex f32 states the CUDA-core sweep and the 3xTF32 tensor-core sweep
+// agree to FP32 accuracy, and which is faster depends on the circuit (how many
+// gates each phase's dense op absorbs) and the state size.  RQ_EXEC_AUTO times
+// both plans on a scratch state of the same shape the first time a gate
+// structure (kinds and qubits, not angles) is seen on a device and keeps the
+// faster; the choice is cached per (device, qubits, structure).
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, uint32_t, uint64_t>, int> g_tune;
+
+uint64_t structure_hash(const rq_gate* g, uint64_t n) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint64_t v) {
+        h ^= v;
+        h *= 1099511628211ull;
+    };
+    for (uint64_t k = 0; k < n; ++k) {
+        mix((uint64_t)g[k].kind);
+        mix((uint64_t)g[k].q0);
+        mix((uint64_t)g[k].q1);
+    }
+    mix(n);
+    return h;
+}
+
+// device time of one execution of P on a scratch state shaped like t (after one warm-up run)
+int time_plan(const rq_state& t, const rq_plan* P, float* ms) {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    RQ_CUDA(cudaEventCreate(&e0));
+    RQ_CUDA(cudaEventCreate(&e1));
+    rq_state u = t;
+    int rc = plan_launch(&u, P);
+    if (rc == RQ_OK) {
+        cudaEventRecord(e0, t.stream);
+        rc = plan_launch(&u, P);
+        cudaEventRecord(e1, t.stream);
+    }
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (rc == RQ_OK && e != cudaSuccess) rc = cuda_fail(e, "autotune timing");
+    if (rc == RQ_OK) cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+}  // namespace
+
+int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes) {
+    *passes = 0;
+    const uint32_t m = sweep_local_qubits(s->nq, s->prec);
+    if (s->prec != RQ_F32 || (m != 12 && m != 13) || n == 0) return RQ_OK;
+    if (const char* e = std::getenv("RUQU_AUTOTUNE"))
+        if (e[0] == '0') return RQ_OK;
+    const auto key = std::make_tuple(s->device, s->nq, structure_hash(gates, n));
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            *passes = it->second;
+            return RQ_OK;
+        }
+    }
+    rq_plan *A = nullptr, *B = nullptr;
+    RQ_TRY(plan_build(s, gates, n, RQ_EXEC_SWEEP, &A, 0));
+    int rc = plan_build(s, gates, n, RQ_EXEC_SWEEP, &B, 3);
+    int choice = 0;
+    if (rc == RQ_OK && B->stats.dense_ops > 0) {
+        void* scratch = nullptr;
+        if (cudaMalloc(&scratch, s->bytes()) == cudaSuccess) {
+            rq_state t = *s;
+            t.amps = scratch;
+            cudaMemsetAsync(scratch, 0, s->bytes(), s->stream);
+            float ta = 0.f, tb = 0.f;
+            rc = time_plan(t, A, &ta);
+            if (rc == RQ_OK) rc = time_plan(t, B, &tb);
+            if (rc == RQ_OK && tb < ta) choice = 3;
+            cudaFree(scratch);
+        } else {
+            cudaGetLastError();   // no room for a scratch state: keep the CUDA-core sweep
+        }
+    }
+    plan_free(A);
+    if (B) plan_free(B);
+    RQ_TRY(rc);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = choice;
+    *passes = choice;
+    return RQ_OK;
+}
 
 int plan_launch(rq_state* s, const rq_plan* P) {
     if (P->mode == RQ_EXEC_PER_GATE) {
