@@ -132,7 +132,9 @@ class WarmStart:
         nval = max(1, int(len(graphs) * val_fraction))
         ntr = len(graphs) - nval
         self.mu = y[:ntr].mean(axis=0)
-        self.sd = np.maximum(y[:ntr].std(axis=0), 1e-6)
+        # angles that hardly vary (a family with few distinct graphs) are not blown up to
+        # unit variance: their spread below 1e-3 rad carries no information for the optimizer
+        self.sd = np.maximum(y[:ntr].std(axis=0), 1e-3)
         z = (y - self.mu) / self.sd
         x = features(graphs[:ntr], copies, seed=seed)
         t = np.repeat(z[:ntr], copies, axis=0).astype(np.float32)
@@ -143,6 +145,8 @@ class WarmStart:
             self.net.train(x, t, batch=batch, steps=chunk_steps, lr=lr if c < (2 * chunks) // 3 else lr / 3)
             vl = float(np.mean((self.net.forward(xv) - tv) ** 2))
             hist.append(vl)
+            if not np.isfinite(vl):     # diverged: keep the best parameters seen so far
+                break
             if vl < best:
                 best, best_p = vl, self.net.get_params()
         if best_p is None:     # never better than the mean: predict the mean

@@ -103,7 +103,7 @@ def test_warm_start_gains_over_linear_ramp():
     g, b, _, _ = qb.optimize(np.tile(g0, (len(train), 1)), np.tile(b0, (len(train), 1)), steps, lr)
     warm = WarmStart(p)
     hist = warm.fit(train, g, b, chunks=4, chunk_steps=300)
-    assert len(hist) == 4 and all(np.isfinite(hist))
+    assert len(hist) == 4 and all(np.isfinite(hist)), hist
     hb = QaoaBatch(held, p, "f32")
     G0, B0 = np.tile(g0, (len(held), 1)), np.tile(b0, (len(held), 1))
     _, _, target, _ = hb.optimize(G0, B0, steps, lr)
