@@ -489,7 +489,7 @@ namespace tc {
 
 constexpr uint32_t B_SBO = 2048;   // bytes between 8-row groups of an image (16 core matrices along K)
 constexpr uint32_t B_LBO = 128;    // bytes between core matrices along K
-constexpr uint32_t COL_D = 0, COL_A = 128, NCOLS = 256;
+constexpr uint32_t COL_D = 0;   // accumulator columns [0, 64 * halves); A follows at col_a = 64 * halves
 
 __device__ int g_tc_timeout = 0;
 
@@ -559,6 +559,7 @@ struct TcCtx {
     uint64_t* bar;       // MMA completion
     uint64_t* ibar;      // image copy completion
     uint32_t tmem;
+    uint32_t col_a;      // first column of A (64 per 128-row half after the accumulator)
     uint32_t parity, iparity;
     int passes;
     bool failed;
@@ -601,7 +602,7 @@ __device__ __forceinline__ void issue(TcCtx& c, uint32_t bsmem, uint32_t halves,
                 "{\n\t.reg .pred p;\n\t"
                 "setp.ne.b32 p, %4, 0;\n\t"
                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
-                ::"r"(c.tmem + COL_D + h * 64), "r"(c.tmem + COL_A + h * 64 + ks * 8), "l"(bd), "r"(IDESC),
+                ::"r"(c.tmem + COL_D + h * 64), "r"(c.tmem + c.col_a + h * 64 + ks * 8), "l"(bd), "r"(IDESC),
                 "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
                 : "memory");
         }
@@ -630,7 +631,7 @@ __device__ __forceinline__ void dense_op(TcCtx& c, float2* reg, uint32_t tid, ui
     const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
     const uint32_t half_col = (warp >> 2) * 64u;
     const uint32_t halves = nthreads / 128;
-    store_a(c, reg, c.tmem + lane_base + COL_A + half_col, false);
+    store_a(c, reg, c.tmem + lane_base + c.col_a + half_col, false);
     // the image copy started at the phase start
     const bool late = !mbar_wait(c.ibar, c.iparity);
     c.iparity ^= 1u;
@@ -647,7 +648,7 @@ __device__ __forceinline__ void dense_op(TcCtx& c, float2* reg, uint32_t tid, ui
     }
     if (!commit_wait(c, tid)) return;
     if (c.passes > 1) {
-        store_a(c, reg, c.tmem + lane_base + COL_A + half_col, true);
+        store_a(c, reg, c.tmem + lane_base + c.col_a + half_col, true);
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (tid == 0) issue(c, bhi, halves, false);
@@ -746,9 +747,12 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc(float2* __restrict__ amps, 
     c.iparity = 0;
     c.passes = passes;
     c.failed = false;
+    // tensor memory: accumulator and A, 64 columns each per 128-row half
+    const uint32_t ncols = 128u * (T_ / 128u);
+    c.col_a = 64u * (T_ / 128u);
     if (tid < 32) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(&tmem_base)),
-                     "r"(tc::NCOLS)
+                     "r"(ncols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -803,7 +807,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc(float2* __restrict__ amps, 
     __syncthreads();
     if (tid < 32) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(c.tmem), "r"(tc::NCOLS) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(c.tmem), "r"(ncols) : "memory");
     }
 }
 
@@ -1098,7 +1102,20 @@ int plan_launch(rq_state* s, const rq_plan* P) {
         const float* img = reinterpret_cast<const float*>(P->dev + P->off_img);
         const size_t img_bytes = (P->tc_passes > 1 ? DENSE_IMAGE_FLOATS : DENSE_FLOATS) * sizeof(float);
         const unsigned threads = 1u << (P->descs.front().m - 5);
-        const unsigned grid = (unsigned)std::min<uint64_t>(P->ntiles, 2ull * (uint64_t)rq::num_sms(s->device));
+        // resident CTAs per SM: by registers and shared memory, and by tensor memory (512 columns per SM)
+        size_t smem_max = 0;
+        for (const auto& d : P->descs) {
+            const size_t nph = d.phase_end - d.phase_begin;
+            const size_t nops = P->host_phases[d.phase_end - 1].op_end - P->host_phases[d.phase_begin].op_begin;
+            smem_max = std::max(smem_max, P->smem + img_bytes + nph * sizeof(PhaseDesc) + nops * sizeof(SwOp));
+        }
+        // 128 registers per thread (launch bounds), 228 KB of shared memory per SM (1 KB reserved per CTA)
+        const int by_regs = 65536 / (128 * (int)threads);
+        const int by_smem = (int)((228u * 1024u) / (smem_max + 1024u + 64u));
+        const int by_tmem = (int)(512u / (128u * (threads / 128u)));
+        int per_sm = std::min(by_regs, std::min(by_smem, by_tmem));
+        if (per_sm < 1) return fail(RQ_ERR_CUDA, "tensor-core sweep kernel does not fit on an SM");
+        const unsigned grid = (unsigned)std::min<uint64_t>(P->ntiles, (uint64_t)per_sm * rq::num_sms(s->device));
         const PhaseDesc* hph = P->host_phases.data();
         for (const auto& d : P->descs) {
             const size_t nph = d.phase_end - d.phase_begin;
