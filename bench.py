@@ -303,6 +303,20 @@ def warmstart_leg(a, ws, rank):
             "median_steps_ramp": float(np.median(st_ramp)), "median_steps_warm": float(np.median(st_warm))}
 
 
+# DRAM bytes (read + write) of one sweep launch measured by ncu on the 26-qubit
+# case of this circuit, per tile; a launch moves every tile once, so the figure
+# scales with the tile count (x16 from 26 to 30 qubits).
+_NCU_BYTES_PER_TILE = {"k_sweep_tc": (537.133824e6 + 487.704576e6) / 2 ** 13,
+                       "k_sweep": (537.2e6 + 485.1e6) / 2 ** 13}
+
+
+def _traffic_per_launch(a, stats):
+    if a.precision != "f32":
+        return None
+    kern = "k_sweep_tc" if stats["dense_ops"] else "k_sweep"
+    return _NCU_BYTES_PER_TILE[kern] * 2 ** (a.qubits - 13)
+
+
 class _DeviceArray:
     """A raw device buffer seen by torch (__cuda_array_interface__), for measurements only."""
 
@@ -539,7 +553,7 @@ def run_ours(a):
                          else "k_sweep (multi-gate sweep)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg_launch_ms,
-                         "traffic": None},
+                         "traffic": _traffic_per_launch(a, stats)},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": a.steps * (1 + stats["launches"]),
