@@ -63,6 +63,7 @@ def _args():
     ap.add_argument("--vqe-sets", type=int, default=512)
     ap.add_argument("--no-warm", action="store_true", help="skip the warm-start leg")
     ap.add_argument("--no-variants", action="store_true", help="skip the per-mode runs and the f64 comparison")
+    ap.add_argument("--no-sampling", action="store_true", help="skip the <Z_i> + shots leg on the final state")
     ap.add_argument("--warm-train", type=int, default=2048, help="training graphs for the warm start")
     ap.add_argument("--warm-eval", type=int, default=256, help="held-out graphs for the warm start")
     return ap.parse_args()
@@ -317,6 +318,34 @@ def _traffic_per_launch(a, stats):
     return _NCU_BYTES_PER_TILE[kern] * 2 ** (a.qubits - 13)
 
 
+def readout_leg(a, state, stream):
+    """Read-out of the final state (the calls the reference's drivers make after a run):
+    <Z_i> for every qubit (one FP64 reduction pass, state.rs:362-408) and 4096 shots
+    (FP64 prefix tree + per-shot walks, the run_shots semantics of simulator.rs:107-147).
+    Device time of each on the state's stream, and its HBM bytes: S for the <Z_i> pass;
+    S read + 2^n x 8 B written for the tree's leaf level, then the fold levels."""
+    import torch
+    n = a.qubits
+    S = (1 << n) * (8 if a.precision == "f32" else 16)
+    zs = [[(q, 3)] for q in range(n)]
+    state.expectation_values(zs)
+    state.sample(16, 1)
+    out = {}
+    for name, fn in (("z_expectations", lambda: state.expectation_values(zs)),
+                     ("shots_4096", lambda: state.sample(4096, 7))):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        state.synchronize()
+        out[name] = {"ms": e0.elapsed_time(e1)}
+    out["z_expectations"]["gbs"] = S / (out["z_expectations"]["ms"] / 1e3) / 1e9
+    tree = (1 << n) * 8
+    out["shots_4096"]["tree_bytes"] = S + 2 * tree
+    out["shots_4096"]["gbs"] = (S + 2 * tree) / (out["shots_4096"]["ms"] / 1e3) / 1e9
+    return out
+
+
 class _DeviceArray:
     """A raw device buffer seen by torch (__cuda_array_interface__), for measurements only."""
 
@@ -506,6 +535,10 @@ def run_ours(a):
                "d2h_bytes_per_step": 8 * a.qubits, "ms_per_step": dt * 1e3,
                "path": "QuantumState.reset + apply_gates(host list) + expectation_values(<Z_i>) -> host"}
 
+    readout = None
+    if not a.no_sampling:
+        readout = readout_leg(a, state, stream)
+
     variants = None
     if not a.no_variants and rank == 0:
         variants = variants_leg(a, garr)
@@ -557,6 +590,7 @@ def run_ours(a):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": a.steps * (1 + stats["launches"]),
+            "readout": readout,
             "variants": variants,
             "qaoa_batch": qaoa,
             "vqe_batch": vqe,
