@@ -109,6 +109,64 @@ __global__ void k_pauli(const typename C2<T>::t* __restrict__ a, uint64_t count,
     }
 }
 
+// Single-qubit Z strings (and the identity) in one pass: <Z_q> = sum_x p(x)(1 - 2 bit_q(x)).
+// Each thread owns chunks of 32 consecutive amplitudes: per chunk it forms the total
+// probability and the five sums over the amplitudes whose low index bit b is set;
+// a string on a low qubit (q < 5) adds total - 2 s_q, one on a high qubit adds
+// +-total by bit q of the chunk's index, the identity adds total.  Up to ZMAX
+// strings per pass; FP64 accumulation, fixed-order block and grid reductions.
+constexpr int ZMAX = 32;
+struct ZChunk {
+    uint8_t q[ZMAX];   // qubit of the string, 64 = identity
+    int k;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256, 2) k_zsingle(const typename C2<T>::t* __restrict__ a, uint64_t nchunks, ZChunk zc,
+                          double* __restrict__ partials, uint32_t slot0, uint32_t stride) {
+    using V = typename C2<T>::t;
+    __shared__ double sh[32];
+    double acc[ZMAX];
+#pragma unroll
+    for (int k = 0; k < ZMAX; ++k) acc[k] = 0.0;
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nchunks;
+         c += (uint64_t)gridDim.x * blockDim.x) {
+        const V* ch = a + c * 32;
+        double tot = 0.0, sb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+            const double pj = norm2(__ldg(ch + j));
+            tot += pj;
+#pragma unroll
+            for (int b = 0; b < 5; ++b)
+                if ((j >> b) & 1) sb[b] += pj;
+        }
+#pragma unroll
+        for (int k = 0; k < ZMAX; ++k) {
+            if (k < zc.k) {
+                const uint32_t q = zc.q[k];
+                double v;
+                if (q >= 64) {
+                    v = tot;
+                } else if (q < 5) {
+                    const double sq = q == 0 ? sb[0] : q == 1 ? sb[1] : q == 2 ? sb[2] : q == 3 ? sb[3] : sb[4];
+                    v = tot - 2.0 * sq;
+                } else {
+                    v = ((c >> (q - 5)) & 1ull) ? -tot : tot;
+                }
+                acc[k] += v;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < ZMAX; ++k) {
+        if (k < zc.k) {
+            double r = block_sum(acc[k], sh);
+            if (threadIdx.x == 0) partials[(size_t)(slot0 + k) * stride + blockIdx.x] = r;
+        }
+    }
+}
+
 // <a|b> = sum conj(a_i) b_i
 template <typename TA, typename TB>
 __global__ void k_inner(const typename C2<TA>::t* __restrict__ a, const typename C2<TB>::t* __restrict__ b,
@@ -196,11 +254,41 @@ int pauli_expect(rq_state* s, const PauliMask* terms, uint32_t nterms, double* o
     if (nterms == 0) return RQ_OK;
     unsigned G = reduction_grid(s);
     RQ_TRY(ensure_partials(s, (size_t)nterms * G + nterms + 8));
-    // group by xmask (stable), chunks of KMAX
-    std::map<uint64_t, std::vector<uint32_t>> groups;
-    for (uint32_t k = 0; k < nterms; ++k) groups[terms[k].xmask].push_back(k);
     std::vector<uint32_t> slot_of(nterms);
     uint32_t slot = 0;
+    // single-qubit Z strings and identities: one pass for up to ZMAX of them
+    std::vector<uint32_t> zs;
+    if (s->nq >= 5)
+        for (uint32_t k = 0; k < nterms; ++k)
+            if (terms[k].xmask == 0 && __builtin_popcountll(terms[k].pmask) <= 1) zs.push_back(k);
+    for (size_t c0 = 0; c0 < zs.size(); c0 += ZMAX) {
+        ZChunk zc{};
+        zc.k = (int)std::min<size_t>(ZMAX, zs.size() - c0);
+        for (int k = 0; k < zc.k; ++k) {
+            const uint64_t pm = terms[zs[c0 + k]].pmask;
+            zc.q[k] = (uint8_t)(pm ? __builtin_ctzll(pm) : 64);
+            slot_of[zs[c0 + k]] = slot + k;
+        }
+        const uint64_t nchunks = s->n >> 5;
+        const unsigned Gz = std::min<unsigned>(G, grid_for(nchunks, TPB, num_sms(s->device), 4));
+        if (s->prec == RQ_F32)
+            k_zsingle<float><<<Gz, TPB, 0, s->stream>>>((const float2*)s->amps, nchunks, zc, s->partials, slot, G);
+        else
+            k_zsingle<double><<<Gz, TPB, 0, s->stream>>>((const double2*)s->amps, nchunks, zc, s->partials, slot, G);
+        RQ_CUDA(cudaGetLastError());
+        // blocks past Gz contribute nothing to these rows
+        if (Gz < G)
+            for (int k = 0; k < zc.k; ++k)
+                RQ_CUDA(cudaMemsetAsync(s->partials + (size_t)(slot + k) * G + Gz, 0, (G - Gz) * sizeof(double),
+                                        s->stream));
+        slot += zc.k;
+    }
+    std::vector<char> done(nterms, 0);
+    for (uint32_t k : zs) done[k] = 1;
+    // the other strings: group by xmask (stable), chunks of KMAX
+    std::map<uint64_t, std::vector<uint32_t>> groups;
+    for (uint32_t k = 0; k < nterms; ++k)
+        if (!done[k]) groups[terms[k].xmask].push_back(k);
     for (auto& kv : groups) {
         uint64_t x = kv.first;
         uint32_t h = x ? 63 - __builtin_clzll(x) : 0;
