@@ -320,7 +320,8 @@ def _traffic_per_launch(a, stats):
 
 def readout_leg(a, state, stream):
     """Read-out of the final state (the calls the reference's drivers make after a run):
-    <Z_i> for every qubit (one FP64 reduction pass, state.rs:362-408) and 4096 shots
+    <Z_i> for every qubit (one FP64 reduction pass, state.rs:362-408), four two-qubit
+    X/Y strings sharing one X/Y pattern (one paired pass) and 4096 shots
     (FP64 prefix tree + per-shot walks, the run_shots semantics of simulator.rs:107-147).
     Device time of each on the state's stream, and its HBM bytes: S for the <Z_i> pass;
     S read + 2^n x 8 B written for the tree's leaf level, then the fold levels."""
@@ -328,10 +329,13 @@ def readout_leg(a, state, stream):
     n = a.qubits
     S = (1 << n) * (8 if a.precision == "f32" else 16)
     zs = [[(q, 3)] for q in range(n)]
+    xy = [[(0, 1), (1, 1)], [(0, 2), (1, 2)], [(0, 1), (1, 2)], [(0, 2), (1, 1)]]   # one X/Y pattern: one pass
     state.expectation_values(zs)
+    state.expectation_values(xy)
     state.sample(16, 1)
     out = {}
     for name, fn in (("z_expectations", lambda: state.expectation_values(zs)),
+                     ("xy_pair_expectations", lambda: state.expectation_values(xy)),
                      ("shots_4096", lambda: state.sample(4096, 7))):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -340,6 +344,7 @@ def readout_leg(a, state, stream):
         state.synchronize()
         out[name] = {"ms": e0.elapsed_time(e1)}
     out["z_expectations"]["gbs"] = S / (out["z_expectations"]["ms"] / 1e3) / 1e9
+    out["xy_pair_expectations"]["gbs"] = S / (out["xy_pair_expectations"]["ms"] / 1e3) / 1e9
     tree = (1 << n) * 8
     out["shots_4096"]["tree_bytes"] = S + 2 * tree
     out["shots_4096"]["gbs"] = (S + 2 * tree) / (out["shots_4096"]["ms"] / 1e3) / 1e9
