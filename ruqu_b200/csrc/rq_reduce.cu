@@ -121,26 +121,61 @@ struct ZChunk {
     int k;
 };
 
+template <typename T> struct ZVec;
+template <> struct ZVec<float> { using t = float4; static constexpr int EPV = 2; };
+template <> struct ZVec<double> { using t = double2; static constexpr int EPV = 1; };
+
+// Warp-cooperative: warp w of the grid owns segments of 1024 consecutive amplitudes;
+// in each, lane l loads the 16-byte vectors it*32 + l (coalesced), so the low index bits
+// of every element it sees are fixed by (lane, position in the vector) and the next bits
+// by the unrolled `it`: the lane keeps its total, the sum with index bit 0 set (f32) and
+// the sums by the bits of `it`; a string's value per segment follows from those
+// (bits 0..9) or from the segment index (bits >= 10).
 template <typename T>
-__global__ void __launch_bounds__(256, 2) k_zsingle(const typename C2<T>::t* __restrict__ a, uint64_t nchunks, ZChunk zc,
-                          double* __restrict__ partials, uint32_t slot0, uint32_t stride) {
-    using V = typename C2<T>::t;
+__global__ void __launch_bounds__(256, 2) k_zsingle(const typename C2<T>::t* __restrict__ a, uint64_t nseg,
+                                                    ZChunk zc, double* __restrict__ partials, uint32_t slot0,
+                                                    uint32_t stride) {
+    using VV = typename ZVec<T>::t;
+    constexpr int EPV = ZVec<T>::EPV;
+    constexpr int NIT = 1024 / (32 * EPV);    // vectors per lane per segment: 16 (f32) or 32 (f64)
+    constexpr int LB = EPV == 2 ? 1 : 0;      // element bits below the lane bits
+    constexpr int ITB = EPV == 2 ? 4 : 5;     // bits of `it`
     __shared__ double sh[32];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     double acc[ZMAX];
 #pragma unroll
     for (int k = 0; k < ZMAX; ++k) acc[k] = 0.0;
-    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < nchunks;
-         c += (uint64_t)gridDim.x * blockDim.x) {
-        const V* ch = a + c * 32;
-        double tot = 0.0, sb[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (uint64_t sg = warp; sg < nseg; sg += nwarps) {
+        const VV* src = reinterpret_cast<const VV*>(a + sg * 1024);
+        double tot = 0.0, odd = 0.0, r[ITB];
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-            const double pj = norm2(__ldg(ch + j));
-            tot += pj;
+        for (int k = 0; k < ITB; ++k) r[k] = 0.0;
 #pragma unroll
-            for (int b = 0; b < 5; ++b)
-                if ((j >> b) & 1) sb[b] += pj;
+        for (int h = 0; h < NIT; h += 8) {
+            VV v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = __ldcs(src + (h + u) * 32 + lane);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int it = h + u;
+                double pit;
+                if constexpr (EPV == 2) {
+                    const double p0 = (double)v[u].x * v[u].x + (double)v[u].y * v[u].y;
+                    const double p1 = (double)v[u].z * v[u].z + (double)v[u].w * v[u].w;
+                    odd += p1;
+                    pit = p0 + p1;
+                } else {
+                    pit = (double)v[u].x * v[u].x + (double)v[u].y * v[u].y;
+                }
+                tot += pit;
+#pragma unroll
+                for (int k = 0; k < ITB; ++k)
+                    if ((it >> k) & 1) r[k] += pit;
+            }
         }
+        // element index bits inside the segment: [0, LB) vector slot, [LB, LB + 5) lane, then `it`
 #pragma unroll
         for (int k = 0; k < ZMAX; ++k) {
             if (k < zc.k) {
@@ -148,11 +183,19 @@ __global__ void __launch_bounds__(256, 2) k_zsingle(const typename C2<T>::t* __r
                 double v;
                 if (q >= 64) {
                     v = tot;
-                } else if (q < 5) {
-                    const double sq = q == 0 ? sb[0] : q == 1 ? sb[1] : q == 2 ? sb[2] : q == 3 ? sb[3] : sb[4];
-                    v = tot - 2.0 * sq;
+                } else if (q < (uint32_t)LB) {
+                    v = tot - 2.0 * odd;
+                } else if (q < (uint32_t)LB + 5) {
+                    v = ((lane >> (q - LB)) & 1u) ? -tot : tot;
+                } else if (q < 10) {
+                    const uint32_t kb = q - LB - 5;
+                    double s = r[0];
+#pragma unroll
+                    for (int t = 1; t < ITB; ++t)
+                        if (kb == (uint32_t)t) s = r[t];
+                    v = tot - 2.0 * s;
                 } else {
-                    v = ((c >> (q - 5)) & 1ull) ? -tot : tot;
+                    v = ((sg >> (q - 10)) & 1ull) ? -tot : tot;
                 }
                 acc[k] += v;
             }
@@ -161,8 +204,8 @@ __global__ void __launch_bounds__(256, 2) k_zsingle(const typename C2<T>::t* __r
 #pragma unroll
     for (int k = 0; k < ZMAX; ++k) {
         if (k < zc.k) {
-            double r = block_sum(acc[k], sh);
-            if (threadIdx.x == 0) partials[(size_t)(slot0 + k) * stride + blockIdx.x] = r;
+            double rr = block_sum(acc[k], sh);
+            if (threadIdx.x == 0) partials[(size_t)(slot0 + k) * stride + blockIdx.x] = rr;
         }
     }
 }
@@ -258,7 +301,7 @@ int pauli_expect(rq_state* s, const PauliMask* terms, uint32_t nterms, double* o
     uint32_t slot = 0;
     // single-qubit Z strings and identities: one pass for up to ZMAX of them
     std::vector<uint32_t> zs;
-    if (s->nq >= 5)
+    if (s->nq >= 10)
         for (uint32_t k = 0; k < nterms; ++k)
             if (terms[k].xmask == 0 && __builtin_popcountll(terms[k].pmask) <= 1) zs.push_back(k);
     for (size_t c0 = 0; c0 < zs.size(); c0 += ZMAX) {
@@ -269,12 +312,12 @@ int pauli_expect(rq_state* s, const PauliMask* terms, uint32_t nterms, double* o
             zc.q[k] = (uint8_t)(pm ? __builtin_ctzll(pm) : 64);
             slot_of[zs[c0 + k]] = slot + k;
         }
-        const uint64_t nchunks = s->n >> 5;
-        const unsigned Gz = std::min<unsigned>(G, grid_for(nchunks, TPB, num_sms(s->device), 4));
+        const uint64_t nseg = s->n >> 10;     // segments of 1024 amplitudes, one warp each
+        const unsigned Gz = std::min<unsigned>(G, grid_for(nseg * 32, TPB, num_sms(s->device), 4));
         if (s->prec == RQ_F32)
-            k_zsingle<float><<<Gz, TPB, 0, s->stream>>>((const float2*)s->amps, nchunks, zc, s->partials, slot, G);
+            k_zsingle<float><<<Gz, TPB, 0, s->stream>>>((const float2*)s->amps, nseg, zc, s->partials, slot, G);
         else
-            k_zsingle<double><<<Gz, TPB, 0, s->stream>>>((const double2*)s->amps, nchunks, zc, s->partials, slot, G);
+            k_zsingle<double><<<Gz, TPB, 0, s->stream>>>((const double2*)s->amps, nseg, zc, s->partials, slot, G);
         RQ_CUDA(cudaGetLastError());
         // blocks past Gz contribute nothing to these rows
         if (Gz < G)
