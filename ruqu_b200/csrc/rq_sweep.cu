@@ -523,10 +523,11 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     return false;
 }
 
+// round to the nearest TF32 value (ties away from zero) with integer operations: add half
+// a unit of the 10-bit mantissa to the magnitude bits and clear the 13 low bits (amplitudes
+// are finite; the carry into the exponent is the correct rounding)
 __device__ __forceinline__ float to_tf32(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
 }
 
 // 16 accumulator columns of this thread's lane -> 8 complex amplitudes
