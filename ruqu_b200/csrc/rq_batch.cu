@@ -25,6 +25,7 @@
 
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -1501,11 +1502,16 @@ __global__ void k_qaoa_shift(const double* __restrict__ theta, const uint32_t* _
 
 // one Adam step (gradient ascent on the expected cut) per instance, FP64 on the device;
 // frozen once the target is met.  done[i] = 1 + the step at which the target was met.
+__global__ void k_step_inc(uint32_t* __restrict__ step) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1;
+}
+
 __global__ void k_qaoa_adam(const double* __restrict__ energy, const uint32_t* __restrict__ act, uint32_t nact,
                             uint32_t p, uint32_t nsets, double* __restrict__ theta, double* __restrict__ m,
                             double* __restrict__ v, double lr, uint32_t step, const double* __restrict__ target,
                             double rtol, uint32_t* __restrict__ done, double* __restrict__ elast, int final_eval,
-                            const double* __restrict__ grad) {
+                            const double* __restrict__ grad, const uint32_t* __restrict__ step_dev) {
+    if (step_dev) step = *step_dev;   // graph replays: the step counter lives on the device
     for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < nact; a += gridDim.x * blockDim.x) {
         const uint32_t i = act[a];
         if (done[i]) continue;
@@ -1624,9 +1630,21 @@ int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* 
             for (size_t j = 0; j < b->classes[k].insts.size(); ++j) cls_of[r++] = (uint32_t)k;
     }
     double *d_th = nullptr, *d_m = nullptr, *d_v = nullptr, *d_tg = nullptr, *d_el = nullptr;
-    uint32_t *d_done = nullptr, *d_act = nullptr;
+    uint32_t *d_done = nullptr, *d_act = nullptr, *d_step = nullptr;
+    // one optimizer step as a CUDA graph, captured per active set (after an uncaptured first
+    // step has sized every buffer) and replayed until the set changes
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    bool use_graph = std::getenv("RUQU_NO_GRAPHS") == nullptr;
+    auto drop_graph = [&]() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        gexec = nullptr;
+        graph = nullptr;
+    };
     auto cleanup = [&]() {
-        void* q[] = {d_th, d_m, d_v, d_tg, d_el, d_done, d_act};
+        drop_graph();
+        void* q[] = {d_th, d_m, d_v, d_tg, d_el, d_done, d_act, d_step};
         for (void* x : q) if (x) cudaFree(x);
     };
     int rc = RQ_OK;
@@ -1637,6 +1655,7 @@ int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* 
     if (rc == RQ_OK) rc = dalloc_b(&d_el, ninst);
     if (rc == RQ_OK) rc = dalloc_b(&d_done, ninst);
     if (rc == RQ_OK) rc = dalloc_b(&d_act, ninst);
+    if (rc == RQ_OK) rc = dalloc_b(&d_step, 1);
     if (rc != RQ_OK) { cleanup(); return rc; }
     // active set: run-order instances still optimising, their circuits' instance map, and per-class counts
     std::vector<uint32_t> act(ninst), ci;
@@ -1661,22 +1680,56 @@ int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* 
     cudaMemsetAsync(d_m, 0, th.size() * sizeof(double), b->stream);
     cudaMemsetAsync(d_v, 0, th.size() * sizeof(double), b->stream);
     cudaMemsetAsync(d_done, 0, ninst * sizeof(uint32_t), b->stream);
+    cudaMemsetAsync(d_step, 0, sizeof(uint32_t), b->stream);
     if (target) cudaMemcpyAsync(d_tg, tg.data(), ninst * sizeof(double), cudaMemcpyHostToDevice, b->stream);
     rc = upload_active();
     const int sms = rq::num_sms(b->device);
     cudaEventRecord(b->ev0, b->stream);
-    for (uint32_t step = 0; step <= steps && rc == RQ_OK; ++step) {
+    // one step: shifted angles, energies (+ gradients), Adam, step counter
+    auto enqueue_step = [&](bool final_eval) -> int {
         const uint32_t nact = (uint32_t)act.size();
         const uint64_t ncirc = (uint64_t)nact * nsets;
         k_qaoa_shift<<<rq::grid_for(ncirc * p, TPB, sms), TPB, 0, b->stream>>>(d_th, d_act, nact, p, nsets, b->d_ang);
-        rc = qaoa_launch(b, nsets, 0, 0, &per_class, adj && step < steps);
-        if (rc != RQ_OK) break;
+        RQ_TRY(qaoa_launch(b, nsets, 0, 0, &per_class, adj && !final_eval));
         k_qaoa_adam<<<rq::grid_for(nact, TPB, sms), TPB, 0, b->stream>>>(b->d_energy, d_act, nact, p, nsets, d_th, d_m,
-                                                                      d_v, lr, step, target ? d_tg : nullptr, rtol,
-                                                                      d_done, d_el, step == steps ? 1 : 0,
-                                                                      adj ? b->d_grad : nullptr);
+                                                                      d_v, lr, 0, target ? d_tg : nullptr, rtol,
+                                                                      d_done, d_el, final_eval ? 1 : 0,
+                                                                      adj ? b->d_grad : nullptr, d_step);
+        k_step_inc<<<1, 32, 0, b->stream>>>(d_step);
         cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) { rc = rq::cuda_fail(e, "optimizer kernels"); break; }
+        if (e != cudaSuccess) return rq::cuda_fail(e, "optimizer kernels");
+        return RQ_OK;
+    };
+    for (uint32_t step = 0; step <= steps && rc == RQ_OK; ++step) {
+        if (step == 0 || step == steps || !use_graph) {
+            rc = enqueue_step(step == steps);
+        } else {
+            if (!gexec) {
+                cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed);
+                int crc = e == cudaSuccess ? enqueue_step(false) : RQ_ERR_CUDA;
+                cudaGraph_t g = nullptr;
+                cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+                if (crc == RQ_OK && e2 == cudaSuccess && g &&
+                    cudaGraphInstantiate(&gexec, g, 0) == cudaSuccess) {
+                    graph = g;
+                } else {   // capture did not work here: plain launches from now on
+                    if (g) cudaGraphDestroy(g);
+                    gexec = nullptr;
+                    use_graph = false;
+                    cudaGetLastError();
+                    rc = enqueue_step(false);
+                    if (rc != RQ_OK) break;
+                    goto polled;
+                }
+            }
+            {
+                cudaError_t e = cudaGraphLaunch(gexec, b->stream);
+                if (e != cudaSuccess) { rc = rq::cuda_fail(e, "optimizer step graph"); break; }
+            }
+        }
+    polled:
+        if (rc != RQ_OK) break;
+        cudaError_t e = cudaSuccess;
         if (target && step < steps && (step % 5 == 4)) {
             // drop the instances that met their target from the next steps' launches; the
             // rest keep their slots' math (every circuit's energy is independent of the batch)
@@ -1689,6 +1742,7 @@ int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* 
             if (still.empty()) break;
             if (still.size() < act.size()) {
                 act.swap(still);
+                drop_graph();   // the next step is captured again for the smaller set
                 rc = upload_active();
             }
         }

@@ -112,3 +112,20 @@ def test_warm_start_gains_over_linear_ramp():
     _, _, e_warm, st_warm = hb.optimize(pg, pb, steps, 0.005, target=target, rtol=1e-5)
     assert np.mean(e_warm >= target * (1 - 1e-5)) >= 0.9
     assert np.median(st_warm) < np.median(st_ramp), (np.median(st_warm), np.median(st_ramp))
+
+
+def test_step_graph_replay_equals_plain_launches(monkeypatch):
+    """The optimizer replays each step as a captured CUDA graph (recaptured when finished
+    instances leave); with graphs switched off the same kernels run as plain launches:
+    the trajectories are identical."""
+    graphs = _graphs(12, [8, 10, 12, 14], 6)
+    p = 3
+    g0, b0 = linear_ramp(p)
+    G, B = np.tile(g0, (12, 1)), np.tile(b0, (12, 1))
+    qb = QaoaBatch(graphs, p, "f32")
+    _, _, e10, _ = qb.optimize(G, B, 10, 0.05)
+    tgt = np.where(np.arange(12) % 3 == 0, e10, 1e9)
+    ga, ba, ea, sa = qb.optimize(G, B, 25, 0.05, target=tgt, rtol=1e-5)
+    monkeypatch.setenv("RUQU_NO_GRAPHS", "1")
+    gb, bb, eb, sb = qb.optimize(G, B, 25, 0.05, target=tgt, rtol=1e-5)
+    assert np.array_equal(ga, gb) and np.array_equal(ba, bb) and np.array_equal(ea, eb) and np.array_equal(sa, sb)
