@@ -838,40 +838,51 @@ __device__ __forceinline__ void tile_group(const VGroup& G, const VTerm* __restr
     const uint32_t count = x == 0 ? L : L >> 1;
     const uint32_t sel = r < rp ? 0u : (1u ^ ((xl >> (M - 1)) & 1u));
     const uint32_t rbase = r << M, pbase = rp << M;
-    for (uint32_t q = threadIdx.x; q < count; q += blockDim.x) {
-        T re = 0, im = 0;
-        uint32_t i;
-        if (x == 0) {
-            i = rbase | q;
-            const V v = own[q];
-            re = v.x * v.x + v.y * v.y;
-        } else {
-            V af, as;
-            if (t == 0) {
-                const uint32_t e = (uint32_t)rqd::insert0(q, G.h);
-                i = rbase | e;
-                af = own[e];
-                as = own[e ^ xl];
-            } else {
-                const uint32_t e = (uint32_t)rqd::insert0(q, M - 1) | (sel << (M - 1));
-                const uint32_t ep = e ^ xl;
-                const uint32_t im_ = rbase | e;
-                const V ao = own[e], ap = src[ep];
-                const bool first_is_mine = !((im_ >> G.h) & 1u);
-                i = first_is_mine ? im_ : (pbase | ep);
-                af = first_is_mine ? ao : ap;
-                as = first_is_mine ? ap : ao;
-            }
-            if (need & 1) re = as.x * af.x + as.y * af.y;
-            if (need & 2) im = as.x * af.y - as.y * af.x;
-        }
-        const double dre = (need & 1) ? (double)re : 0.0;
-        const double dim = (need & 2) ? (double)im : 0.0;
+    // one warp owns the group: its lanes walk all pairs, one warp reduction per group.  The
+    // products are summed in T over 16 pairs of a lane, then added into the FP64 accumulators
+    // (16 terms in f32 keep the partial within ~1e-6 relative).
+    for (uint32_t q0 = lane; q0 < count; q0 += 32 * 16) {
+        T part[NT];
 #pragma unroll
-        for (int k = 0; k < NT; ++k) {
-            const double v = od[k] ? dim : dre;
-            acc[k] += (__popc(i & pm[k]) & 1) ? -v : v;
+        for (int k = 0; k < NT; ++k) part[k] = (T)0;
+#pragma unroll 4
+        for (uint32_t u = 0; u < 16; ++u) {
+            const uint32_t q = q0 + 32 * u;
+            if (q >= count) break;
+            T re = 0, im = 0;
+            uint32_t i;
+            if (x == 0) {
+                i = rbase | q;
+                const V v = own[q];
+                re = v.x * v.x + v.y * v.y;
+            } else {
+                V af, as;
+                if (t == 0) {
+                    const uint32_t e = (uint32_t)rqd::insert0(q, G.h);
+                    i = rbase | e;
+                    af = own[e];
+                    as = own[e ^ xl];
+                } else {
+                    const uint32_t e = (uint32_t)rqd::insert0(q, M - 1) | (sel << (M - 1));
+                    const uint32_t ep = e ^ xl;
+                    const uint32_t im_ = rbase | e;
+                    const V ao = own[e], ap = src[ep];
+                    const bool first_is_mine = !((im_ >> G.h) & 1u);
+                    i = first_is_mine ? im_ : (pbase | ep);
+                    af = first_is_mine ? ao : ap;
+                    as = first_is_mine ? ap : ao;
+                }
+                if (need & 1) re = as.x * af.x + as.y * af.y;
+                if (need & 2) im = as.x * af.y - as.y * af.x;
+            }
+#pragma unroll
+            for (int k = 0; k < NT; ++k) {
+                const T v = od[k] ? im : re;
+                part[k] += (__popc(i & pm[k]) & 1) ? -v : v;
+            }
         }
+#pragma unroll
+        for (int k = 0; k < NT; ++k) acc[k] += (double)part[k];
     }
 #pragma unroll
     for (int k = 0; k < NT; ++k) {
@@ -886,9 +897,10 @@ __device__ __forceinline__ void tile_group(const VGroup& G, const VTerm* __restr
 // pattern has top part x >> M == t from on-chip memory.  Pairs inside tile r
 // (t = 0) are all counted by that CTA; pairs between tiles lo < hi are split
 // by bit M-1 of their element in tile lo (0: CTA lo, 1: CTA hi), so each pair
-// is counted once.  Per-warp, per-string sums land in shared memory, the CTA
-// writes one partial per string, and k_vqe_finalize adds the tiles and the
-// strings in a fixed order.
+// is counted once.  Each group is walked by one warp (groups dealt round-robin
+// to the warps), whose per-string sums land in shared memory; the CTA writes one
+// partial per string, and k_vqe_finalize adds the tiles and the strings in a
+// fixed order.
 template <typename T>
 __global__ void __launch_bounds__(512, 1) k_vqe_energy_tiles(const typename C2<T>::t* __restrict__ states, uint32_t n,
                                                              uint32_t M, uint64_t ncirc,
@@ -923,7 +935,7 @@ __global__ void __launch_bounds__(512, 1) k_vqe_energy_tiles(const typename C2<T
                 src = par;
             }
             const bool r_is_lo = r < rp;
-            for (uint32_t g = gofs[t]; g < gofs[t + 1]; ++g) {
+            for (uint32_t g = gofs[t] + warp; g < gofs[t + 1]; g += nw) {
                 const VGroup G = groups[g];
                 switch (G.nt) {
                     case 1: tile_group<T, 1>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp); break;
