@@ -208,6 +208,15 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
+__device__ __forceinline__ void bcp_async8(void* smem, const void* gmem) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void bcp_async16(void* smem, const void* gmem) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+
 // Batched QAOA sweep over (circuit, tile) work items of one class.
 template <typename T, int RB>
 __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const PhaseDesc* __restrict__ phases,
@@ -252,23 +261,20 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
 
         const bool init = (d.flags & (SWEEP_INIT_UNIFORM | SWEEP_INIT_ZERO)) != 0;
         if (!init) {
-#pragma unroll 1
-            for (int j0 = 0; j0 < VPT; j0 += 8) {
-                VV v[8];
+            // all of the tile's copies in flight at once (cp.async, element-granular for the swizzle)
 #pragma unroll
-                for (int jj = 0; jj < 8; ++jj)
-                    v[jj] = __ldcs(reinterpret_cast<const VV*>(amps + (base | dep_tid | d.gj[j0 + jj])));
-#pragma unroll
-                for (int jj = 0; jj < 8; ++jj) {
-                    const uint32_t se = stid ^ d.sgj[j0 + jj];
-                    if constexpr (EPV == 2) {
-                        sm[se] = make_float2(v[jj].x, v[jj].y);
-                        sm[se ^ 1u] = make_float2(v[jj].z, v[jj].w);
-                    } else {
-                        sm[se] = *reinterpret_cast<V*>(&v[jj]);
-                    }
+            for (int j = 0; j < VPT; ++j) {
+                const V* g = amps + (base | dep_tid | d.gj[j]);
+                const uint32_t se = stid ^ d.sgj[j];
+                if constexpr (EPV == 2) {
+                    bcp_async8(sm + se, g);
+                    bcp_async8(sm + (se ^ 1u), g + 1);
+                } else {
+                    bcp_async16(sm + se, g);
                 }
             }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         }
         __syncthreads();
 
