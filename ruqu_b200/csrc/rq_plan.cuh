@@ -170,7 +170,10 @@ inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t 
                 blocked |= qm;
                 continue;
             }
-            uint64_t L2 = sw.L | needs(g, all_slots);
+            // locality as for CUDA-core sweeps also in tensor-core plans: a gate qubit that
+            // stays outside the sweep's local set is uniform over each tile (see fuse_dense)
+            (void)all_slots;
+            uint64_t L2 = sw.L | needs(g, false);
             if ((uint32_t)__builtin_popcountll(L2) > m) {
                 blocked |= qm;
                 continue;
@@ -192,6 +195,8 @@ inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t 
     return out;
 }
 
+constexpr int DENSE_MAX_VQ_PLAN = 3;   // qubits outside the tile per tensor-core phase (2^3 image variants)
+
 struct PhasePlan {
     uint64_t R;               // register qubits (global mask)
     std::vector<int> ops;     // indices into the sweep's op list
@@ -205,6 +210,7 @@ inline std::vector<PhasePlan> plan_phases(const Sweep& sw, uint32_t rb, bool all
         PhasePlan ph;
         ph.R = 0;
         uint64_t blocked = 0;
+        uint64_t outside = 0;   // tensor-core plans: gate qubits outside the tile used by the phase
         for (size_t k = first; k < sw.ops.size(); ++k) {
             if (taken[k]) continue;
             const PGate& g = sw.ops[k];
@@ -213,11 +219,15 @@ inline std::vector<PhasePlan> plan_phases(const Sweep& sw, uint32_t rb, bool all
                 blocked |= qm;
                 continue;
             }
-            uint64_t R2 = ph.R | needs(g, all_slots);
-            if ((uint32_t)__builtin_popcountll(R2) > rb) {
+            // tensor-core plans: every local qubit of the gate is a register slot, and the phase
+            // uses at most DENSE_MAX_VQ qubits outside the tile (one operand image per assignment)
+            uint64_t R2 = ph.R | needs(g, false) | (all_slots ? (qm & sw.L) : 0ull);
+            const uint64_t out2 = all_slots ? (outside | (qm & ~sw.L)) : 0ull;
+            if ((uint32_t)__builtin_popcountll(R2) > rb || __builtin_popcountll(out2) > DENSE_MAX_VQ_PLAN) {
                 blocked |= qm;
                 continue;
             }
+            outside = out2;
             ph.R = R2;
             taken[k] = 1;
             ph.ops.push_back((int)k);
@@ -397,22 +407,10 @@ inline void build_program(std::vector<Sweep>& sweeps, uint32_t nq, uint32_t m, u
 constexpr int DENSE_FLOATS = 64 * 64;          // one 64x64 operand image
 constexpr int DENSE_IMAGE_FLOATS = 2 * DENSE_FLOATS;
 
-inline bool slot_local(const SwOp& o) {
-    switch (o.type) {
-        case OP_U1: case OP_D1: return o.k0 >= 0;
-        case OP_CX: case OP_CZ: case OP_ZZ: return o.k0 >= 0 && o.k1 >= 0;
-        default: return false;
-    }
-}
-
-inline uint64_t op_qubits(const SwOp& o) {
-    uint64_t m = 1ull << o.q0;
-    if (o.type == OP_CX || o.type == OP_CZ || o.type == OP_ZZ) m |= 1ull << o.q1;
-    return m;
-}
-
-// v <- op(v) on a 32-vector of register amplitudes (the kernel's op semantics)
-inline void apply_op32(const SwOp& o, const double* mt, double* v /* 64: re, im interleaved */) {
+// v <- op(v) on a 32-vector of register amplitudes (the kernel's op semantics); u0 / u1
+// are the values of q0 / q1 when they are not register slots (uniform over a tile)
+inline void apply_op32(const SwOp& o, const double* mt, double* v /* 64: re, im interleaved */, int u0 = 0,
+                       int u1 = 0) {
     auto re = [&](int i) -> double& { return v[2 * i]; };
     auto im = [&](int i) -> double& { return v[2 * i + 1]; };
     if (o.type == OP_U1) {
@@ -428,7 +426,7 @@ inline void apply_op32(const SwOp& o, const double* mt, double* v /* 64: re, im 
         }
     } else if (o.type == OP_D1) {
         for (int i = 0; i < 32; ++i) {
-            const int bit = (i >> o.k0) & 1;
+            const int bit = o.k0 >= 0 ? (i >> o.k0) & 1 : u0;
             const double dr = bit ? mt[2] : mt[0], di = bit ? mt[3] : mt[1];
             const double xr = re(i), xi = im(i);
             re(i) = xr * dr - xi * di;
@@ -437,16 +435,19 @@ inline void apply_op32(const SwOp& o, const double* mt, double* v /* 64: re, im 
     } else if (o.type == OP_CX) {
         const int t = 1 << o.k1;
         for (int i = 0; i < 32; ++i)
-            if (!(i & t) && ((i >> o.k0) & 1)) {
+            if (!(i & t) && (o.k0 >= 0 ? (i >> o.k0) & 1 : u0)) {
                 std::swap(re(i), re(i | t));
                 std::swap(im(i), im(i | t));
             }
     } else if (o.type == OP_CZ) {
-        for (int i = 0; i < 32; ++i)
-            if (((i >> o.k0) & 1) && ((i >> o.k1) & 1)) { re(i) = -re(i); im(i) = -im(i); }
+        for (int i = 0; i < 32; ++i) {
+            const int b0 = o.k0 >= 0 ? (i >> o.k0) & 1 : u0, b1 = o.k1 >= 0 ? (i >> o.k1) & 1 : u1;
+            if (b0 && b1) { re(i) = -re(i); im(i) = -im(i); }
+        }
     } else if (o.type == OP_ZZ) {
         for (int i = 0; i < 32; ++i) {
-            const bool diff = (((i >> o.k0) ^ (i >> o.k1)) & 1) != 0;
+            const int b0 = o.k0 >= 0 ? (i >> o.k0) & 1 : u0, b1 = o.k1 >= 0 ? (i >> o.k1) & 1 : u1;
+            const bool diff = (b0 ^ b1) != 0;
             const double dr = diff ? mt[2] : mt[0], di = diff ? mt[3] : mt[1];
             const double xr = re(i), xi = im(i);
             re(i) = xr * dr - xi * di;
@@ -491,13 +492,27 @@ inline void dense_image(const std::vector<double>& U /* 32 x 32 complex, [col][i
         }
 }
 
-// Rewrites ops/phases in place; appends the operand images of the new dense ops
-// (in phase order, so a sweep's images are consecutive) and records each sweep's
-// image range; at most max_per_sweep dense ops per sweep (they stay resident in
-// shared memory during the sweep's launch).
-inline void fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& phases, std::vector<SwOp>& ops,
-                       const std::vector<double>& mats, uint32_t min_ops, uint32_t max_per_sweep,
-                       std::vector<float>& images, uint64_t* ndense) {
+// Tensor-core plans: every phase becomes one OP_DENSE.  Gate qubits that are register
+// slots index the 32-dimensional space; the other gate qubits are outside the sweep's local
+// set (the phase planner makes every local gate qubit a slot), so their values are fixed
+// for a whole tile.  For the at most DENSE_MAX_VQ such qubits of a phase one image is built
+// per value assignment (variant v: bit j of v = value of the j-th qubit); the kernel picks
+// the variant from the tile's index bits.  Returns false when a phase needs more.
+constexpr int DENSE_MAX_VQ = 5;
+
+__host__ __device__ inline int dense_nvq(const SwOp& o) { return o.k0; }
+__host__ __device__ inline uint32_t dense_vq(const SwOp& o, int j) {
+    switch (j) {
+        case 0: return o.q0;
+        case 1: return o.q1;
+        case 2: return o.pad;
+        case 3: return o.pad2 & 0xFFu;
+        default: return (o.pad2 >> 8) & 0xFFu;
+    }
+}
+
+inline bool fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& phases, std::vector<SwOp>& ops,
+                       const std::vector<double>& mats, std::vector<float>& images, uint64_t* ndense) {
     std::vector<SwOp> out;
     std::vector<uint32_t> sweep_of(phases.size(), 0);
     for (size_t d = 0; d < descs.size(); ++d) {
@@ -508,45 +523,64 @@ inline void fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& ph
     for (size_t pi = 0; pi < phases.size(); ++pi) {
         auto& ph = phases[pi];
         SweepDesc& sd = descs[sweep_of[pi]];
-        std::vector<SwOp> dense, deferred;
-        uint64_t held = 0;
+        // the phase's tile-uniform qubits, in first-use order
+        std::vector<uint32_t> vq;
+        auto note = [&](int k, uint32_t q) {
+            if (k < 0 && std::find(vq.begin(), vq.end(), q) == vq.end()) vq.push_back(q);
+        };
         for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
             const SwOp& op = ops[o];
-            if (slot_local(op) && !(op_qubits(op) & held)) {
-                dense.push_back(op);
-            } else {
-                deferred.push_back(op);
-                held |= op_qubits(op);
+            switch (op.type) {
+                case OP_U1: if (op.k0 < 0) return false; break;
+                case OP_D1: note(op.k0, op.q0); break;
+                case OP_CX: if (op.k1 < 0) return false; note(op.k0, op.q0); break;
+                case OP_CZ: case OP_ZZ: note(op.k0, op.q0); note(op.k1, op.q1); break;
+                default: return false;
             }
         }
-        const uint32_t begin = (uint32_t)out.size();
-        if (dense.size() >= min_ops && min_ops > 0 && sd.img_count < max_per_sweep) {
+        if (vq.size() > (size_t)DENSE_MAX_VQ) return false;
+        const size_t first = images.size() / DENSE_IMAGE_FLOATS;
+        const uint32_t nvar = 1u << vq.size();
+        for (uint32_t var = 0; var < nvar; ++var) {
+            auto val = [&](uint32_t q) {
+                for (size_t j = 0; j < vq.size(); ++j)
+                    if (vq[j] == q) return (int)((var >> j) & 1u);
+                return 0;
+            };
             std::vector<double> U(32 * 64, 0.0);
             for (int col = 0; col < 32; ++col) {
                 double* v = &U[(size_t)col * 64];
                 v[2 * col] = 1.0;
-                for (const auto& op : dense) apply_op32(op, mats.data() + 2 * (size_t)op.mat, v);
+                for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
+                    const SwOp& op = ops[o];
+                    apply_op32(op, mats.data() + 2 * (size_t)op.mat, v, val(op.q0), val(op.q1));
+                }
             }
-            const size_t idx = images.size() / DENSE_IMAGE_FLOATS;
-            if (sd.img_count == 0) sd.img_begin = (uint32_t)idx;
-            ++sd.img_count;
             images.resize(images.size() + DENSE_IMAGE_FLOATS);
-            dense_image(U, images.data() + idx * DENSE_IMAGE_FLOATS);
-            SwOp d{};
-            d.type = OP_DENSE;
-            d.k0 = d.k1 = -1;
-            d.mat = (uint32_t)idx;
-            out.push_back(d);
-            for (const auto& op : deferred) out.push_back(op);
-            ++*ndense;
-        } else {
-            for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) out.push_back(ops[o]);
+            dense_image(U, images.data() + (images.size() - DENSE_IMAGE_FLOATS));
         }
+        if (sd.img_count == 0) sd.img_begin = (uint32_t)first;
+        sd.img_count += nvar;
+        SwOp d{};
+        d.type = OP_DENSE;
+        d.k0 = (int8_t)vq.size();
+        d.k1 = -1;
+        uint8_t b[5] = {0, 0, 0, 0, 0};
+        for (size_t j = 0; j < vq.size(); ++j) b[j] = (uint8_t)vq[j];
+        d.q0 = b[0];
+        d.q1 = b[1];
+        d.pad = b[2];
+        d.pad2 = (uint32_t)b[3] | ((uint32_t)b[4] << 8);
+        d.mat = (uint32_t)first;
+        const uint32_t begin = (uint32_t)out.size();
+        out.push_back(d);
         ph.op_begin = begin;
         ph.op_end = (uint32_t)out.size();
+        ++*ndense;
     }
     if (out.empty()) out.push_back(SwOp{});
     ops.swap(out);
+    return true;
 }
 
 }  // namespace rqp

@@ -670,13 +670,19 @@ __device__ __forceinline__ void dense_op(TcCtx& c, float2* reg, uint32_t tid, ui
 // qubit planned onto a register slot, each phase of such a plan is exactly
 // one OP_DENSE (the planner checks this).
 __device__ __forceinline__ void run_phases_tc(float2* sm, const SweepDesc& d, const PhaseDesc* phases,
-                                              const SwOp* ops, const float* __restrict__ images, uint32_t tid,
-                                              uint32_t nthreads, tc::TcCtx& c) {
+                                              const SwOp* ops, const float* __restrict__ images, uint64_t base,
+                                              uint32_t tid, uint32_t nthreads, tc::TcCtx& c) {
     using V = float2;
     constexpr int NR = 32;
     for (uint32_t p = d.phase_begin; p < d.phase_end; ++p) {
         const PhaseDesc& ph = phases[p];
-        if (tid == 0) tc::start_image(c, images + (size_t)ops[ph.op_begin].mat * DENSE_IMAGE_FLOATS);
+        if (tid == 0) {
+            // the image variant for this tile's values of the phase's qubits outside the tile
+            const SwOp& op = ops[ph.op_begin];
+            uint32_t var = 0;
+            for (int j = 0; j < dense_nvq(op); ++j) var |= (uint32_t)((base >> dense_vq(op, j)) & 1ull) << j;
+            tc::start_image(c, images + (size_t)(op.mat + var) * DENSE_IMAGE_FLOATS);
+        }
         uint32_t ebase = 0;
         for (uint32_t b = 0; b < ph.nt; ++b)
             if ((tid >> b) & 1u) ebase |= 1u << ph.tbit_local[b];
@@ -788,7 +794,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc(float2* __restrict__ amps, 
         cp_async_commit();
         cp_async_wait0();
         __syncthreads();
-        run_phases_tc(sm, d, lph, lop, images, tid, T_, c);
+        run_phases_tc(sm, d, lph, lop, images, base, tid, T_, c);
         if (c.failed) break;
 #pragma unroll
         for (int j = 0; j < VPT; ++j) {
@@ -900,8 +906,8 @@ static uint32_t sweep_local_qubits(uint32_t nq, int32_t prec) {
     return std::min(nq, m);
 }
 
-// tc_passes > 0 fuses each phase's slot-local ops (at least tc_min_ops of them) into one
-// dense 32x32 op applied on the tensor cores (complex f32 states, m in {12, 13} only).
+// tc_passes > 0 turns every phase into one dense 32x32 op applied on the tensor cores
+// (complex f32 states, m in {12, 13} only); tc_min_ops is kept for the ABI of this helper.
 int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out, int tc_passes,
                uint32_t tc_min_ops) {
     rq_plan* P = new rq_plan();
@@ -951,7 +957,10 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
     uint64_t ndense = 0;
     if (tcp) {
         // images resident in shared memory next to one tile
-        fuse_dense(P->descs, phases, ops, mats, 1, UINT32_MAX, images, &ndense);
+        if (!fuse_dense(P->descs, phases, ops, mats, images, &ndense)) {
+            delete P;
+            return fail(RQ_ERR_CIRCUIT, "tensor-core plan: a phase touches more than 5 qubits outside the tile");
+        }
         for (const auto& ph : phases)
             if (ph.op_end != ph.op_begin + 1 || ops[ph.op_begin].type != OP_DENSE) {
                 delete P;
@@ -1065,9 +1074,11 @@ int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes
     }
     rq_plan *A = nullptr, *B = nullptr;
     RQ_TRY(plan_build(s, gates, n, RQ_EXEC_SWEEP, &A, 0));
-    int rc = plan_build(s, gates, n, RQ_EXEC_SWEEP, &B, 3);
+    // a circuit the tensor-core planner cannot take keeps the CUDA-core sweep
+    if (plan_build(s, gates, n, RQ_EXEC_SWEEP, &B, 3) != RQ_OK) B = nullptr;
+    int rc = RQ_OK;
     int choice = 0;
-    if (rc == RQ_OK && B->stats.dense_ops > 0) {
+    if (B && B->stats.dense_ops > 0) {
         void* scratch = nullptr;
         if (cudaMalloc(&scratch, s->bytes()) == cudaSuccess) {
             rq_state t = *s;
