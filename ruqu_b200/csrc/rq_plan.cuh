@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -195,7 +196,7 @@ inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t 
     return out;
 }
 
-constexpr int DENSE_MAX_VQ_PLAN = 3;   // qubits outside the tile per tensor-core phase (2^3 image variants)
+constexpr int DENSE_MAX_VQ_PLAN = 4;   // qubits outside the tile per tensor-core phase (2^4 image variants)
 
 struct PhasePlan {
     uint64_t R;               // register qubits (global mask)
@@ -520,6 +521,15 @@ inline bool fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& ph
         descs[d].img_begin = 0;
         descs[d].img_count = 0;
     }
+    // one job per (phase, variant): the image slot, the phase's op range and its outside qubits
+    struct Job {
+        size_t slot;
+        uint32_t op_begin, op_end, var;
+        uint32_t vq[DENSE_MAX_VQ];
+        uint32_t nvq;
+    };
+    std::vector<Job> jobs;
+    size_t nimg = 0;
     for (size_t pi = 0; pi < phases.size(); ++pi) {
         auto& ph = phases[pi];
         SweepDesc& sd = descs[sweep_of[pi]];
@@ -539,25 +549,17 @@ inline bool fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& ph
             }
         }
         if (vq.size() > (size_t)DENSE_MAX_VQ) return false;
-        const size_t first = images.size() / DENSE_IMAGE_FLOATS;
+        const size_t first = nimg;
         const uint32_t nvar = 1u << vq.size();
         for (uint32_t var = 0; var < nvar; ++var) {
-            auto val = [&](uint32_t q) {
-                for (size_t j = 0; j < vq.size(); ++j)
-                    if (vq[j] == q) return (int)((var >> j) & 1u);
-                return 0;
-            };
-            std::vector<double> U(32 * 64, 0.0);
-            for (int col = 0; col < 32; ++col) {
-                double* v = &U[(size_t)col * 64];
-                v[2 * col] = 1.0;
-                for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
-                    const SwOp& op = ops[o];
-                    apply_op32(op, mats.data() + 2 * (size_t)op.mat, v, val(op.q0), val(op.q1));
-                }
-            }
-            images.resize(images.size() + DENSE_IMAGE_FLOATS);
-            dense_image(U, images.data() + (images.size() - DENSE_IMAGE_FLOATS));
+            Job jb{};
+            jb.slot = nimg++;
+            jb.op_begin = ph.op_begin;
+            jb.op_end = ph.op_end;
+            jb.var = var;
+            jb.nvq = (uint32_t)vq.size();
+            for (size_t k = 0; k < vq.size(); ++k) jb.vq[k] = vq[k];
+            jobs.push_back(jb);
         }
         if (sd.img_count == 0) sd.img_begin = (uint32_t)first;
         sd.img_count += nvar;
@@ -566,7 +568,7 @@ inline bool fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& ph
         d.k0 = (int8_t)vq.size();
         d.k1 = -1;
         uint8_t b[5] = {0, 0, 0, 0, 0};
-        for (size_t j = 0; j < vq.size(); ++j) b[j] = (uint8_t)vq[j];
+        for (size_t k = 0; k < vq.size(); ++k) b[k] = (uint8_t)vq[k];
         d.q0 = b[0];
         d.q1 = b[1];
         d.pad = b[2];
@@ -577,6 +579,41 @@ inline bool fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& ph
         ph.op_begin = begin;
         ph.op_end = (uint32_t)out.size();
         ++*ndense;
+    }
+    // build the images (the products in f64 and their TF32 split) on the host's cores
+    images.assign(nimg * DENSE_IMAGE_FLOATS, 0.0f);
+    auto work = [&](size_t j0, size_t j1) {
+        std::vector<double> U(32 * 64);
+        for (size_t jj = j0; jj < j1; ++jj) {
+            const Job& jb = jobs[jj];
+            auto val = [&](uint32_t q) {
+                for (uint32_t k = 0; k < jb.nvq; ++k)
+                    if (jb.vq[k] == q) return (int)((jb.var >> k) & 1u);
+                return 0;
+            };
+            std::fill(U.begin(), U.end(), 0.0);
+            for (int col = 0; col < 32; ++col) {
+                double* v = &U[(size_t)col * 64];
+                v[2 * col] = 1.0;
+                for (uint32_t o = jb.op_begin; o < jb.op_end; ++o) {
+                    const SwOp& op = ops[o];
+                    apply_op32(op, mats.data() + 2 * (size_t)op.mat, v, val(op.q0), val(op.q1));
+                }
+            }
+            dense_image(U, images.data() + jb.slot * DENSE_IMAGE_FLOATS);
+        }
+    };
+    const size_t nt = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), (jobs.size() + 15) / 16));
+    if (nt <= 1) {
+        work(0, jobs.size());
+    } else {
+        std::vector<std::thread> pool;
+        const size_t per = (jobs.size() + nt - 1) / nt;
+        for (size_t t = 0; t < nt; ++t) {
+            const size_t j0 = t * per, j1 = std::min(jobs.size(), j0 + per);
+            if (j0 < j1) pool.emplace_back(work, j0, j1);
+        }
+        for (auto& th : pool) th.join();
     }
     if (out.empty()) out.push_back(SwOp{});
     ops.swap(out);
