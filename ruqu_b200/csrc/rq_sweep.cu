@@ -1162,14 +1162,62 @@ bool plan_fits(const rq_plan* p, const rq_state* s) {
     return p->nq == s->nq && p->prec == s->prec && p->device == s->device;
 }
 
+// Prepared programs of recent gate lists, so that applying the same list again (a circuit
+// re-run from |0>, the repeated evaluations of a driver) skips the host planning and the
+// upload.  Keyed by device, qubit count, precision, tensor-core passes and every byte of
+// the gate list; a few entries, oldest evicted (its cudaFree waits for launches reading it).
+namespace {
+struct CachedPlan {
+    int device;
+    uint32_t nq;
+    int32_t prec;
+    int passes;
+    uint64_t hash;
+    std::vector<rq_gate> gates;
+    rq_plan* plan;
+};
+std::mutex g_plan_mu;
+std::vector<CachedPlan> g_plans;
+constexpr size_t PLAN_CACHE = 4;
+
+uint64_t bytes_hash(const void* p, size_t n) {
+    const unsigned char* b = static_cast<const unsigned char*>(p);
+    uint64_t h = 1469598103934665603ull;
+    for (size_t k = 0; k < n; ++k) {
+        h ^= b[k];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+}  // namespace
+
 int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n, int tc_passes) {
     if (n == 0) return RQ_OK;
+    const uint64_t h = bytes_hash(gates, n * sizeof(rq_gate));
+    std::lock_guard<std::mutex> lk(g_plan_mu);
+    for (size_t k = 0; k < g_plans.size(); ++k) {
+        CachedPlan& c = g_plans[k];
+        if (c.device == s->device && c.nq == s->nq && c.prec == s->prec && c.passes == tc_passes && c.hash == h &&
+            c.gates.size() == n && std::memcmp(c.gates.data(), gates, n * sizeof(rq_gate)) == 0) {
+            std::rotate(g_plans.begin() + k, g_plans.begin() + k + 1, g_plans.end());   // most recent last
+            return plan_launch(s, g_plans.back().plan);
+        }
+    }
     rq_plan* P = nullptr;
     RQ_TRY(plan_build(s, gates, n, RQ_EXEC_SWEEP, &P, tc_passes));
     int rc = plan_launch(s, P);
-    // cudaFree of the program waits for the launches that read it
-    plan_free(P);
-    return rc;
+    if (rc != RQ_OK) {
+        plan_free(P);
+        return rc;
+    }
+    if (g_plans.size() >= PLAN_CACHE) {
+        cudaSetDevice(g_plans.front().device);
+        plan_free(g_plans.front().plan);
+        g_plans.erase(g_plans.begin());
+        cudaSetDevice(s->device);
+    }
+    g_plans.push_back(CachedPlan{s->device, s->nq, s->prec, tc_passes, h, std::vector<rq_gate>(gates, gates + n), P});
+    return RQ_OK;
 }
 
 }  // namespace rq

@@ -88,3 +88,24 @@ def test_tc_plan_replays_and_equals_cuda_sweep_24q():
         pa.execute(a)
         pb.execute(b)
     assert np.max(np.abs(a.state_vector() - b.state_vector())) < 1e-5
+
+
+def test_repeated_gate_lists_reuse_their_program_and_changes_are_seen():
+    """apply_gates keeps the prepared programs of recent gate lists: the same list again gives
+    the same amplitudes, and a list that differs in one angle is planned afresh."""
+    n = 14
+    gates = workloads.random_layer_circuit(n, 4, 2)
+    g = QuantumState(n, 0, "f32")
+    g.apply_gates(gates, rq.RQ_EXEC_SWEEP_TC)
+    first = g.state_vector()
+    g.reset()
+    g.apply_gates(gates, rq.RQ_EXEC_SWEEP_TC)
+    assert np.array_equal(first, g.state_vector())
+    changed = list(gates)
+    k = next(i for i, x in enumerate(changed) if x[0] in (9, 10))   # an Rx / Ry / Rz angle
+    kind, a, b, ang = changed[k]
+    changed[k] = (kind, a, b, ang + 0.3)
+    g.reset()
+    g.apply_gates(changed, rq.RQ_EXEC_SWEEP_TC)
+    ref = _oracle_f64(n, changed)
+    assert float(np.max(np.abs(g.state_vector() - ref))) < 1e-5
