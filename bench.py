@@ -64,6 +64,7 @@ def _args():
     ap.add_argument("--no-warm", action="store_true", help="skip the warm-start leg")
     ap.add_argument("--no-variants", action="store_true", help="skip the per-mode runs and the f64 comparison")
     ap.add_argument("--no-sampling", action="store_true", help="skip the <Z_i> + shots leg on the final state")
+    ap.add_argument("--no-small", action="store_true", help="skip the 20-qubit f64 circuit leg")
     ap.add_argument("--warm-train", type=int, default=2048, help="training graphs for the warm start")
     ap.add_argument("--warm-eval", type=int, default=256, help="held-out graphs for the warm start")
     return ap.parse_args()
@@ -318,6 +319,51 @@ def _traffic_per_launch(a, stats):
     return _NCU_BYTES_PER_TILE[kern] * 2 ** (a.qubits - 13)
 
 
+def small_circuit_leg(with_cpu):
+    """The reference's small configuration: 20 qubits, complex f64, 40 random layers
+    (seed 0), then <Z_i> for every qubit and 4096 shots (a full simulator run with its
+    read-out).  Device time through the public API (state created, gates applied from the
+    host list, results back on the host), gates/s, per-layer GB/s; beside it the oracle's
+    scalar f64 reference kernels on the same circuit (gate application only)."""
+    import torch
+
+    import ruqu_b200 as rq
+    from ruqu_b200 import workloads
+    n, layers = 20, 40
+    gates = workloads.random_layer_circuit(n, layers, 0)
+    zs = [[(q, 3)] for q in range(n)]
+
+    def run():
+        st = rq.QuantumState(n, 0, "f64")
+        st.apply_gates(gates)
+        z = st.expectation_values(zs)
+        bits = st.sample(4096, 42)
+        return z, bits
+
+    run()
+    ms = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run()
+        torch.cuda.synchronize()
+        ms.append((time.perf_counter() - t0) * 1e3)
+    S = (1 << n) * 16
+    out = {"workload": "20 qubits, complex f64, 40 random layers (seed 0), <Z_i> x 20, 4096 shots",
+           "ms": min(ms), "gates_per_s": len(gates) / (min(ms) / 1e3),
+           "gbs_per_layer": (S + 2 * S * layers) / (min(ms) / 1e3) / 1e9}
+    if with_cpu:
+        import oracle
+        o = oracle.OracleState(n, oracle.RQ_F64, 0)
+        t0 = time.perf_counter()
+        o.apply(gates)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = {"ms": cpu_s * 1e3, "cores": 1, "kind": "port",
+                               "sample": "the same %d gates on the oracle's scalar f64 reference kernels" % len(gates)}
+        out["speedup_vs_cpu"] = cpu_s * 1e3 / min(ms)
+    return out
+
+
 def readout_leg(a, state, stream):
     """Read-out of the final state (the calls the reference's drivers make after a run):
     <Z_i> for every qubit (one FP64 reduction pass, state.rs:362-408), four two-qubit
@@ -544,6 +590,10 @@ def run_ours(a):
     if not a.no_sampling:
         readout = readout_leg(a, state, stream)
 
+    small = None
+    if not a.no_small and rank == 0:
+        small = small_circuit_leg(with_cpu=(ws == 1 and not a.no_cpu_baseline))
+
     variants = None
     if not a.no_variants and rank == 0:
         variants = variants_leg(a, garr)
@@ -596,6 +646,7 @@ def run_ours(a):
             "e2e": e2e,
             "gpu_launches": a.steps * (1 + stats["launches"]),
             "readout": readout,
+            "small_circuit": small,
             "variants": variants,
             "qaoa_batch": qaoa,
             "vqe_batch": vqe,
