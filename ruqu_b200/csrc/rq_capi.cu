@@ -361,8 +361,9 @@ int rq_plan_create(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t 
     RQ_TRY(set_device(s));
     int use_sweep = (mode != RQ_EXEC_PER_GATE && (mode != RQ_EXEC_AUTO || s->nq >= 12)) && s->nq >= 7;
     int passes = rq::tc_passes_of(mode);
-    if (mode == RQ_EXEC_AUTO && use_sweep) RQ_TRY(rq::autotune_tc(s, gates, n, &passes));
-    return rq::plan_build(s, gates, n, use_sweep ? RQ_EXEC_SWEEP : RQ_EXEC_PER_GATE, out, passes);
+    uint32_t m = 0;
+    if (mode == RQ_EXEC_AUTO && use_sweep) RQ_TRY(rq::autotune_tc(s, gates, n, &passes, &m));
+    return rq::plan_build(s, gates, n, use_sweep ? RQ_EXEC_SWEEP : RQ_EXEC_PER_GATE, out, passes, 2, m);
 }
 
 int rq_plan_execute(rq_state* s, const rq_plan* p) {
@@ -465,8 +466,9 @@ int rq_state_apply_mode(rq_state* s, const rq_gate* gates, uint64_t n, int32_t m
             for (uint64_t j = k; j < e; ++j)
                 if (gates[j].kind != RQ_GATE_BARRIER) run.push_back(gates[j]);
             int passes = rq::tc_passes_of(mode);
-            if (mode == RQ_EXEC_AUTO) RQ_TRY(rq::autotune_tc(s, run.data(), run.size(), &passes));
-            RQ_TRY(rq::apply_sweeps(s, run.data(), run.size(), passes));
+            uint32_t m = 0;
+            if (mode == RQ_EXEC_AUTO) RQ_TRY(rq::autotune_tc(s, run.data(), run.size(), &passes, &m));
+            RQ_TRY(rq::apply_sweeps(s, run.data(), run.size(), passes, m));
         } else {
             for (uint64_t j = k; j < e; ++j)
                 if (gates[j].kind != RQ_GATE_BARRIER) RQ_TRY(rq::apply_one_gate(s, gates[j]));

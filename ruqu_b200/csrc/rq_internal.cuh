@@ -102,12 +102,14 @@ int sample(rq_state* s, const uint32_t* qubits, uint32_t nq, uint64_t base_seed,
 // ---- fused sweeps and prepared plans (rq_sweep.cu) ---------------------------
 // tc_passes > 0: fuse each phase's slot-local gate runs into dense 32x32 unitaries
 // on the tensor cores (3 = 3xTF32, 1 = one TF32 pass); complex f32, m in {12, 13}
-int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n, int tc_passes = 0);
+// m > 0 overrides the number of local qubits of a sweep (the tile shape)
+int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n, int tc_passes = 0, uint32_t m = 0);
 int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out, int tc_passes = 0,
-               uint32_t tc_min_ops = 2);
-// RQ_EXEC_AUTO's measured choice between the CUDA-core and the 3xTF32 tensor-core sweep
-// (0 or 3 passes), cached per (device, qubits, gate structure)
-int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes);
+               uint32_t tc_min_ops = 2, uint32_t m = 0);
+// RQ_EXEC_AUTO's measured choice of execution (CUDA-core sweep, or 3xTF32 tensor-core sweep
+// with 13 or 12 local qubits): tensor-core passes (0 or 3) and tile shape (m, 0 = default),
+// cached per (device, qubits, gate structure)
+int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes, uint32_t* m);
 // the tensor-core passes a mode asks for (0: none)
 inline int tc_passes_of(int32_t mode) { return mode == RQ_EXEC_SWEEP_TC ? 3 : mode == RQ_EXEC_SWEEP_TC_FAST ? 1 : 0; }
 int plan_launch(rq_state* s, const rq_plan* p);

@@ -909,7 +909,7 @@ static uint32_t sweep_local_qubits(uint32_t nq, int32_t prec) {
 // tc_passes > 0 turns every phase into one dense 32x32 op applied on the tensor cores
 // (complex f32 states, m in {12, 13} only); tc_min_ops is kept for the ABI of this helper.
 int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out, int tc_passes,
-               uint32_t tc_min_ops) {
+               uint32_t tc_min_ops, uint32_t m_override) {
     rq_plan* P = new rq_plan();
     P->nq = s->nq;
     P->prec = s->prec;
@@ -935,7 +935,7 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
         return RQ_OK;
     }
     P->mode = RQ_EXEC_SWEEP;
-    const uint32_t m = sweep_local_qubits(nq, s->prec);
+    const uint32_t m = m_override ? std::min(nq, m_override) : sweep_local_qubits(nq, s->prec);
     if (s->prec != RQ_F32 || (m != 12 && m != 13)) tc_passes = 0;   // the tensor-core sweep's tile shapes
     const uint32_t c = std::min<uint32_t>(m, 5);
     std::vector<PGate> pg;
@@ -1019,7 +1019,7 @@ int apply_one_gate(rq_state* s, const rq_gate& g);   // rq_capi.cu
 // faster; the choice is cached per (device, qubits, structure).
 namespace {
 std::mutex g_tune_mu;
-std::map<std::tuple<int, uint32_t, uint64_t>, int> g_tune;
+std::map<std::tuple<int, uint32_t, uint64_t>, std::pair<int, uint32_t>> g_tune;
 
 uint64_t structure_hash(const rq_gate* g, uint64_t n) {
     uint64_t h = 1469598103934665603ull;
@@ -1057,8 +1057,9 @@ int time_plan(const rq_state& t, const rq_plan* P, float* ms) {
 }
 }  // namespace
 
-int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes) {
+int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes, uint32_t* m_out) {
     *passes = 0;
+    *m_out = 0;
     const uint32_t m = sweep_local_qubits(s->nq, s->prec);
     if (s->prec != RQ_F32 || (m != 12 && m != 13) || n == 0) return RQ_OK;
     if (const char* e = std::getenv("RUQU_AUTOTUNE"))
@@ -1068,37 +1069,56 @@ int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes
         std::lock_guard<std::mutex> lk(g_tune_mu);
         auto it = g_tune.find(key);
         if (it != g_tune.end()) {
-            *passes = it->second;
+            *passes = it->second.first;
+            *m_out = it->second.second;
             return RQ_OK;
         }
     }
-    rq_plan *A = nullptr, *B = nullptr;
-    RQ_TRY(plan_build(s, gates, n, RQ_EXEC_SWEEP, &A, 0));
-    // a circuit the tensor-core planner cannot take keeps the CUDA-core sweep
-    if (plan_build(s, gates, n, RQ_EXEC_SWEEP, &B, 3) != RQ_OK) B = nullptr;
-    int rc = RQ_OK;
-    int choice = 0;
-    if (B && B->stats.dense_ops > 0) {
-        void* scratch = nullptr;
-        if (cudaMalloc(&scratch, s->bytes()) == cudaSuccess) {
-            rq_state t = *s;
-            t.amps = scratch;
-            cudaMemsetAsync(scratch, 0, s->bytes(), s->stream);
-            float ta = 0.f, tb = 0.f;
-            rc = time_plan(t, A, &ta);
-            if (rc == RQ_OK) rc = time_plan(t, B, &tb);
-            if (rc == RQ_OK && tb < ta) choice = 3;
-            cudaFree(scratch);
-        } else {
-            cudaGetLastError();   // no room for a scratch state: keep the CUDA-core sweep
+    // candidates: CUDA-core sweep; 3xTF32 tensor-core sweep with the default tile and with one
+    // local qubit fewer (twice the CTAs per SM, more sweeps)
+    struct Cand {
+        int passes;
+        uint32_t m;
+        rq_plan* plan;
+        float ms;
+    };
+    std::vector<Cand> cands = {{0, 0, nullptr, 0.f}, {3, 0, nullptr, 0.f}};
+    if (m == 13 && s->nq > 13) cands.push_back({3, 12, nullptr, 0.f});
+    for (auto& c : cands)
+        if (plan_build(s, gates, n, RQ_EXEC_SWEEP, &c.plan, c.passes, 2, c.m) != RQ_OK) {
+            if (c.passes == 0) {   // the CUDA-core plan is the reference point
+                for (auto& d : cands) plan_free(d.plan);
+                return fail(RQ_ERR_CIRCUIT, "circuit error: the gate list cannot be planned");
+            }
+            c.plan = nullptr;       // a circuit the tensor-core planner cannot take
+            cudaGetLastError();
         }
+    int rc = RQ_OK;
+    int best = 0;
+    void* scratch = nullptr;
+    const bool any_tc = std::any_of(cands.begin() + 1, cands.end(), [](const Cand& c) {
+        return c.plan && c.plan->stats.dense_ops > 0;
+    });
+    if (any_tc && cudaMalloc(&scratch, s->bytes()) == cudaSuccess) {
+        rq_state t = *s;
+        t.amps = scratch;
+        cudaMemsetAsync(scratch, 0, s->bytes(), s->stream);
+        for (size_t k = 0; k < cands.size() && rc == RQ_OK; ++k)
+            if (cands[k].plan) rc = time_plan(t, cands[k].plan, &cands[k].ms);
+        for (size_t k = 1; k < cands.size() && rc == RQ_OK; ++k)
+            if (cands[k].plan && cands[k].plan->stats.dense_ops > 0 && cands[k].ms < cands[best].ms) best = (int)k;
+        cudaFree(scratch);
+    } else {
+        cudaGetLastError();   // no room for a scratch state (or nothing to compare): CUDA-core sweep
     }
-    plan_free(A);
-    if (B) plan_free(B);
+    const int choice_passes = cands[best].passes;
+    const uint32_t choice_m = cands[best].m;
+    for (auto& c : cands) plan_free(c.plan);
     RQ_TRY(rc);
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[key] = choice;
-    *passes = choice;
+    g_tune[key] = std::make_pair(choice_passes, choice_m);
+    *passes = choice_passes;
+    *m_out = choice_m;
     return RQ_OK;
 }
 
@@ -1172,6 +1192,7 @@ struct CachedPlan {
     uint32_t nq;
     int32_t prec;
     int passes;
+    uint32_t m;
     uint64_t hash;
     std::vector<rq_gate> gates;
     rq_plan* plan;
@@ -1191,20 +1212,21 @@ uint64_t bytes_hash(const void* p, size_t n) {
 }
 }  // namespace
 
-int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n, int tc_passes) {
+int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n, int tc_passes, uint32_t m) {
     if (n == 0) return RQ_OK;
     const uint64_t h = bytes_hash(gates, n * sizeof(rq_gate));
     std::lock_guard<std::mutex> lk(g_plan_mu);
     for (size_t k = 0; k < g_plans.size(); ++k) {
         CachedPlan& c = g_plans[k];
-        if (c.device == s->device && c.nq == s->nq && c.prec == s->prec && c.passes == tc_passes && c.hash == h &&
+        if (c.device == s->device && c.nq == s->nq && c.prec == s->prec && c.passes == tc_passes && c.m == m &&
+            c.hash == h &&
             c.gates.size() == n && std::memcmp(c.gates.data(), gates, n * sizeof(rq_gate)) == 0) {
             std::rotate(g_plans.begin() + k, g_plans.begin() + k + 1, g_plans.end());   // most recent last
             return plan_launch(s, g_plans.back().plan);
         }
     }
     rq_plan* P = nullptr;
-    RQ_TRY(plan_build(s, gates, n, RQ_EXEC_SWEEP, &P, tc_passes));
+    RQ_TRY(plan_build(s, gates, n, RQ_EXEC_SWEEP, &P, tc_passes, 2, m));
     int rc = plan_launch(s, P);
     if (rc != RQ_OK) {
         plan_free(P);
@@ -1216,7 +1238,7 @@ int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n, int tc_passes) {
         g_plans.erase(g_plans.begin());
         cudaSetDevice(s->device);
     }
-    g_plans.push_back(CachedPlan{s->device, s->nq, s->prec, tc_passes, h, std::vector<rq_gate>(gates, gates + n), P});
+    g_plans.push_back(CachedPlan{s->device, s->nq, s->prec, tc_passes, m, h, std::vector<rq_gate>(gates, gates + n), P});
     return RQ_OK;
 }
 
