@@ -353,6 +353,15 @@ RQ_API int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, d
                                   const double* target, double rtol, int32_t gradient, double* energies,
                                   uint32_t* steps_taken);
 
+/* As rq_qaoa_batch_optimize with exact gradients, but each step is a preconditioned
+ * ascent step theta += alpha_i * P_i * grad E with the caller's 2p x 2p matrix P_i per
+ * instance (precond: ninst x 2p x 2p, row-major, theta = (gammas, betas)), e.g. a learned
+ * -H^-1 of the family's energy landscape; alpha_i starts at alpha and halves whenever the
+ * instance's energy fell since its previous step.  No reference counterpart. */
+RQ_API int rq_qaoa_batch_optimize_precond(rq_qaoa_batch* b, uint32_t steps, const double* precond, double alpha,
+                                          double* gammas, double* betas, const double* target, double rtol,
+                                          double* energies, uint32_t* steps_taken);
+
 /* Final amplitudes of one circuit of the last run (2^n interleaved doubles);
  * only circuits of the last memory wave of that run are still held. */
 RQ_API int rq_qaoa_batch_state(rq_qaoa_batch* b, uint64_t circuit, double* interleaved);

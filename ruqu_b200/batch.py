@@ -101,6 +101,26 @@ class QaoaBatch:
         self.nsets = 1 if gradient == "adjoint" else 1 + 4 * self.p
         return g, b, e, st
 
+    def optimize_precond(self, gammas, betas, precond, steps: int, alpha: float = 0.8, target=None,
+                         rtol: float = 1e-5):
+        """Preconditioned ascent with exact gradients: theta += alpha_i P_i grad E per instance
+        (precond: ninst x 2p x 2p; alpha_i halves when an instance's energy falls).
+        Returns (gammas, betas, energies, steps_taken)."""
+        g = np.ascontiguousarray(np.array(gammas, dtype=np.float64).reshape(len(self.graphs), self.p))
+        b = np.ascontiguousarray(np.array(betas, dtype=np.float64).reshape(len(self.graphs), self.p))
+        P = np.ascontiguousarray(np.asarray(precond, dtype=np.float64).reshape(len(self.graphs), 2 * self.p,
+                                                                                 2 * self.p))
+        e = np.empty(len(self.graphs))
+        st = np.empty(len(self.graphs), dtype=np.uint32)
+        tp = None
+        if target is not None:
+            t = np.ascontiguousarray(target, dtype=np.float64)
+            tp = _dp(t)
+        check(lib.rq_qaoa_batch_optimize_precond(self._h, int(steps), _dp(P), float(alpha), _dp(g), _dp(b), tp,
+                                                 float(rtol), _dp(e), _u32p(st)))
+        self.nsets = 1
+        return g, b, e, st
+
     def state(self, circuit: int) -> np.ndarray:
         n = self.graphs[circuit // self.nsets][0]
         out = np.empty(2 << n)

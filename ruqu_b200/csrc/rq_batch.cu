@@ -1520,6 +1520,41 @@ __global__ void k_qaoa_shift(const double* __restrict__ theta, const uint32_t* _
 
 // one Adam step (gradient ascent on the expected cut) per instance, FP64 on the device;
 // frozen once the target is met.  done[i] = 1 + the step at which the target was met.
+// one preconditioned ascent step per instance: theta += alpha * P grad with the instance's
+// 2p x 2p preconditioner P (a learned -H^-1); alpha halves whenever the energy fell since the
+// previous step.  Frozen once the target is met, as the Adam step.
+__global__ void k_qaoa_precond(const double* __restrict__ energy, const uint32_t* __restrict__ act, uint32_t nact,
+                               uint32_t p, double* __restrict__ theta, const double* __restrict__ pre,
+                               double* __restrict__ alpha, double* __restrict__ eprev,
+                               const double* __restrict__ target, double rtol, uint32_t* __restrict__ done,
+                               double* __restrict__ elast, int final_eval, const double* __restrict__ grad,
+                               const uint32_t* __restrict__ step_dev) {
+    const uint32_t step = *step_dev;
+    const uint32_t P2 = 2 * p;
+    for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < nact; a += gridDim.x * blockDim.x) {
+        const uint32_t i = act[a];
+        if (done[i]) continue;
+        const double e = energy[a];
+        elast[i] = e;
+        if (target && e >= target[i] * (1.0 - rtol)) {
+            done[i] = step + 1;
+            continue;
+        }
+        if (final_eval) continue;
+        if (e < eprev[i]) alpha[i] *= 0.5;
+        eprev[i] = e;
+        const double* g = grad + (uint64_t)a * P2;
+        const double* P = pre + (uint64_t)i * P2 * P2;
+        double d[128];
+        for (uint32_t r = 0; r < P2; ++r) {
+            double s = 0.0;
+            for (uint32_t k = 0; k < P2; ++k) s += P[r * P2 + k] * g[k];
+            d[r] = s;
+        }
+        for (uint32_t r = 0; r < P2; ++r) theta[(uint64_t)i * P2 + r] += alpha[i] * d[r];
+    }
+}
+
 __global__ void k_step_inc(uint32_t* __restrict__ step) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1;
 }
@@ -1617,10 +1652,18 @@ int rq_qaoa_batch_gradient(rq_qaoa_batch* b, const double* gammas, const double*
     return RQ_OK;
 }
 
-int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, double* betas,
-                           const double* target, double rtol, int32_t gradient, double* energies,
-                           uint32_t* steps_taken) {
+}  // extern "C"
+
+namespace {
+
+// Adam (precond == nullptr) or preconditioned ascent (precond: ninst x 2p x 2p, caller order)
+int optimize_impl(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, double* betas, const double* target,
+                  double rtol, int32_t gradient, const double* precond, double alpha0, double* energies,
+                  uint32_t* steps_taken) {
     if (!b || !gammas || !betas || !energies || !steps_taken) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (precond && gradient != RQ_QAOA_GRAD_ADJOINT)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "preconditioned steps take the exact (adjoint) gradient");
+    if (precond && 2 * b->p > 128) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "preconditioned steps take p <= 64");
     if (gradient != RQ_QAOA_GRAD_ADJOINT && gradient != RQ_QAOA_GRAD_SHIFT)
         return rq::fail(RQ_ERR_INVALID_ARGUMENT, "gradient must be RQ_QAOA_GRAD_ADJOINT or RQ_QAOA_GRAD_SHIFT");
     RQ_CUDA(cudaSetDevice(b->device));
@@ -1648,6 +1691,7 @@ int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* 
             for (size_t j = 0; j < b->classes[k].insts.size(); ++j) cls_of[r++] = (uint32_t)k;
     }
     double *d_th = nullptr, *d_m = nullptr, *d_v = nullptr, *d_tg = nullptr, *d_el = nullptr;
+    double *d_pre = nullptr, *d_alpha = nullptr, *d_eprev = nullptr;
     uint32_t *d_done = nullptr, *d_act = nullptr, *d_step = nullptr;
     // one optimizer step as a CUDA graph, captured per active set (after an uncaptured first
     // step has sized every buffer) and replayed until the set changes
@@ -1662,7 +1706,7 @@ int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* 
     };
     auto cleanup = [&]() {
         drop_graph();
-        void* q[] = {d_th, d_m, d_v, d_tg, d_el, d_done, d_act, d_step};
+        void* q[] = {d_th, d_m, d_v, d_tg, d_el, d_done, d_act, d_step, d_pre, d_alpha, d_eprev};
         for (void* x : q) if (x) cudaFree(x);
     };
     int rc = RQ_OK;
@@ -1674,7 +1718,24 @@ int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* 
     if (rc == RQ_OK) rc = dalloc_b(&d_done, ninst);
     if (rc == RQ_OK) rc = dalloc_b(&d_act, ninst);
     if (rc == RQ_OK) rc = dalloc_b(&d_step, 1);
+    if (precond) {
+        if (rc == RQ_OK) rc = dalloc_b(&d_pre, (size_t)ninst * P2 * P2);
+        if (rc == RQ_OK) rc = dalloc_b(&d_alpha, ninst);
+        if (rc == RQ_OK) rc = dalloc_b(&d_eprev, ninst);
+    }
     if (rc != RQ_OK) { cleanup(); return rc; }
+    std::vector<double> pre_run, alpha_init, eprev_init;
+    if (precond) {   // preconditioners in run order
+        pre_run.resize((size_t)ninst * P2 * P2);
+        for (uint32_t r = 0; r < ninst; ++r)
+            std::memcpy(&pre_run[(size_t)r * P2 * P2], precond + (size_t)inst_order[r] * P2 * P2,
+                        (size_t)P2 * P2 * sizeof(double));
+        alpha_init.assign(ninst, alpha0);
+        eprev_init.assign(ninst, -1e300);
+        cudaMemcpyAsync(d_pre, pre_run.data(), pre_run.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+        cudaMemcpyAsync(d_alpha, alpha_init.data(), ninst * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+        cudaMemcpyAsync(d_eprev, eprev_init.data(), ninst * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+    }
     // active set: run-order instances still optimising, their circuits' instance map, and per-class counts
     std::vector<uint32_t> act(ninst), ci;
     for (uint32_t r = 0; r < ninst; ++r) act[r] = r;
@@ -1709,10 +1770,15 @@ int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* 
         const uint64_t ncirc = (uint64_t)nact * nsets;
         k_qaoa_shift<<<rq::grid_for(ncirc * p, TPB, sms), TPB, 0, b->stream>>>(d_th, d_act, nact, p, nsets, b->d_ang);
         RQ_TRY(qaoa_launch(b, nsets, 0, 0, &per_class, adj && !final_eval));
-        k_qaoa_adam<<<rq::grid_for(nact, TPB, sms), TPB, 0, b->stream>>>(b->d_energy, d_act, nact, p, nsets, d_th, d_m,
-                                                                      d_v, lr, 0, target ? d_tg : nullptr, rtol,
-                                                                      d_done, d_el, final_eval ? 1 : 0,
-                                                                      adj ? b->d_grad : nullptr, d_step);
+        if (precond)
+            k_qaoa_precond<<<rq::grid_for(nact, TPB, sms), TPB, 0, b->stream>>>(
+                b->d_energy, d_act, nact, p, d_th, d_pre, d_alpha, d_eprev, target ? d_tg : nullptr, rtol, d_done,
+                d_el, final_eval ? 1 : 0, b->d_grad, d_step);
+        else
+            k_qaoa_adam<<<rq::grid_for(nact, TPB, sms), TPB, 0, b->stream>>>(b->d_energy, d_act, nact, p, nsets, d_th,
+                                                                          d_m, d_v, lr, 0, target ? d_tg : nullptr,
+                                                                          rtol, d_done, d_el, final_eval ? 1 : 0,
+                                                                          adj ? b->d_grad : nullptr, d_step);
         k_step_inc<<<1, 32, 0, b->stream>>>(d_step);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return rq::cuda_fail(e, "optimizer kernels");
@@ -1789,6 +1855,25 @@ int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* 
         steps_taken[i] = dn[r] ? dn[r] - 1 : steps;
     }
     return RQ_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rq_qaoa_batch_optimize(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, double* betas,
+                           const double* target, double rtol, int32_t gradient, double* energies,
+                           uint32_t* steps_taken) {
+    return optimize_impl(b, steps, lr, gammas, betas, target, rtol, gradient, nullptr, 0.0, energies, steps_taken);
+}
+
+int rq_qaoa_batch_optimize_precond(rq_qaoa_batch* b, uint32_t steps, const double* precond, double alpha,
+                                   double* gammas, double* betas, const double* target, double rtol,
+                                   double* energies, uint32_t* steps_taken) {
+    if (!precond) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (!(alpha > 0.0)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "alpha must be positive");
+    return optimize_impl(b, steps, 0.0, gammas, betas, target, rtol, RQ_QAOA_GRAD_ADJOINT, precond, alpha, energies,
+                         steps_taken);
 }
 
 int rq_qaoa_batch_state(rq_qaoa_batch* b, uint64_t circuit, double* interleaved) {

@@ -125,6 +125,7 @@ class WarmStart:
         self.net = Mlp(h1=hidden, h2=hidden, n_out=2 * p, seed=seed)
         self.mu = np.zeros(2 * p)
         self.sd = np.ones(2 * p)
+        self.precond = {}
 
     def fit(self, graphs, gammas, betas, copies: int = 4, val_fraction: float = 0.125, chunks: int = 12,
             chunk_steps: int = 500, lr: float = 1e-3, batch: int = 256, seed: int = 3) -> list:
@@ -154,6 +155,42 @@ class WarmStart:
         else:
             self.net.set_params(best_p)
         return hist
+
+    def fit_curvature(self, graphs, gammas, betas, h: float = 1e-3, max_graphs: int = 512) -> dict:
+        """Learn the curvature of the energy landscape near the optimum: for each graph size n,
+        the average Hessian of <C> at the training graphs' optimised angles (central
+        differences, step h, of exact adjoint gradients on the GPU), stored as the ascent
+        preconditioner P_n = -H_n^-1 (eigenvalues clamped to keep -H positive definite).
+        Returns {n: eigenvalues of H_n}."""
+        from .batch import QaoaBatch
+        th = np.concatenate([np.asarray(gammas, dtype=np.float64), np.asarray(betas, dtype=np.float64)], axis=1)
+        sub = np.arange(min(len(graphs), max_graphs))
+        qb = QaoaBatch([graphs[i] for i in sub], self.p, "f32")
+        cols = []
+        for j in range(2 * self.p):
+            tp, tm = th[sub].copy(), th[sub].copy()
+            tp[:, j] += h
+            tm[:, j] -= h
+            _, gp = qb.gradient(tp[:, :self.p], tp[:, self.p:])
+            _, gm = qb.gradient(tm[:, :self.p], tm[:, self.p:])
+            cols.append((gp - gm) / (2 * h))
+        H = np.stack(cols, axis=2)
+        H = 0.5 * (H + H.transpose(0, 2, 1))
+        ns = np.array([graphs[i][0] for i in sub])
+        self.precond = {}
+        eig = {}
+        for n in sorted(set(ns.tolist())):
+            Hn = H[ns == n].mean(axis=0)
+            w, V = np.linalg.eigh(Hn)
+            eig[n] = w
+            w = np.minimum(w, -1e-3 * max(1.0, float(np.max(np.abs(w)))))
+            self.precond[n] = (V * (-1.0 / w)) @ V.T
+        return eig
+
+    def preconditioners(self, graphs) -> np.ndarray:
+        """P_n of each graph's size (the nearest learned size when n was not seen)."""
+        sizes = np.array(sorted(self.precond))
+        return np.stack([self.precond[int(sizes[np.argmin(np.abs(sizes - n))])] for n, _ in graphs])
 
     def predict(self, graphs, tta: int = 8, seed: int = 9):
         x = features(graphs, tta, seed=seed)

@@ -129,3 +129,63 @@ def test_step_graph_replay_equals_plain_launches(monkeypatch):
     monkeypatch.setenv("RUQU_NO_GRAPHS", "1")
     gb, bb, eb, sb = qb.optimize(G, B, 25, 0.05, target=tgt, rtol=1e-5)
     assert np.array_equal(ga, gb) and np.array_equal(ba, bb) and np.array_equal(ea, eb) and np.array_equal(sa, sb)
+
+
+def test_preconditioned_steps_match_host_loop():
+    """theta += alpha_i P_i grad, alpha_i halved when the energy fell, frozen at the target:
+    the device loop against the same rule on the host over the engine's exact gradients."""
+    graphs = _graphs(5, [8, 10, 12], 8)
+    p, steps = 2, 6
+    g0, b0 = linear_ramp(p)
+    G, B = np.tile(g0, (5, 1)), np.tile(b0, (5, 1))
+    r = np.random.default_rng(3)
+    A = r.normal(size=(5, 2 * p, 2 * p))
+    P = 0.01 * (np.einsum('kij,klj->kil', A, A) + np.eye(2 * p))
+    qb = QaoaBatch(graphs, p, "f64")
+    _, _, e3, _ = qb.optimize(G, B, 3, 0.05)
+    target = np.where(np.arange(5) % 2 == 0, e3, 1e9)
+    g, b, e, st = qb.optimize_precond(G, B, P, steps, 0.8, target=target, rtol=1e-5)
+    th = np.concatenate([G, B], axis=1)
+    alpha = np.full(5, 0.8)
+    eprev = np.full(5, -1e300)
+    done = np.zeros(5, dtype=int)
+    elast = np.zeros(5)
+    for t in range(steps + 1):
+        en, gr = qb.gradient(th[:, :p], th[:, p:])
+        for k in range(5):
+            if done[k]:
+                continue
+            elast[k] = en[k]
+            if en[k] >= target[k] * (1 - 1e-5):
+                done[k] = t + 1
+                continue
+            if t == steps:
+                continue
+            if en[k] < eprev[k]:
+                alpha[k] *= 0.5
+            eprev[k] = en[k]
+            th[k] += alpha[k] * (P[k] @ gr[k])
+    assert np.max(np.abs(g - th[:, :p])) < 1e-12 and np.max(np.abs(b - th[:, p:])) < 1e-12
+    assert np.max(np.abs(e - elast)) < 1e-12
+    assert np.array_equal(st, np.where(done > 0, done - 1, steps))
+
+
+def test_learned_curvature_pipeline_beats_plain():
+    p, steps, lr = 4, 100, 0.05
+    train = _graphs(768, [8, 10, 12], 3)
+    held = _graphs(64, [10, 12], 4)
+    g0, b0 = linear_ramp(p)
+    qb = QaoaBatch(train, p, "f32")
+    g, b, _, _ = qb.optimize(np.tile(g0, (len(train), 1)), np.tile(b0, (len(train), 1)), steps, lr)
+    warm = WarmStart(p)
+    warm.fit(train, g, b, chunks=4, chunk_steps=300)
+    eig = warm.fit_curvature(train, g, b)
+    assert all(np.all(w < 0) for w in eig.values())          # a maximum: negative curvature
+    hb = QaoaBatch(held, p, "f32")
+    G0, B0 = np.tile(g0, (len(held), 1)), np.tile(b0, (len(held), 1))
+    _, _, target, _ = hb.optimize(G0, B0, steps, lr)
+    _, _, e_ramp, st_ramp = hb.optimize(G0, B0, steps, lr, target=target, rtol=1e-5)
+    pg, pb = warm.predict(held)
+    _, _, e_wp, st_wp = hb.optimize_precond(pg, pb, warm.preconditioners(held), steps, 0.8, target=target, rtol=1e-5)
+    assert np.mean(e_wp >= target * (1 - 1e-5)) >= 0.9
+    assert np.median(st_wp) < 0.5 * np.median(st_ramp), (np.median(st_wp), np.median(st_ramp))
