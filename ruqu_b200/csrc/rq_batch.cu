@@ -1814,7 +1814,7 @@ int optimize_impl(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, d
     polled:
         if (rc != RQ_OK) break;
         cudaError_t e = cudaSuccess;
-        if (target && step < steps && (step % 5 == 4)) {
+        if (target && step < steps && (step % 2 == 1)) {
             // drop the instances that met their target from the next steps' launches; the
             // rest keep their slots' math (every circuit's energy is independent of the batch)
             e = cudaMemcpyAsync(dn.data(), d_done, ninst * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);

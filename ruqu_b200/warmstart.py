@@ -102,11 +102,32 @@ def features(graphs, copies: int = 1, seed=None) -> np.ndarray:
     with its nodes placed at random distinct rows of the padded matrix (graph-major
     order): the angles do not depend on node labels, and every input position is
     exercised during training whatever the graph sizes."""
+    for n, _ in graphs:
+        if n > PAD_NODES:
+            raise ValueError(f"graphs up to {PAD_NODES} nodes")
+    nrows = len(graphs) * (copies if seed is not None else 1)
     if seed is None:
-        return np.stack([graph_features(n, e) for n, e in graphs]).astype(np.float32)
-    r = np.random.default_rng(seed)
-    rows = [graph_features(n, e, r.permutation(PAD_NODES)[:n]) for n, e in graphs for _ in range(copies)]
-    return np.stack(rows).astype(np.float32)
+        pos = np.tile(np.arange(PAD_NODES), (nrows, 1))
+    else:   # a random placement per row: the first n entries of a random permutation
+        pos = np.argsort(np.random.default_rng(seed).random((nrows, PAD_NODES)), axis=1)
+    reps = copies if seed is not None else 1
+    row_of, us, vs = [], [], []
+    for gi, (n, edges) in enumerate(graphs):
+        if not len(edges):
+            continue
+        e = np.asarray(edges, dtype=np.int64).reshape(-1, 2)
+        for c in range(reps):
+            r = gi * reps + c
+            row_of.append(np.full(len(e), r))
+            us.append(pos[r, e[:, 0]])
+            vs.append(pos[r, e[:, 1]])
+    a = np.zeros((nrows, PAD_NODES, PAD_NODES), dtype=np.float32)
+    if row_of:
+        rr, uu, vv = np.concatenate(row_of), np.concatenate(us), np.concatenate(vs)
+        a[rr, uu, vv] = 1.0
+        a[rr, vv, uu] = 1.0
+    iu = np.triu_indices(PAD_NODES, 1)
+    return np.ascontiguousarray(a[:, iu[0], iu[1]])
 
 
 class WarmStart:
