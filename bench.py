@@ -228,10 +228,22 @@ def vqe_batch_leg(a, ws, rank, with_cpu):
         wall.append(time.perf_counter() - t0)
         ms.append(vb.last_ms())
     circuits = len(params) * (1 + 2 * n * depth)
+    # the same energies and gradients by the adjoint pass (one forward, lambda = H psi, one backward)
+    vb.run(params[:2], gradient="adjoint")
+    ams = []
+    for _ in range(3):
+        ea, ga = vb.run(params, gradient="adjoint")
+        ams.append(vb.last_ms())
+    scale = float(np.sum(np.abs(coeffs)))
     res = {"workload": "batched VQE, 16 qubits, 200-term Pauli Hamiltonian, depth-8 Ry+CZ ansatz, %d parameter "
                        "sets x 257 parameter-shift circuits, f32 states" % a.vqe_sets,
            "circuits_per_rank": circuits, "device_ms": min(ms), "wall_ms": 1e3 * min(wall),
-           "circuits_per_s": circuits * ws / (min(ms) / 1e3), "mean_energy": float(np.mean(e))}
+           "circuits_per_s": circuits * ws / (min(ms) / 1e3), "mean_energy": float(np.mean(e)),
+           "gradient_sets_per_s_shift": len(params) * ws / (min(ms) / 1e3),
+           "adjoint": {"device_ms": min(ams), "gradient_sets_per_s": len(params) * ws / (min(ams) / 1e3),
+                       "speedup_vs_shift": min(ms) / min(ams),
+                       "max_abs_grad_diff_vs_shift_rel": float(np.max(np.abs(ga - g))) / scale,
+                       "energies_identical": bool(np.array_equal(ea, e))}}
     if with_cpu:
         import oracle
         t0 = time.perf_counter()

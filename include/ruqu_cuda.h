@@ -388,11 +388,21 @@ RQ_API int rq_vqe_batch_create(uint32_t num_qubits, uint32_t depth, const double
                                const rq_pauli_op* ops, const uint32_t* offsets, uint32_t nterms,
                                int32_t precision, rq_vqe_batch** out);
 
+/* Gradient modes of rq_vqe_batch_run.
+ * RQ_VQE_GRAD_SHIFT: gradients[s*P + k] = (E(theta_k + pi/2) - E(theta_k - pi/2)) / 2,
+ *   the parameter-shift rule of run_vqe (vqe.rs:186-198): 1 + 2P circuits per set.
+ * RQ_VQE_GRAD_ADJOINT: the same derivative (the shift rule is exact for Ry) by one
+ *   backward pass per set: lambda = H psi, then psi and lambda run back through the
+ *   ansatz and every Ry(theta_k) = exp(-i theta_k Y/2) contributes Im <lambda|Y|psi>.
+ *   No reference counterpart (run_vqe only has the shift rule). */
+#define RQ_VQE_GRAD_NONE 0
+#define RQ_VQE_GRAD_SHIFT 1
+#define RQ_VQE_GRAD_ADJOINT 2
+
 /* energies[s] = <psi(params_s)|H|psi(params_s)> (evaluate_energy, vqe.rs:122-131)
- * for s < nsets, params_s = params[s*P .. s*P+P).  With with_gradient != 0 also
- * gradients[s*P + k] = (E(theta_k + pi/2) - E(theta_k - pi/2)) / 2 (the
- * parameter-shift rule of vqe.rs:186-198): 1 + 2P circuits per set, all run
- * on the device in waves.  Energies accumulate in FP64. */
+ * for s < nsets, params_s = params[s*P .. s*P+P); with_gradient (RQ_VQE_GRAD_*)
+ * selects whether and how gradients[s*P + k] = dE/dtheta_k is computed.  All
+ * circuits run on the device in waves; energies and gradients accumulate in FP64. */
 RQ_API int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* params,
                             int32_t with_gradient, double* energies, double* gradients);
 

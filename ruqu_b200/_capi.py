@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(HERE, "libruqu_cuda.so")
 
 RQ_F32, RQ_F64 = 0, 1
 RQ_QAOA_GRAD_ADJOINT, RQ_QAOA_GRAD_SHIFT = 0, 1
+RQ_VQE_GRAD_NONE, RQ_VQE_GRAD_SHIFT, RQ_VQE_GRAD_ADJOINT = 0, 1, 2
 RQ_EXEC_AUTO, RQ_EXEC_PER_GATE, RQ_EXEC_SWEEP, RQ_EXEC_SWEEP_TC, RQ_EXEC_SWEEP_TC_FAST = 0, 1, 2, 3, 4
 
 (RQ_OK, RQ_ERR_QUBIT_LIMIT_EXCEEDED, RQ_ERR_INVALID_QUBIT_INDEX, RQ_ERR_MEMORY_ALLOCATION,

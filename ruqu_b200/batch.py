@@ -159,15 +159,21 @@ class VqeBatch:
                                       RQ_F32 if precision == "f32" else RQ_F64, C.byref(h)))
         self._h = h
 
-    def run(self, params, gradient: bool = False):
-        """params: (nsets, P).  Returns energies (nsets,) and, with gradient=True, (nsets, P) gradients."""
+    def run(self, params, gradient=False):
+        """params: (nsets, P).  Returns energies (nsets,) and, with a gradient, (nsets, P)
+        gradients: gradient=True or "shift" for the parameter-shift rule of run_vqe
+        (vqe.rs:186-198, 1 + 2P circuits per set), "adjoint" for the same derivative by one
+        backward pass per set."""
+        mode = {False: _capi.RQ_VQE_GRAD_NONE, None: _capi.RQ_VQE_GRAD_NONE, True: _capi.RQ_VQE_GRAD_SHIFT,
+                "shift": _capi.RQ_VQE_GRAD_SHIFT, "adjoint": _capi.RQ_VQE_GRAD_ADJOINT}[gradient]
         p = np.ascontiguousarray(np.atleast_2d(np.asarray(params, dtype=np.float64)))
         nsets = p.shape[0]
-        assert p.shape[1] == self.P
+        if p.shape[1] != self.P:
+            raise ValueError(f"params must have {self.P} columns")
         e = np.empty(nsets)
-        g = np.empty((nsets, self.P)) if gradient else np.empty(1)
-        check(lib.rq_vqe_batch_run(self._h, nsets, _dp(p), 1 if gradient else 0, _dp(e), _dp(g)))
-        return (e, g) if gradient else e
+        g = np.empty((nsets, self.P)) if mode else np.empty(1)
+        check(lib.rq_vqe_batch_run(self._h, nsets, _dp(p), mode, _dp(e), _dp(g)))
+        return (e, g) if mode else e
 
     def last_ms(self) -> float:
         ms = C.c_float()

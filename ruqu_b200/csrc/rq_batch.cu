@@ -68,7 +68,8 @@ struct QArgs {
     double* epart;                 // [wave circuit][ntiles]
     T amp0;                        // 2^(-n/2)
     typename C2<T>::t* lam;        // adjoint sweeps: lambda of circuit c at lam + c * 2^n
-    double* gpart;                 // adjoint sweeps: [wave circuit][ntiles][2p] gradient partials
+    double* gpart;                 // adjoint sweeps: [wave circuit][ntiles][gwidth] gradient partials
+    uint32_t gwidth;               // adjoint sweeps: gradient entries per circuit (2p for QAOA, P for VQE)
 };
 
 // cut(x) for the register amplitudes of one thread: x = U | deposit(i).
@@ -427,6 +428,34 @@ __device__ __forceinline__ double dispatch_im_x(int k, const V* p, const V* l) {
     return 0.0;
 }
 
+// Im <lambda|Y_K|psi> over the register pairs: Y|0> = i|1>, Y|1> = -i|0>, so
+// <lambda|Y psi> = sum_pairs i conj(l_j) p_i - i conj(l_i) p_j and its imaginary
+// part is Re(conj(l_j) p_i) - Re(conj(l_i) p_j).
+template <int K, int NR, typename V>
+__device__ __forceinline__ double im_y_overlap(const V* p, const V* l) {
+    double acc = 0.0;
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+        if (i & (1 << K)) continue;
+        const int j = i | (1 << K);
+        acc += (double)(l[j].x * p[i].x + l[j].y * p[i].y) - (double)(l[i].x * p[j].x + l[i].y * p[j].y);
+    }
+    return acc;
+}
+
+template <int NR, typename V>
+__device__ __forceinline__ double dispatch_im_y(int k, const V* p, const V* l) {
+    switch (k) {
+        case 0: return im_y_overlap<0, NR>(p, l);
+        case 1: return im_y_overlap<1, NR>(p, l);
+        case 2: return im_y_overlap<2, NR>(p, l);
+        case 3: if constexpr (NR > 8) return im_y_overlap<3, NR>(p, l); break;
+        case 4: if constexpr (NR > 16) return im_y_overlap<4, NR>(p, l); break;
+        default: break;
+    }
+    return 0.0;
+}
+
 template <typename T, int RB>
 __global__ void __launch_bounds__(512, 1) k_batch_adjoint(const SweepDesc d, const PhaseDesc* __restrict__ phases,
                                                         const SwOp* __restrict__ ops, QArgs<T> a) {
@@ -447,7 +476,7 @@ __global__ void __launch_bounds__(512, 1) k_batch_adjoint(const SweepDesc d, con
     const uint32_t ngroup = small ? T_ : (T_ >> 5);
     const uint32_t grp = small ? tid : (tid >> 5);
     const uint32_t lane = tid & 31u;
-    const uint32_t P2 = 2 * a.p;
+    const uint32_t P2 = a.gwidth;
     const uint64_t cmask = (1ull << d.c) - 1;
     uint64_t dep_tid = 0;
     {
@@ -459,7 +488,7 @@ __global__ void __launch_bounds__(512, 1) k_batch_adjoint(const SweepDesc d, con
     const uint32_t stid = swzb<T>(tid * EPV);
     const uint64_t nwork = a.ncirc * a.ntiles;
     const uint64_t nstate = 1ull << d.n;
-    const bool initl = (d.flags & SWEEP_INIT_LAMBDA) != 0;
+    const bool initl = (d.flags & SWEEP_INIT_LAMBDA) != 0;   // QAOA only: lambda = C psi
 
     auto flush = [&](double v, uint32_t idx) {
         if (!small) {
@@ -475,9 +504,13 @@ __global__ void __launch_bounds__(512, 1) k_batch_adjoint(const SweepDesc d, con
         const uint64_t gcirc = a.circ0 + circ;
         V* psi = a.amps + circ * nstate;
         V* lam = a.lam + circ * nstate;
-        const uint32_t inst = a.circ_inst[gcirc];
-        const uint8_t* edges = a.edges + 2 * (size_t)a.eoff[inst];
-        const uint32_t ne = a.ne[inst];
+        const uint8_t* edges = nullptr;
+        uint32_t ne = 0;
+        if (a.circ_inst) {
+            const uint32_t inst = a.circ_inst[gcirc];
+            edges = a.edges + 2 * (size_t)a.eoff[inst];
+            ne = a.ne[inst];
+        }
         uint64_t base = 0;
         for (uint32_t b = 0; b < d.nonlocal_count; ++b)
             if ((tile >> b) & 1ull) base |= 1ull << d.nonlocal[b];
@@ -560,6 +593,26 @@ __global__ void __launch_bounds__(512, 1) k_batch_adjoint(const SweepDesc d, con
                         rl[i] = cmulv(rl[i], tab[2 * c], -tab[2 * c + 1]);
                     }
                     flush(2.0 * acc, op.param);
+                } else if (op.type == OP_RYP) {
+                    // Ry(theta) = exp(-i theta Y / 2): dE/dtheta = Im <lambda|Y|psi>
+                    const T* r = a.rot + ((size_t)gcirc * a.nparam + op.param) * 2;
+                    flush(dispatch_im_y<NR>(op.k0, rp, rl), op.param);
+                    dispatch_ry<NR>(op.k0, rp, r[0], -r[1]);
+                    dispatch_ry<NR>(op.k0, rl, r[0], -r[1]);
+                } else if (op.type == OP_CZ) {   // self-inverse
+                    const int k0 = op.k0, k1 = op.k1;
+                    const int u0 = (int)((U >> op.q0) & 1ull), u1 = (int)((U >> op.q1) & 1ull);
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) {
+                        const int b0 = k0 >= 0 ? ((i >> k0) & 1) : u0;
+                        const int b1 = k1 >= 0 ? ((i >> k1) & 1) : u1;
+                        if (b0 & b1) {
+                            rp[i].x = -rp[i].x;
+                            rp[i].y = -rp[i].y;
+                            rl[i].x = -rl[i].x;
+                            rl[i].y = -rl[i].y;
+                        }
+                    }
                 }
             }
 #pragma unroll
@@ -1000,6 +1053,44 @@ constexpr int TPB = 256;
 
 }  // namespace
 
+// One Hamiltonian string as the operator i^ny X^x Z^pm: (P psi)[i] = c_k (-1)^popc((i^x) & pm) psi[i ^ x]
+// with c_k = coeff * i^ny (ny = number of Y factors); (cr, ci) = c_k.
+struct HTerm {
+    uint64_t x, pm;
+    double cr, ci;
+};
+
+// lambda = H psi for every circuit of a wave (the start of the VQE adjoint pass).  One
+// output amplitude per thread and grid-stride step; the strings are read in order by
+// every thread (uniform loads), psi[i ^ x] from L2 (a warp's 32 indices map to one
+// aligned 32-amplitude block), the sum over strings in FP64.
+template <typename T>
+__global__ void __launch_bounds__(256) k_vqe_apply_h(const typename C2<T>::t* __restrict__ psi,
+                                                     typename C2<T>::t* __restrict__ lam, uint32_t n, uint64_t ncirc,
+                                                     const HTerm* __restrict__ terms, uint32_t nterms) {
+    using V = typename C2<T>::t;
+    const uint64_t N = 1ull << n;
+    const uint64_t total = ncirc * N;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total; w += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = w >> n, i = w & (N - 1);
+        const V* src = psi + c * N;
+        double re = 0.0, im = 0.0;
+        for (uint32_t k = 0; k < nterms; ++k) {
+            const HTerm t = terms[k];
+            const uint64_t j = i ^ t.x;
+            const V v = src[j];
+            const double sg = (__popcll(j & t.pm) & 1) ? -1.0 : 1.0;
+            const double cr = sg * t.cr, ci = sg * t.ci;
+            re += cr * (double)v.x - ci * (double)v.y;
+            im += cr * (double)v.y + ci * (double)v.x;
+        }
+        V o;
+        o.x = (T)re;
+        o.y = (T)im;
+        lam[w] = o;
+    }
+}
+
 // ===========================================================================
 // batch object
 // ===========================================================================
@@ -1170,6 +1261,7 @@ int adjoint_class(rq_qaoa_batch* b, QClass& K, uint64_t ncirc, uint64_t circ0, v
     a.p = b->p;
     a.phs = b->phs;
     a.gpart = b->d_gpart;
+    a.gwidth = P2;
     const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(K.aprog);
     const SwOp* op = reinterpret_cast<const SwOp*>(K.aprog + K.aoff_ops);
     auto kern = k_batch_adjoint<T, RBc>;
@@ -1933,6 +2025,7 @@ struct rq_vqe_batch {
     VTerm* d_terms = nullptr;
     uint32_t* d_gofs = nullptr;   // groups of top pattern t: [gofs[t], gofs[t+1])
     uint32_t ngroups = 0, nterms = 0;
+    uint32_t em = 0;              // log2 amplitudes of an energy tile
     double* d_part = nullptr;
     size_t part_cap = 0;
     double* d_params = nullptr;
@@ -1945,6 +2038,20 @@ struct rq_vqe_batch {
     size_t energy_cap = 0;
     float last_ms = 0.f;
     size_t wave_bytes = (size_t)96 << 20;   // states per wave kept around the L2 size
+    // exact gradients: the reversed ansatz as an adjoint program, H as operator strings
+    uint32_t am = 0;
+    uint64_t antiles = 0;
+    std::vector<SweepDesc> adescs;
+    unsigned char* aprog = nullptr;
+    size_t aoff_ops = 0;
+    HTerm* d_hterms = nullptr;
+    uint32_t nhterms = 0;
+    void* d_lam = nullptr;
+    size_t lam_cap = 0;
+    double* d_gpart = nullptr;
+    size_t gpart_cap = 0;
+    double* d_grad = nullptr;
+    size_t grad_cap = 0;
 };
 
 namespace {
@@ -1954,7 +2061,7 @@ template <typename T>
 int vqe_energy(rq_vqe_batch* b, uint64_t ncirc, uint64_t circ0) {
     using V = typename C2<T>::t;
     const uint32_t n = b->n;
-    const uint32_t M = std::min<uint32_t>(n, 13);
+    const uint32_t M = b->em;
     const uint32_t ntile = 1u << (n - M);
     const uint32_t threads = 512;
     const size_t smem = 2 * ((size_t)1 << M) * sizeof(V) + (size_t)(threads / 32) * b->nterms * sizeof(double);
@@ -2004,6 +2111,51 @@ int vqe_wave(rq_vqe_batch* b, uint64_t ncirc, uint64_t circ0) {
     return vqe_energy<T>(b, ncirc, circ0);
 }
 
+// exact gradients of a wave whose final states vqe_wave left in d_states: lambda = H psi,
+// then both states run backwards through the adjoint program; every Ry adds
+// Im <lambda|Y_q|psi> to its parameter's entry of d_grad (zeroed by the caller)
+template <typename T>
+int vqe_adjoint(rq_vqe_batch* b, uint64_t ncirc, uint64_t circ0) {
+    using V = typename C2<T>::t;
+    constexpr int RBc = std::is_same<T, float>::value ? 4 : 3;
+    const int sms = rq::num_sms(b->device);
+    const uint64_t amps = ncirc << b->n;
+    const unsigned hgrid = (unsigned)std::min<uint64_t>((amps + 255) / 256, (uint64_t)sms * 8);
+    k_vqe_apply_h<T><<<hgrid, 256, 0, b->stream>>>((const V*)b->d_states, (V*)b->d_lam, b->n, ncirc, b->d_hterms,
+                                                   b->nhterms);
+    RQ_CUDA(cudaGetLastError());
+    QArgs<T> a{};
+    a.amps = (V*)b->d_states;
+    a.lam = (V*)b->d_lam;
+    a.ncirc = ncirc;
+    a.ntiles = b->antiles;
+    a.circ0 = circ0;
+    a.rot = (const T*)b->d_rot;
+    a.nparam = b->P;
+    a.gpart = b->d_gpart;
+    a.gwidth = b->P;
+    const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(b->aprog);
+    const SwOp* op = reinterpret_cast<const SwOp*>(b->aprog + b->aoff_ops);
+    auto kern = k_batch_adjoint<T, RBc>;
+    const unsigned threads = 1u << (b->am - RBc);
+    const unsigned ngroup = threads < 32 ? threads : threads / 32;
+    const size_t smem = 2 * ((size_t)1 << b->am) * sizeof(V) + (size_t)ngroup * b->P * sizeof(double);
+    if (smem > 227 * 1024) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "too many parameters for the adjoint kernel");
+    RQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    RQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)threads, smem));
+    if (per_sm < 1) return rq::fail(RQ_ERR_CUDA, "adjoint sweep kernel does not fit on an SM");
+    const unsigned grid = (unsigned)std::min<uint64_t>(ncirc * b->antiles, (uint64_t)sms * per_sm);
+    for (const auto& d : b->adescs) {
+        kern<<<grid, threads, smem, b->stream>>>(d, ph, op, a);
+        RQ_CUDA(cudaGetLastError());
+        k_grad_finalize<<<rq::grid_for(ncirc * b->P, TPB, sms), TPB, 0, b->stream>>>(b->d_gpart, ncirc, b->antiles,
+                                                                                   b->P, circ0, b->d_grad);
+        RQ_CUDA(cudaGetLastError());
+    }
+    return RQ_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2025,6 +2177,7 @@ int rq_vqe_batch_create(uint32_t num_qubits, uint32_t depth, const double* coeff
     cudaGetDevice(&b->device);
     // Hamiltonian in mask form, grouped by X/Y pattern, chunks of <= 8 terms
     std::map<uint64_t, std::vector<std::pair<uint64_t, std::pair<uint32_t, double>>>> by_x;   // x -> (pmask, (ny, coeff))
+    std::vector<HTerm> hterms;
     for (uint32_t k = 0; k < nterms; ++k) {
         if (offsets[k + 1] < offsets[k]) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing");
         uint64_t x = 0, pm = 0;
@@ -2040,9 +2193,20 @@ int rq_vqe_batch_create(uint32_t num_qubits, uint32_t depth, const double* coeff
             if (o == RQ_PAULI_Y) ++ny;
         }
         by_x[x].push_back({pm, {ny & 3u, coeffs[k]}});
+        // the adjoint pass applies the Hermitian part of H; a string whose operator
+        // i^ny X^x Z^pm is anti-Hermitian (a qubit repeated within the string) has no
+        // real expectation and drops out
+        if (((ny + (uint32_t)__builtin_popcountll(x & pm)) & 1u) == 0) {
+            const double cf = coeffs[k];
+            const uint32_t r = ny & 3u;
+            HTerm h{x, pm, r == 0 ? cf : (r == 2 ? -cf : 0.0), r == 1 ? cf : (r == 3 ? -cf : 0.0)};
+            hterms.push_back(h);
+        }
     }
     auto re_ip = [](uint32_t k) { k &= 3u; return k == 0 ? 1.0 : (k == 2 ? -1.0 : 0.0); };
-    const uint32_t Mt = std::min<uint32_t>(num_qubits, 13);
+    // energy tiles: two tiles (own + partner) in shared memory, 2^13 f32 / 2^12 f64 amplitudes each
+    const uint32_t Mt = std::min<uint32_t>(num_qubits, precision == RQ_F32 ? 13 : 12);
+    b->em = Mt;
     const uint32_t ntile = 1u << (num_qubits - Mt);
     std::vector<VGroup> groups;
     std::vector<VTerm> terms;
@@ -2120,6 +2284,46 @@ int rq_vqe_batch_create(uint32_t num_qubits, uint32_t depth, const double* coeff
     std::memcpy(host.data() + b->off_ops, opsv.data(), opsv.size() * sizeof(SwOp));
     RQ_CUDA(cudaMalloc((void**)&b->prog, total));
     RQ_CUDA(cudaMemcpy(b->prog, host.data(), total, cudaMemcpyHostToDevice));
+    {
+        // the adjoint program: per layer in reverse, the CZ ladder, then Ry^-1 on every qubit
+        b->nhterms = (uint32_t)hterms.size();
+        if (hterms.empty()) hterms.push_back(HTerm{});
+        RQ_CUDA(cudaMalloc((void**)&b->d_hterms, hterms.size() * sizeof(HTerm)));
+        RQ_CUDA(cudaMemcpy(b->d_hterms, hterms.data(), hterms.size() * sizeof(HTerm), cudaMemcpyHostToDevice));
+        const uint32_t arb = precision == RQ_F32 ? 4 : 3;
+        b->am = std::min(num_qubits, precision == RQ_F32 ? 13u : 12u);
+        b->antiles = 1ull << (num_qubits - b->am);
+        const uint32_t ac = std::min<uint32_t>(b->am, 5);
+        std::vector<PGate> ga;
+        for (uint32_t l = depth; l-- > 0;) {
+            for (uint32_t q = num_qubits - 1; q-- > 0;) {
+                PGate z{};
+                z.type = OP_CZ;
+                z.q0 = q;
+                z.q1 = q + 1;
+                ga.push_back(z);
+            }
+            for (uint32_t q = num_qubits; q-- > 0;) {
+                PGate r{};
+                r.type = OP_RYP;
+                r.q0 = q;
+                r.param = (uint16_t)(l * num_qubits + q);
+                ga.push_back(r);
+            }
+        }
+        auto asw = plan_sweeps(ga, num_qubits, b->am, ac);
+        std::vector<PhaseDesc> aph;
+        std::vector<SwOp> aops;
+        std::vector<double> amats;
+        build_program(asw, num_qubits, b->am, ac, arb, precision == RQ_F32 ? 2 : 1, b->adescs, aph, aops, amats);
+        b->aoff_ops = (aph.size() * sizeof(PhaseDesc) + 255) & ~size_t(255);
+        const size_t atotal = b->aoff_ops + aops.size() * sizeof(SwOp);
+        std::vector<unsigned char> ah(atotal);
+        std::memcpy(ah.data(), aph.data(), aph.size() * sizeof(PhaseDesc));
+        std::memcpy(ah.data() + b->aoff_ops, aops.data(), aops.size() * sizeof(SwOp));
+        RQ_CUDA(cudaMalloc((void**)&b->aprog, atotal));
+        RQ_CUDA(cudaMemcpy(b->aprog, ah.data(), atotal, cudaMemcpyHostToDevice));
+    }
     RQ_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     RQ_CUDA(cudaEventCreate(&b->ev0));
     RQ_CUDA(cudaEventCreate(&b->ev1));
@@ -2132,9 +2336,12 @@ int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* params, int3
     if (!b || !params || !energies || (with_gradient && !gradients))
         return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
     if (nsets == 0) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "nsets must be >= 1");
+    if (with_gradient < RQ_VQE_GRAD_NONE || with_gradient > RQ_VQE_GRAD_ADJOINT)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "with_gradient must be RQ_VQE_GRAD_NONE, _SHIFT or _ADJOINT");
     RQ_CUDA(cudaSetDevice(b->device));
     const uint32_t P = b->P;
-    const uint32_t V = with_gradient ? 1 + 2 * P : 1;
+    const bool adj = with_gradient == RQ_VQE_GRAD_ADJOINT;
+    const uint32_t V = with_gradient == RQ_VQE_GRAD_SHIFT ? 1 + 2 * P : 1;
     const uint64_t ncirc = (uint64_t)nsets * V;
     const size_t es = b->prec == RQ_F32 ? sizeof(float) : sizeof(double);
     RQ_TRY(grow(&b->d_params, &b->params_cap, (size_t)nsets * P));
@@ -2143,6 +2350,12 @@ int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* params, int3
     const size_t state_bytes = ((size_t)1 << b->n) * elem_size(b->prec);
     const uint64_t wave = std::max<uint64_t>(1, std::min<uint64_t>(ncirc, b->wave_bytes / state_bytes));
     RQ_TRY(grow_bytes(&b->d_states, &b->states_cap, wave * state_bytes));
+    if (adj) {
+        RQ_TRY(grow_bytes(&b->d_lam, &b->lam_cap, wave * state_bytes));
+        RQ_TRY(grow(&b->d_gpart, &b->gpart_cap, wave * b->antiles * P));
+        RQ_TRY(grow(&b->d_grad, &b->grad_cap, (size_t)nsets * P));
+        RQ_CUDA(cudaMemsetAsync(b->d_grad, 0, (size_t)nsets * P * sizeof(double), b->stream));
+    }
     RQ_CUDA(cudaMemcpyAsync(b->d_params, params, (size_t)nsets * P * sizeof(double), cudaMemcpyHostToDevice, b->stream));
     const int sms = rq::num_sms(b->device);
     RQ_CUDA(cudaEventRecord(b->ev0, b->stream));
@@ -2153,17 +2366,25 @@ int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* params, int3
     RQ_CUDA(cudaGetLastError());
     for (uint64_t w0 = 0; w0 < ncirc; w0 += wave) {
         const uint64_t wn = std::min<uint64_t>(wave, ncirc - w0);
-        if (b->prec == RQ_F32) RQ_TRY(vqe_wave<float>(b, wn, w0));
-        else RQ_TRY(vqe_wave<double>(b, wn, w0));
+        if (b->prec == RQ_F32) {
+            RQ_TRY(vqe_wave<float>(b, wn, w0));
+            if (adj) RQ_TRY(vqe_adjoint<float>(b, wn, w0));
+        } else {
+            RQ_TRY(vqe_wave<double>(b, wn, w0));
+            if (adj) RQ_TRY(vqe_adjoint<double>(b, wn, w0));
+        }
     }
     RQ_CUDA(cudaEventRecord(b->ev1, b->stream));
     std::vector<double> e(ncirc);
     RQ_CUDA(cudaMemcpyAsync(e.data(), b->d_energy, ncirc * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    if (adj)
+        RQ_CUDA(cudaMemcpyAsync(gradients, b->d_grad, (size_t)nsets * P * sizeof(double), cudaMemcpyDeviceToHost,
+                                b->stream));
     RQ_CUDA(cudaStreamSynchronize(b->stream));
     RQ_CUDA(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
     for (uint32_t s = 0; s < nsets; ++s) {
         energies[s] = e[(uint64_t)s * V];
-        if (with_gradient)
+        if (with_gradient == RQ_VQE_GRAD_SHIFT)
             for (uint32_t k = 0; k < P; ++k)
                 gradients[(uint64_t)s * P + k] = (e[(uint64_t)s * V + 1 + 2 * k] - e[(uint64_t)s * V + 2 + 2 * k]) / 2.0;
     }
@@ -2180,8 +2401,8 @@ int rq_vqe_batch_destroy(rq_vqe_batch* b) {
     if (!b) return RQ_OK;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
-    void* ptrs[] = {b->prog, b->d_groups, b->d_terms, b->d_gofs, b->d_part, b->d_params, b->d_rot, b->d_states,
-                    b->d_energy};
+    void* ptrs[] = {b->prog,     b->d_groups, b->d_terms, b->d_gofs,  b->d_part, b->d_params, b->d_rot,
+                    b->d_states, b->d_energy, b->aprog,   b->d_hterms, b->d_lam,  b->d_gpart,  b->d_grad};
     for (void* q : ptrs) if (q) cudaFree(q);
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);

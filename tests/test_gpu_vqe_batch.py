@@ -63,3 +63,15 @@ def test_vqe_batch_config_shape_16q():
     pm[k] -= math.pi / 2
     want = (_energy(n, depth, pp, coeffs, strings) - _energy(n, depth, pm, coeffs, strings)) / 2
     assert abs(g[0, k] - want) < 1e-5 * scale
+
+
+def test_vqe_batch_f64_two_energy_tiles():
+    """f64 states above 12 qubits: the energy kernel pairs 2^12-amplitude tiles."""
+    n, depth = 14, 2
+    coeffs, strings = workloads.pauli_hamiltonian(n, 12, 8)
+    params = workloads.vqe_parameter_sets(2, n * depth, 9)
+    vb = VqeBatch(n, depth, coeffs, strings, "f64")
+    e = vb.run(params)
+    for s in range(2):
+        want = _energy(n, depth, params[s], coeffs, strings)
+        assert abs(e[s] - want) < 1e-10, (e[s], want)
