@@ -202,6 +202,25 @@ RQ_API int rq_state_apply_mode(rq_state* s, const rq_gate* gates, uint64_t n,
                         int32_t mode, rq_measurement* out, uint64_t cap,
                         uint64_t* nout);
 
+/* NoiseModel (types.rs:249-263). */
+typedef struct rq_noise_model {
+    double depolarizing_rate;
+    double bit_flip_rate;
+    double phase_flip_rate;
+} rq_noise_model;
+
+/* rq_state_apply with a noise model: the gate loop of Simulator::run_with_config
+ * when config.noise is set (simulator.rs:67-78).  After every gate with qubits
+ * (Measure and Reset included, Barrier not), each of its qubits in order draws
+ * from the state's measurement stream as apply_noise does (simulator.rs:177-221):
+ * a depolarising draw r (< rate: a second draw picks X / Y / Z by thirds), a
+ * bit-flip draw (< rate: X), a phase-flip draw (< rate: Z); a channel whose rate
+ * is 0 draws nothing.  Measurements keep their place in the same stream.  The
+ * chosen Paulis are applied on the device with the rest of the list. */
+RQ_API int rq_state_apply_noisy(rq_state* s, const rq_gate* gates, uint64_t n,
+                                const rq_noise_model* noise, rq_measurement* out, uint64_t cap,
+                                uint64_t* nout);
+
 /* apply_single_qubit_gate (state.rs:214-229): m = 8 doubles, (re,im) pairs. */
 RQ_API int rq_state_apply_1q_matrix(rq_state* s, uint32_t qubit, const double* m);
 

@@ -63,6 +63,7 @@ def _load() -> C.CDLL:
         "orc_state_from_amplitudes": (i32, [P(dbl), u64, u32, i32, u64, P(vp)]),
         "orc_state_free": (None, [vp]),
         "orc_apply": (i32, [vp, P(Gate), u64, P(Measurement), u64, P(u64), i32]),
+        "orc_apply_noisy": (i32, [vp, P(Gate), u64, P(C.c_double), P(Measurement), u64, P(u64)]),
         "orc_apply_1q_matrix": (i32, [vp, u32, P(dbl)]),
         "orc_apply_2q_matrix": (i32, [vp, u32, u32, P(dbl)]),
         "orc_measure": (i32, [vp, u32, P(Measurement)]),
@@ -192,6 +193,15 @@ class OracleState:
         out = (Measurement * (len(gates) + 1))()
         nout = C.c_uint64()
         _check(lib().orc_apply(self._h, arr, len(gates), out, len(gates) + 1, C.byref(nout), 1 if parallel else 0))
+        return [(out[k].qubit, bool(out[k].result), out[k].probability) for k in range(nout.value)]
+
+    def apply_noisy(self, gates, rates):
+        """run_with_config's gate loop with NoiseModel rates (depolarizing, bit_flip, phase_flip)."""
+        arr = gate_array(gates)
+        r = np.ascontiguousarray(rates, dtype=np.float64)
+        out = (Measurement * (len(gates) + 1))()
+        nout = C.c_uint64()
+        _check(lib().orc_apply_noisy(self._h, arr, len(gates), _dp(r), out, len(gates) + 1, C.byref(nout)))
         return [(out[k].qubit, bool(out[k].result), out[k].probability) for k in range(nout.value)]
 
     def apply_1q_matrix(self, q, m8):

@@ -519,6 +519,58 @@ int orc_apply(void* h, const rq_gate* gates, uint64_t n, rq_measurement* out, ui
     return RQ_OK;
 }
 
+// Simulator::run_with_config's gate loop with a noise model (simulator.rs:67-78):
+// every gate, then apply_noise (simulator.rs:177-221) for each qubit of Gate::qubits()
+// (gate.rs:40-63; empty for Barrier): depolarising draw (+ the X/Y/Z choice by
+// thirds), bit-flip draw, phase-flip draw, each only when its rate is > 0; the
+// Paulis go through apply_single_qubit_gate with Gate::matrix_1q.  Draws come from
+// the state's stream (the same one measurements use).
+int orc_apply_noisy(void* h, const rq_gate* gates, uint64_t n, const double* rates, rq_measurement* out,
+                    uint64_t cap, uint64_t* nout) {
+    StateBase* s = (StateBase*)h;
+    std::vector<rq_measurement> outs;
+    const double dep = rates[0], bf = rates[1], pf = rates[2];
+    auto pauli = [&](int kind, uint32_t q) {
+        rq_gate p{};
+        p.kind = kind;
+        p.q0 = q;
+        M2 m;
+        matrix_1q(p, m);
+        if (auto d = as<double>(s)) d->apply_1q(q, m); else as<float>(s)->apply_1q(q, m);
+    };
+    for (uint64_t k = 0; k < n; ++k) {
+        const rq_gate& g = gates[k];
+        int rc;
+        if (auto d = as<double>(s)) rc = apply_gate_impl(d, g, &outs, false);
+        else rc = apply_gate_impl(as<float>(s), g, &outs, false);
+        if (rc) return rc;
+        if (g.kind == RQ_GATE_BARRIER) continue;
+        const uint32_t qs[2] = {g.q0, g.q1};
+        const int nq = is_2q(g.kind) ? 2 : 1;
+        for (int j = 0; j < nq; ++j) {
+            const uint32_t q = qs[j];
+            if (dep > 0.0) {
+                const double r = s->next_uniform();
+                if (r < dep) {
+                    const double c = s->next_uniform();
+                    pauli(c < 1.0 / 3.0 ? RQ_GATE_X : (c < 2.0 / 3.0 ? RQ_GATE_Y : RQ_GATE_Z), q);
+                }
+            }
+            if (bf > 0.0) {
+                const double r = s->next_uniform();
+                if (r < bf) pauli(RQ_GATE_X, q);
+            }
+            if (pf > 0.0) {
+                const double r = s->next_uniform();
+                if (r < pf) pauli(RQ_GATE_Z, q);
+            }
+        }
+    }
+    if (nout) *nout = outs.size();
+    for (size_t k = 0; k < outs.size() && k < cap; ++k) out[k] = outs[k];
+    return RQ_OK;
+}
+
 int orc_apply_1q_matrix(void* h, uint32_t q, const double* m8) {
     StateBase* s = (StateBase*)h;
     if (q >= s->nq) return RQ_ERR_INVALID_QUBIT_INDEX;

@@ -15,11 +15,12 @@ from .error import (CircuitError, CudaError, DeviceTimeout, InvalidArgument, Inv
 from .gate import Gate, GateKind
 from .simulator import ShotResult, SimConfig, SimulationResult, Simulator
 from .state import MAX_QUBITS, MAX_QUBITS_F32, Plan, QuantumState, set_device
-from .types import Hamiltonian, MeasurementOutcome, PauliOp, PauliString, SimulationMetrics
+from .types import Hamiltonian, MeasurementOutcome, NoiseModel, PauliOp, PauliString, SimulationMetrics
 
 __all__ = [
     "QuantumState", "Plan", "set_device", "QuantumCircuit", "Gate", "GateKind", "Simulator", "SimConfig", "SimulationResult",
     "ShotResult", "PauliOp", "PauliString", "Hamiltonian", "MeasurementOutcome", "SimulationMetrics",
+    "NoiseModel",
     "QuantumError", "QubitLimitExceeded", "InvalidQubitIndex", "MemoryAllocationFailed", "InvalidStateVector",
     "CircuitError", "CudaError", "DeviceTimeout", "InvalidArgument", "MAX_QUBITS", "MAX_QUBITS_F32",
     "RQ_F32", "RQ_F64", "RQ_EXEC_AUTO", "RQ_EXEC_PER_GATE", "RQ_EXEC_SWEEP", "RQ_EXEC_SWEEP_TC",

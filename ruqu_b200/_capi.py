@@ -29,6 +29,10 @@ class RqMeasurement(C.Structure):
     _fields_ = [("qubit", C.c_uint32), ("result", C.c_int32), ("probability", C.c_double)]
 
 
+class RqNoiseModel(C.Structure):
+    _fields_ = [("depolarizing_rate", C.c_double), ("bit_flip_rate", C.c_double), ("phase_flip_rate", C.c_double)]
+
+
 class RqPauliOp(C.Structure):
     _fields_ = [("qubit", C.c_uint32), ("op", C.c_int32)]
 
@@ -61,6 +65,7 @@ SIGNATURES = {
     "rq_state_synchronize": (C.c_int, [_vp]),
     "rq_state_apply": (C.c_int, [_vp, _P(RqGate), _u64, _P(RqMeasurement), _u64, _P(_u64)]),
     "rq_state_apply_mode": (C.c_int, [_vp, _P(RqGate), _u64, _i32, _P(RqMeasurement), _u64, _P(_u64)]),
+    "rq_state_apply_noisy": (C.c_int, [_vp, _P(RqGate), _u64, _P(RqNoiseModel), _P(RqMeasurement), _u64, _P(_u64)]),
     "rq_state_apply_1q_matrix": (C.c_int, [_vp, _u32, _P(_dbl)]),
     "rq_state_apply_2q_matrix": (C.c_int, [_vp, _u32, _u32, _P(_dbl)]),
     "rq_state_measure": (C.c_int, [_vp, _u32, _P(RqMeasurement)]),

@@ -431,21 +431,26 @@ int rq_state_synchronize(rq_state* s) {
     return RQ_OK;
 }
 
-int rq_state_apply_mode(rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_measurement* out,
-                        uint64_t cap, uint64_t* nout) {
-    if (!s || (!gates && n)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
-    if (mode < RQ_EXEC_AUTO || mode > RQ_EXEC_SWEEP_TC_FAST)
-        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "bad execution mode");
-    RQ_TRY(set_device(s));
-    for (uint64_t k = 0; k < n; ++k) RQ_TRY(validate_gate(s, gates[k]));
+}  // extern "C"
+
+namespace {
+
+// The gate loop of run_with_config (simulator.rs:67-78) over a validated list:
+// measurements and resets in order, every maximal run of unitary gates through the
+// sweep path (or per-gate kernels).  With mdraw, the k-th measurement / reset of the
+// list takes draw index mdraw[k] of the state's stream (noise draws interleave).
+int run_gate_list(rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_measurement* out, uint64_t cap,
+                  uint64_t* nout, const uint64_t* mdraw) {
     // states below 7 qubits are smaller than one sweep tile: per-gate kernels
     int use_sweep = (mode != RQ_EXEC_PER_GATE && (mode != RQ_EXEC_AUTO || s->nq >= 12)) && s->nq >= 7;
-    uint64_t nm = 0;
+    uint64_t nm = 0, nmr = 0;
     uint64_t k = 0;
     while (k < n) {
         const rq_gate& g = gates[k];
         if (g.kind == RQ_GATE_BARRIER) { ++k; continue; }
         if (g.kind == RQ_GATE_MEASURE || g.kind == RQ_GATE_RESET) {
+            if (mdraw) s->draws = mdraw[nmr];
+            ++nmr;
             rq_measurement m;
             if (g.kind == RQ_GATE_MEASURE) {
                 RQ_TRY(do_measure(s, g.q0, &m));
@@ -477,6 +482,66 @@ int rq_state_apply_mode(rq_state* s, const rq_gate* gates, uint64_t n, int32_t m
     }
     if (nout) *nout = nm;
     return RQ_OK;
+}
+
+rq_gate pauli_gate(int kind, uint32_t q) {
+    rq_gate p{};
+    p.kind = kind;
+    p.q0 = q;
+    return p;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rq_state_apply_mode(rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_measurement* out,
+                        uint64_t cap, uint64_t* nout) {
+    if (!s || (!gates && n)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (mode < RQ_EXEC_AUTO || mode > RQ_EXEC_SWEEP_TC_FAST)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "bad execution mode");
+    RQ_TRY(set_device(s));
+    for (uint64_t k = 0; k < n; ++k) RQ_TRY(validate_gate(s, gates[k]));
+    return run_gate_list(s, gates, n, mode, out, cap, nout, nullptr);
+}
+
+int rq_state_apply_noisy(rq_state* s, const rq_gate* gates, uint64_t n, const rq_noise_model* noise,
+                         rq_measurement* out, uint64_t cap, uint64_t* nout) {
+    if (!s || (!gates && n) || !noise) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    RQ_TRY(set_device(s));
+    for (uint64_t k = 0; k < n; ++k) RQ_TRY(validate_gate(s, gates[k]));
+    // The noise decisions depend on the stream only, not on the state: walk the list once
+    // on the host, drawing in apply_noise's order (simulator.rs:177-221) -- per qubit of
+    // each gate: depolarising r (and the Pauli choice when r < rate), bit-flip r, phase-flip
+    // r -- with each measurement / reset keeping its own draw in between, and insert the
+    // chosen Paulis after their gate.  The expanded list then runs on the device.
+    const double dep = noise->depolarizing_rate, bf = noise->bit_flip_rate, pf = noise->phase_flip_rate;
+    std::vector<rq_gate> ex;
+    ex.reserve(n + n / 4);
+    std::vector<uint64_t> mdraw;
+    uint64_t d = s->draws;
+    for (uint64_t k = 0; k < n; ++k) {
+        const rq_gate& g = gates[k];
+        if (g.kind == RQ_GATE_BARRIER) continue;   // Gate::qubits() is empty: no noise
+        ex.push_back(g);
+        if (g.kind == RQ_GATE_MEASURE || g.kind == RQ_GATE_RESET) mdraw.push_back(d++);
+        const uint32_t qs[2] = {g.q0, g.q1};
+        const int nq = is_2q(g.kind) ? 2 : 1;
+        for (int j = 0; j < nq; ++j) {
+            const uint32_t q = qs[j];
+            if (dep > 0.0) {
+                if (rqd::uniform(s->seed, 0, d++) < dep) {
+                    const double c = rqd::uniform(s->seed, 0, d++);
+                    ex.push_back(pauli_gate(c < 1.0 / 3.0 ? RQ_GATE_X : (c < 2.0 / 3.0 ? RQ_GATE_Y : RQ_GATE_Z), q));
+                }
+            }
+            if (bf > 0.0 && rqd::uniform(s->seed, 0, d++) < bf) ex.push_back(pauli_gate(RQ_GATE_X, q));
+            if (pf > 0.0 && rqd::uniform(s->seed, 0, d++) < pf) ex.push_back(pauli_gate(RQ_GATE_Z, q));
+        }
+    }
+    const int rc = run_gate_list(s, ex.data(), ex.size(), s->exec_mode, out, cap, nout, mdraw.data());
+    if (rc == RQ_OK) s->draws = d;
+    return rc;
 }
 
 int rq_state_apply(rq_state* s, const rq_gate* gates, uint64_t n, rq_measurement* out, uint64_t cap,

@@ -49,12 +49,16 @@ class Simulator:
 
     @staticmethod
     def run_with_config(circuit: QuantumCircuit, config: SimConfig) -> SimulationResult:
-        """simulator.rs:56-101: fresh |0...0>, every gate in order, metrics."""
-        if config.noise is not None:
-            raise NotImplementedError("noise channels are not part of the GPU state-vector path")
+        """simulator.rs:56-101: fresh |0...0>, every gate in order, metrics; with
+        config.noise (a NoiseModel) the Pauli noise of apply_noise after every gate."""
         t0 = time.perf_counter_ns()
         state = QuantumState(circuit.num_qubits(), config.seed, config.precision)
-        meas = state.apply_gates(circuit.packed()) if circuit.gate_count() else []
+        if not circuit.gate_count():
+            meas = []
+        elif config.noise is not None:
+            meas = state.apply_gates_noisy(circuit.packed(), config.noise)
+        else:
+            meas = state.apply_gates(circuit.packed())
         state.synchronize()
         ns = time.perf_counter_ns() - t0
         unitary = sum(1 for g in circuit.gates() if not g.is_non_unitary())

@@ -168,6 +168,20 @@ class QuantumState:
         self._record.extend(res)
         return res
 
+    def apply_gates_noisy(self, gates, noise) -> list:
+        """The gates with per-gate Pauli noise drawn from this state's stream, as
+        Simulator::run_with_config applies a NoiseModel (simulator.rs:67-78, 177-221)."""
+        arr = gates if isinstance(gates, C.Array) else gates_to_array(gates)
+        n = len(gates)
+        nm = _capi.RqNoiseModel(float(noise.depolarizing_rate), float(noise.bit_flip_rate),
+                                float(noise.phase_flip_rate))
+        out = (RqMeasurement * max(1, n))()
+        nout = C.c_uint64()
+        check(lib.rq_state_apply_noisy(self._h, arr, n, C.byref(nm), out, n, C.byref(nout)))
+        res = [MeasurementOutcome(out[k].qubit, bool(out[k].result), out[k].probability) for k in range(nout.value)]
+        self._record.extend(res)
+        return res
+
     def apply_single_qubit_gate(self, qubit: int, matrix) -> None:
         m = np.ascontiguousarray(np.asarray(matrix, dtype=np.complex128).reshape(2, 2)).view(np.float64)
         check(lib.rq_state_apply_1q_matrix(self._h, int(qubit), _dp(m)))

@@ -56,3 +56,12 @@ class SimulationMetrics:
     peak_memory_bytes: int = 0
     gates_per_second: float = 0.0
     gates_fused: int = 0
+
+
+@dataclass
+class NoiseModel:
+    """types.rs:249-263: per-gate stochastic Pauli noise for Simulator.run_with_config."""
+
+    depolarizing_rate: float = 0.0
+    bit_flip_rate: float = 0.0
+    phase_flip_rate: float = 0.0
