@@ -313,6 +313,18 @@ RQ_API int rq_state_norm_sq(rq_state* s, double* out);
 RQ_API int rq_state_normalize(rq_state* s);                         /* state.rs:415-423 */
 RQ_API int rq_state_fidelity(rq_state* a, rq_state* b, double* out); /* state.rs:426-435 */
 
+/* The host amplitude edits of run_grover (grover.rs:128-153, through
+ * amplitudes_mut) as device passes, so the state stays on the device.
+ * rq_state_negate_amplitudes: amps[i] = -amps[i] for every listed index (the
+ * oracle step, grover.rs:128-139); an index listed twice is negated twice, as
+ * the reference's loop does; an index >= 2^n is rejected (run_grover asserts,
+ * grover.rs:103-111) and nothing changes.
+ * rq_state_negate_all_except: amps[i] = -amps[i] for every i != keep (the
+ * diffuser's 2|0><0| - I between the Hadamard layers with keep = 0,
+ * grover.rs:144-153).  No reference counterpart as functions. */
+RQ_API int rq_state_negate_amplitudes(rq_state* s, const uint64_t* indices, uint64_t count);
+RQ_API int rq_state_negate_all_except(rq_state* s, uint64_t keep);
+
 /* ------------------------------------------------------------------------ */
 /* batched QAOA-MaxCut (qaoa.rs:125-201 over many graphs / parameter sets)    */
 /* ------------------------------------------------------------------------ */

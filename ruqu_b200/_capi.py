@@ -66,6 +66,8 @@ SIGNATURES = {
     "rq_state_apply": (C.c_int, [_vp, _P(RqGate), _u64, _P(RqMeasurement), _u64, _P(_u64)]),
     "rq_state_apply_mode": (C.c_int, [_vp, _P(RqGate), _u64, _i32, _P(RqMeasurement), _u64, _P(_u64)]),
     "rq_state_apply_noisy": (C.c_int, [_vp, _P(RqGate), _u64, _P(RqNoiseModel), _P(RqMeasurement), _u64, _P(_u64)]),
+    "rq_state_negate_amplitudes": (C.c_int, [_vp, _P(_u64), _u64]),
+    "rq_state_negate_all_except": (C.c_int, [_vp, _u64]),
     "rq_state_apply_1q_matrix": (C.c_int, [_vp, _u32, _P(_dbl)]),
     "rq_state_apply_2q_matrix": (C.c_int, [_vp, _u32, _u32, _P(_dbl)]),
     "rq_state_measure": (C.c_int, [_vp, _u32, _P(RqMeasurement)]),

@@ -8,6 +8,8 @@
 // rq_sample.cu and rq_sweep.cu; nothing here computes on amplitudes.
 #include "rq_internal.cuh"
 
+#include <algorithm>
+
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -671,6 +673,39 @@ int rq_state_normalize(rq_state* s) {
     RQ_TRY(rq_state_norm_sq(s, &ns));
     if (ns > 0.0) RQ_TRY(rq::scale_all(s, 1.0 / std::sqrt(ns)));
     return RQ_OK;
+}
+
+int rq_state_negate_amplitudes(rq_state* s, const uint64_t* indices, uint64_t count) {
+    if (!s || (!indices && count)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    std::vector<uint64_t> v(indices, indices + count);
+    for (uint64_t i : v)
+        if (i >= s->n)
+            return rq::fail(RQ_ERR_INVALID_ARGUMENT, "amplitude index " + std::to_string(i) + " out of range for " +
+                                                         std::to_string(s->nq) + " qubits");
+    // an index listed k times is negated k times: keep those with k odd, once each
+    std::sort(v.begin(), v.end());
+    std::vector<uint64_t> odd;
+    for (size_t a = 0; a < v.size();) {
+        size_t b = a;
+        while (b < v.size() && v[b] == v[a]) ++b;
+        if ((b - a) & 1) odd.push_back(v[a]);
+        a = b;
+    }
+    if (odd.empty()) return RQ_OK;
+    RQ_TRY(set_device(s));
+    RQ_TRY(rq::ensure_partials(s, odd.size()));
+    uint64_t* d_idx = reinterpret_cast<uint64_t*>(s->partials);
+    RQ_CUDA(cudaMemcpyAsync(d_idx, odd.data(), odd.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream));
+    RQ_TRY(rq::negate_list(s, d_idx, odd.size()));
+    // the host list goes out of scope on return: finish the copy first
+    RQ_CUDA(cudaStreamSynchronize(s->stream));
+    return RQ_OK;
+}
+
+int rq_state_negate_all_except(rq_state* s, uint64_t keep) {
+    if (!s) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null state");
+    RQ_TRY(set_device(s));
+    return rq::negate_except(s, keep);
 }
 
 int rq_state_fidelity(rq_state* a, rq_state* b, double* out) {

@@ -205,6 +205,32 @@ __global__ void k_to_f64(const typename C2<T>::t* __restrict__ a, double2* __res
     }
 }
 
+// host amplitude edits of run_grover (grover.rs:128-153) as device passes
+template <typename T>
+__global__ void k_negate_except(typename C2<T>::t* __restrict__ a, uint64_t n, uint64_t keep) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        if (i == keep) continue;
+        auto x = a[i];
+        x.x = -x.x;
+        x.y = -x.y;
+        a[i] = x;
+    }
+}
+
+// distinct indices (the host folds repeats), so no two threads touch one amplitude
+template <typename T>
+__global__ void k_negate_list(typename C2<T>::t* __restrict__ a, const uint64_t* __restrict__ idx, uint64_t count) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < count;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = idx[k];
+        auto x = a[i];
+        x.x = -x.x;
+        x.y = -x.y;
+        a[i] = x;
+    }
+}
+
 template <typename T>
 __global__ void k_basis(typename C2<T>::t* __restrict__ a, uint64_t n, uint64_t index) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -309,6 +335,19 @@ int gate_cz(rq_state* s, uint32_t q1, uint32_t q2) {
     uint64_t ng = s->n >> 2;
     if (s->prec == RQ_F32) RQ_LAUNCH(k_cz<float>, ng, (float2*)s->amps, ng, q1, q2);
     else RQ_LAUNCH(k_cz<double>, ng, (double2*)s->amps, ng, q1, q2);
+    return RQ_OK;
+}
+
+int negate_except(rq_state* s, uint64_t keep) {
+    if (s->prec == RQ_F32) RQ_LAUNCH(k_negate_except<float>, s->n, (float2*)s->amps, s->n, keep);
+    else RQ_LAUNCH(k_negate_except<double>, s->n, (double2*)s->amps, s->n, keep);
+    return RQ_OK;
+}
+
+int negate_list(rq_state* s, const uint64_t* dev_idx, uint64_t count) {
+    if (count == 0) return RQ_OK;
+    if (s->prec == RQ_F32) RQ_LAUNCH(k_negate_list<float>, count, (float2*)s->amps, dev_idx, count);
+    else RQ_LAUNCH(k_negate_list<double>, count, (double2*)s->amps, dev_idx, count);
     return RQ_OK;
 }
 

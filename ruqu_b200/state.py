@@ -182,6 +182,16 @@ class QuantumState:
         self._record.extend(res)
         return res
 
+    def negate_amplitudes(self, indices) -> None:
+        """amps[i] = -amps[i] for every listed index, on the device (the oracle step that
+        run_grover does through amplitudes_mut, grover.rs:128-139)."""
+        idx = np.ascontiguousarray(np.asarray(indices, dtype=np.uint64).reshape(-1))
+        check(lib.rq_state_negate_amplitudes(self._h, idx.ctypes.data_as(C.POINTER(C.c_uint64)), idx.size))
+
+    def negate_all_except(self, keep: int = 0) -> None:
+        """amps[i] = -amps[i] for every i != keep, on the device (grover.rs:144-153)."""
+        check(lib.rq_state_negate_all_except(self._h, int(keep)))
+
     def apply_single_qubit_gate(self, qubit: int, matrix) -> None:
         m = np.ascontiguousarray(np.asarray(matrix, dtype=np.complex128).reshape(2, 2)).view(np.float64)
         check(lib.rq_state_apply_1q_matrix(self._h, int(qubit), _dp(m)))
