@@ -152,8 +152,10 @@ struct Sweep {
     std::vector<PGate> ops;   // in execution order (after fusion)
 };
 
-inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c,
-                                      bool all_slots = false) {
+// First-come local sets: each sweep admits the qubits of the remaining gates in list
+// order until m are local.
+inline std::vector<Sweep> plan_sweeps_first_come(const std::vector<PGate>& gates, uint32_t n, uint32_t m,
+                                                 uint32_t c) {
     std::vector<Sweep> out;
     std::vector<char> taken(gates.size(), 0);
     size_t first = 0;
@@ -171,9 +173,6 @@ inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t 
                 blocked |= qm;
                 continue;
             }
-            // locality as for CUDA-core sweeps also in tensor-core plans: a gate qubit that
-            // stays outside the sweep's local set is uniform over each tile (see fuse_dense)
-            (void)all_slots;
             uint64_t L2 = sw.L | needs(g, false);
             if ((uint32_t)__builtin_popcountll(L2) > m) {
                 blocked |= qm;
@@ -194,6 +193,121 @@ inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t 
         out.push_back(std::move(sw));
     }
     return out;
+}
+
+// Gates a sweep with the fixed local set L would take from the remaining list (per-qubit
+// order kept: a gate that cannot run holds its qubits back for the rest of the list);
+// marks them in *mark when given.  Stops once every qubit is held back.
+inline int sweep_closure(const std::vector<PGate>& gates, const std::vector<char>& taken, size_t first, uint64_t L,
+                         uint64_t allq, std::vector<char>* mark) {
+    uint64_t blocked = 0;
+    int cnt = 0;
+    for (size_t k = first; k < gates.size(); ++k) {
+        if (taken[k]) continue;
+        const PGate& g = gates[k];
+        const uint64_t qm = qmask(g);
+        if ((qm & blocked) || (needs(g, false) & ~L)) {
+            blocked |= qm;
+            if ((blocked & allq) == allq) break;
+            continue;
+        }
+        ++cnt;
+        if (mark) (*mark)[k] = 1;
+    }
+    return cnt;
+}
+
+// Candidate local sets for the next sweep: the first-come set (padded to m qubits) and
+// every window of m - c consecutive qubits above the always-local low c qubits (the
+// shape that follows nearest-neighbour circuits as their light cones move).
+inline std::vector<uint64_t> sweep_candidates(const std::vector<PGate>& gates, const std::vector<char>& taken,
+                                              size_t first, uint32_t n, uint32_t m, uint32_t c) {
+    const uint64_t base = (c >= 64) ? ~0ull : ((1ull << c) - 1);
+    std::vector<uint64_t> out;
+    uint64_t L = base, blocked = 0;
+    for (size_t k = first; k < gates.size(); ++k) {
+        if (taken[k]) continue;
+        const uint64_t qm = qmask(gates[k]);
+        if (qm & blocked) { blocked |= qm; continue; }
+        const uint64_t L2 = L | needs(gates[k], false);
+        if ((uint32_t)__builtin_popcountll(L2) > m) { blocked |= qm; continue; }
+        L = L2;
+    }
+    for (uint32_t q = 0; q < n && (uint32_t)__builtin_popcountll(L) < m; ++q) L |= 1ull << q;
+    out.push_back(L);
+    const uint32_t w = m > c ? m - c : 0;
+    for (uint32_t a0 = c; w && a0 + w <= n; ++a0) {
+        uint64_t W = base;
+        for (uint32_t q = a0; q < a0 + w; ++q) W |= 1ull << q;
+        if (W != L) out.push_back(W);
+    }
+    return out;
+}
+
+// Lookahead local sets: each sweep takes the candidate set that maximises the gates it
+// runs plus the most the following sweep could then run (two-step lookahead over the
+// candidates of sweep_candidates).
+inline std::vector<Sweep> plan_sweeps_lookahead(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c) {
+    std::vector<Sweep> out;
+    std::vector<char> taken(gates.size(), 0);
+    const uint64_t allq = (n >= 64) ? ~0ull : ((1ull << n) - 1);
+    size_t first = 0;
+    while (first < gates.size()) {
+        const auto cands = sweep_candidates(gates, taken, first, n, m, c);
+        double best = -1.0;
+        uint64_t bestL = cands[0];
+        for (uint64_t L : cands) {
+            std::vector<char> t2 = taken;
+            double score = sweep_closure(gates, taken, first, L, allq, &t2);
+            size_t f2 = first;
+            while (f2 < gates.size() && t2[f2]) ++f2;
+            int next = 0;
+            if (f2 < gates.size())
+                for (uint64_t L2 : sweep_candidates(gates, t2, f2, n, m, c))
+                    next = std::max(next, sweep_closure(gates, t2, f2, L2, allq, nullptr));
+            score += 0.999 * next;   // ties go to the set that runs more gates now
+            if (score > best) {
+                best = score;
+                bestL = L;
+            }
+        }
+        Sweep sw;
+        sw.L = bestL;
+        std::vector<int> last(n, -1);   // index in sw.ops of the last op on each qubit
+        uint64_t blocked = 0;
+        for (size_t k = first; k < gates.size(); ++k) {
+            if (taken[k]) continue;
+            const PGate& g = gates[k];
+            const uint64_t qm = qmask(g);
+            if ((qm & blocked) || (needs(g, false) & ~bestL)) {
+                blocked |= qm;
+                continue;
+            }
+            taken[k] = 1;
+            if (is_1q(g.type) && last[g.q0] >= 0 && is_1q(sw.ops[last[g.q0]].type)) {
+                fuse_into(sw.ops[last[g.q0]], g);
+            } else {
+                sw.ops.push_back(g);
+                const int idx = (int)sw.ops.size() - 1;
+                for (uint32_t q = 0; q < n; ++q)
+                    if ((qm >> q) & 1) last[q] = idx;
+            }
+        }
+        while (first < gates.size() && taken[first]) ++first;
+        out.push_back(std::move(sw));
+    }
+    return out;
+}
+
+// The sweep plan: both planners, keeping the one with fewer sweeps (each sweep is a full
+// read and write of the state); first-come on a tie.  A gate qubit that stays outside a
+// sweep's local set is uniform over each tile, for CUDA-core and tensor-core plans alike.
+inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c,
+                                      bool all_slots = false) {
+    (void)all_slots;
+    auto a = plan_sweeps_first_come(gates, n, m, c);
+    auto b = plan_sweeps_lookahead(gates, n, m, c);
+    return b.size() < a.size() ? b : a;
 }
 
 constexpr int DENSE_MAX_VQ_PLAN = 4;   // qubits outside the tile per tensor-core phase (2^4 image variants)
