@@ -317,7 +317,9 @@ struct PhasePlan {
     std::vector<int> ops;     // indices into the sweep's op list
 };
 
-inline std::vector<PhasePlan> plan_phases(const Sweep& sw, uint32_t rb, bool all_slots = false) {
+// First-come register slots: each phase admits the slot qubits of the sweep's remaining
+// ops in order until rb are taken.
+inline std::vector<PhasePlan> plan_phases_first_come(const Sweep& sw, uint32_t rb, bool all_slots) {
     std::vector<PhasePlan> out;
     std::vector<char> taken(sw.ops.size(), 0);
     size_t first = 0;
@@ -354,6 +356,106 @@ inline std::vector<PhasePlan> plan_phases(const Sweep& sw, uint32_t rb, bool all
         out.push_back(std::move(ph));
     }
     return out;
+}
+
+// Ops of the sweep a phase with slot set R would take (per-qubit order kept), with the
+// same rules as plan_phases_first_come; marks them in *mark when given.
+inline int phase_closure(const Sweep& sw, const std::vector<char>& taken, size_t first, uint64_t R, bool all_slots,
+                         std::vector<int>* mark) {
+    uint64_t blocked = 0, outside = 0;
+    int cnt = 0;
+    for (size_t k = first; k < sw.ops.size(); ++k) {
+        if (taken[k]) continue;
+        const PGate& g = sw.ops[k];
+        const uint64_t qm = qmask(g);
+        const uint64_t need = needs(g, false) | (all_slots ? (qm & sw.L) : 0ull);
+        const uint64_t out2 = all_slots ? (outside | (qm & ~sw.L)) : 0ull;
+        if ((qm & blocked) || (need & ~R) || __builtin_popcountll(out2) > DENSE_MAX_VQ_PLAN) {
+            blocked |= qm;
+            continue;
+        }
+        outside = out2;
+        ++cnt;
+        if (mark) mark->push_back((int)k);
+    }
+    return cnt;
+}
+
+// Lookahead register slots: candidates are the first-come slot set and every window of
+// rb consecutive local qubits; each phase takes the one maximising the ops it runs plus
+// the most the next phase could then run.
+inline std::vector<PhasePlan> plan_phases_lookahead(const Sweep& sw, uint32_t rb, bool all_slots) {
+    std::vector<PhasePlan> out;
+    std::vector<char> taken(sw.ops.size(), 0);
+    std::vector<uint32_t> loc;
+    for (uint32_t q = 0; q < 64; ++q)
+        if ((sw.L >> q) & 1) loc.push_back(q);
+    auto cands = [&](const std::vector<char>& tk, size_t f) {
+        std::vector<uint64_t> c;
+        // the first-come choice for the remaining ops
+        uint64_t R = 0, blocked = 0, outside = 0;
+        for (size_t k = f; k < sw.ops.size(); ++k) {
+            if (tk[k]) continue;
+            const PGate& g = sw.ops[k];
+            const uint64_t qm = qmask(g);
+            if (qm & blocked) { blocked |= qm; continue; }
+            const uint64_t R2 = R | needs(g, false) | (all_slots ? (qm & sw.L) : 0ull);
+            const uint64_t out2 = all_slots ? (outside | (qm & ~sw.L)) : 0ull;
+            if ((uint32_t)__builtin_popcountll(R2) > rb || __builtin_popcountll(out2) > DENSE_MAX_VQ_PLAN) {
+                blocked |= qm;
+                continue;
+            }
+            R = R2;
+            outside = out2;
+        }
+        for (uint32_t q : loc)
+            if ((uint32_t)__builtin_popcountll(R) < rb && !((R >> q) & 1)) R |= 1ull << q;
+        c.push_back(R);
+        for (size_t a0 = 0; a0 + rb <= loc.size(); ++a0) {
+            uint64_t W = 0;
+            for (size_t j = a0; j < a0 + rb; ++j) W |= 1ull << loc[j];
+            if (W != R) c.push_back(W);
+        }
+        return c;
+    };
+    size_t first = 0;
+    while (first < sw.ops.size()) {
+        const auto c = cands(taken, first);
+        double best = -1.0;
+        uint64_t bestR = c[0];
+        for (uint64_t R : c) {
+            std::vector<int> got;
+            double score = phase_closure(sw, taken, first, R, all_slots, &got);
+            if (got.empty()) continue;
+            std::vector<char> t2 = taken;
+            for (int k : got) t2[k] = 1;
+            size_t f2 = first;
+            while (f2 < sw.ops.size() && t2[f2]) ++f2;
+            int next = 0;
+            if (f2 < sw.ops.size())
+                for (uint64_t R2 : cands(t2, f2)) next = std::max(next, phase_closure(sw, t2, f2, R2, all_slots, nullptr));
+            score += 0.999 * next;   // ties go to the set that runs more ops now
+            if (score > best) {
+                best = score;
+                bestR = R;
+            }
+        }
+        PhasePlan ph;
+        ph.R = bestR;
+        if (phase_closure(sw, taken, first, bestR, all_slots, &ph.ops) == 0) return {};   // no progress: give up
+        for (int k : ph.ops) taken[k] = 1;
+        while (first < sw.ops.size() && taken[first]) ++first;
+        out.push_back(std::move(ph));
+    }
+    return out;
+}
+
+// The phase plan: both planners, keeping the one with fewer phases (first-come on a tie
+// or when the lookahead finds no progress).
+inline std::vector<PhasePlan> plan_phases(const Sweep& sw, uint32_t rb, bool all_slots = false) {
+    auto a = plan_phases_first_come(sw, rb, all_slots);
+    auto b = plan_phases_lookahead(sw, rb, all_slots);
+    return (!b.empty() && b.size() < a.size()) ? b : a;
 }
 
 inline bool to_pgates(const rq_gate* gates, uint64_t n, std::vector<PGate>& out) {
