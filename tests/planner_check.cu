@@ -1,0 +1,165 @@
+// Host check of the sweep and phase planners of rq_plan.cuh (no GPU needed).
+//
+// Random circuits are planned with every planner combination (first-come and
+// lookahead sweeps, first-come and lookahead phases, CUDA-core and tensor-core
+// slot rules); the planned ops are applied in plan order (sweep, phase, op) to a
+// state vector in double precision, which must equal the gates applied in list
+// order.  The planners' own rules are checked on the way: every op's required
+// qubits are local and on slots, slot sets fit the register count, tensor-core
+// phases keep every local gate qubit on a slot and at most four qubits outside.
+// Exit status 0 = all good; the first failure is printed.
+#include "rq_plan.cuh"
+
+#include <complex>
+#include <cstdio>
+#include <random>
+
+using namespace rqp;
+using Cx = std::complex<double>;
+
+static void apply(std::vector<Cx>& a, const PGate& g) {
+    const uint64_t N = a.size();
+    const uint64_t b0 = 1ull << g.q0, b1 = 1ull << g.q1;
+    switch (g.type) {
+        case OP_U1: {
+            const Cx m00(g.m[0], g.m[1]), m01(g.m[2], g.m[3]), m10(g.m[4], g.m[5]), m11(g.m[6], g.m[7]);
+            for (uint64_t i = 0; i < N; ++i)
+                if (!(i & b0)) {
+                    const Cx x = a[i], y = a[i | b0];
+                    a[i] = m00 * x + m01 * y;
+                    a[i | b0] = m10 * x + m11 * y;
+                }
+            break;
+        }
+        case OP_D1:
+            for (uint64_t i = 0; i < N; ++i) a[i] *= (i & b0) ? Cx(g.m[2], g.m[3]) : Cx(g.m[0], g.m[1]);
+            break;
+        case OP_CX:
+            for (uint64_t i = 0; i < N; ++i)
+                if ((i & b0) && !(i & b1)) std::swap(a[i], a[i | b1]);
+            break;
+        case OP_CZ:
+            for (uint64_t i = 0; i < N; ++i)
+                if ((i & b0) && (i & b1)) a[i] = -a[i];
+            break;
+        case OP_ZZ:
+            for (uint64_t i = 0; i < N; ++i)
+                a[i] *= (!(i & b0) == !(i & b1)) ? Cx(g.m[0], g.m[1]) : Cx(g.m[2], g.m[3]);
+            break;
+        default:
+            std::printf("unexpected op type %d\n", (int)g.type);
+            std::exit(2);
+    }
+}
+
+static std::vector<rq_gate> random_circuit(uint32_t n, std::mt19937_64& r, bool brickwork) {
+    std::vector<rq_gate> out;
+    std::uniform_real_distribution<double> ang(0.0, 6.283185307179586);
+    const int kinds1[] = {RQ_GATE_H, RQ_GATE_X, RQ_GATE_Y, RQ_GATE_Z, RQ_GATE_S, RQ_GATE_T, RQ_GATE_RX,
+                          RQ_GATE_RY, RQ_GATE_RZ, RQ_GATE_PHASE};
+    const int kinds2[] = {RQ_GATE_CNOT, RQ_GATE_CZ, RQ_GATE_RZZ, RQ_GATE_SWAP};
+    if (brickwork) {
+        for (int l = 0; l < 8; ++l) {
+            for (uint32_t q = 0; q < n; ++q) {
+                rq_gate z{}; z.kind = RQ_GATE_RZ; z.q0 = q; z.angle = ang(r); out.push_back(z);
+                rq_gate x{}; x.kind = RQ_GATE_RX; x.q0 = q; x.angle = ang(r); out.push_back(x);
+            }
+            for (uint32_t q = l & 1; q + 1 < n; q += 2) {
+                rq_gate c{}; c.kind = RQ_GATE_CNOT; c.q0 = q; c.q1 = q + 1; out.push_back(c);
+            }
+        }
+        return out;
+    }
+    const int count = 60 + (int)(r() % 120);
+    for (int k = 0; k < count; ++k) {
+        rq_gate g{};
+        g.angle = ang(r);
+        g.q0 = (uint32_t)(r() % n);
+        if (r() % 3 == 0) {
+            g.kind = kinds2[r() % 4];
+            do g.q1 = (uint32_t)(r() % n); while (g.q1 == g.q0);
+        } else {
+            g.kind = kinds1[r() % 10];
+        }
+        out.push_back(g);
+    }
+    return out;
+}
+
+static int fail(const char* what, int trial) {
+    std::printf("trial %d: %s\n", trial, what);
+    return 1;
+}
+
+int main() {
+    std::mt19937_64 r(12345);
+    int trials = 0;
+    for (int trial = 0; trial < 240; ++trial) {
+        const uint32_t n = 8 + (uint32_t)(trial % 5);          // 8..12 qubits
+        const uint32_t m = 6 + (uint32_t)(trial % 3);          // 6..8 local
+        const uint32_t c = 3;
+        const bool brick = (trial % 4) == 0;
+        const auto circ = random_circuit(n, r, brick);
+        std::vector<PGate> pg;
+        if (!to_pgates(circ.data(), circ.size(), pg)) return fail("to_pgates", trial);
+        std::vector<Cx> want((size_t)1 << n);
+        std::normal_distribution<double> nd;
+        for (auto& v : want) v = Cx(nd(r), nd(r));
+        const std::vector<Cx> start = want;
+        for (const auto& g : pg) apply(want, g);
+        for (int sp = 0; sp < 3; ++sp) {
+            std::vector<Sweep> sweeps = sp == 0 ? plan_sweeps_first_come(pg, n, m, c)
+                                      : sp == 1 ? plan_sweeps_lookahead(pg, n, m, c)
+                                                : plan_sweeps(pg, n, m, c);
+            for (int pp = 0; pp < 3; ++pp)
+                for (int tc = 0; tc < 2; ++tc) {
+                    const uint32_t rb = tc ? 5 : (trial % 2 ? 5 : 4);
+                    std::vector<Cx> a = start;
+                    bool gave_up = false;
+                    for (Sweep sw : sweeps) {
+                        for (uint32_t q = 0; q < n && (uint32_t)__builtin_popcountll(sw.L) < m; ++q) sw.L |= 1ull << q;
+                        if ((uint32_t)__builtin_popcountll(sw.L) > m) return fail("sweep has too many local qubits", trial);
+                        for (const auto& g : sw.ops)
+                            if (needs(g, false) & ~sw.L) return fail("op needs a qubit outside its sweep", trial);
+                        const auto phases = pp == 0 ? plan_phases_first_come(sw, rb, tc)
+                                            : pp == 1 ? plan_phases_lookahead(sw, rb, tc)
+                                                      : plan_phases(sw, rb, tc);
+                        if (phases.empty() && !sw.ops.empty()) {
+                            if (pp == 1) {   // the lookahead may give up; plan_phases then falls back
+                                gave_up = true;
+                                break;
+                            }
+                            return fail("no phase plan", trial);
+                        }
+                        std::vector<int> seen(sw.ops.size(), 0);
+                        for (const auto& ph : phases) {
+                            if ((uint32_t)__builtin_popcountll(ph.R) > rb) return fail("too many slots", trial);
+                            if (ph.R & ~sw.L) return fail("slot outside the tile", trial);
+                            uint64_t outside = 0;
+                            for (int k : ph.ops) {
+                                const PGate& g = sw.ops[k];
+                                const uint64_t need = needs(g, false) | (tc ? (qmask(g) & sw.L) : 0ull);
+                                if (need & ~ph.R) return fail("op qubit not on a slot", trial);
+                                if (tc) outside |= qmask(g) & ~sw.L;
+                                ++seen[k];
+                                apply(a, g);
+                            }
+                            if (__builtin_popcountll(outside) > DENSE_MAX_VQ_PLAN) return fail("too many outside qubits", trial);
+                        }
+                        for (int v : seen)
+                            if (v != 1) return fail("op not applied exactly once", trial);
+                    }
+                    if (gave_up) continue;
+                    double err = 0.0;
+                    for (size_t i = 0; i < a.size(); ++i) err = std::max(err, std::abs(a[i] - want[i]));
+                    if (err > 1e-10) {
+                        std::printf("trial %d sweeps %d phases %d tc %d: max error %.3e\n", trial, sp, pp, tc, err);
+                        return 1;
+                    }
+                    ++trials;
+                }
+        }
+    }
+    std::printf("ok %d plans\n", trials);
+    return 0;
+}
