@@ -325,6 +325,19 @@ RQ_API int rq_state_fidelity(rq_state* a, rq_state* b, double* out); /* state.rs
 RQ_API int rq_state_negate_amplitudes(rq_state* s, const uint64_t* indices, uint64_t count);
 RQ_API int rq_state_negate_all_except(rq_state* s, uint64_t keep);
 
+/* A state split over ranks by its top qubits (a distributed state) makes a global
+ * qubit local by swapping it with a local qubit: each rank sends the half of its
+ * amplitudes whose local bit `qubit` differs from its own bit of the global qubit and
+ * receives the partner's half into the same places.  rq_state_half_copy copies the
+ * half with bit `qubit` == `value` (2^(n-1) amplitudes of the state's precision, in
+ * the order of the other bits) into a contiguous device buffer (RQ_HALF_PACK) or back
+ * from one (RQ_HALF_UNPACK), on the state's stream.  No reference counterpart (the
+ * reference has no distributed state). */
+#define RQ_HALF_PACK 0
+#define RQ_HALF_UNPACK 1
+RQ_API int rq_state_half_copy(rq_state* s, uint32_t qubit, uint32_t value, void* device_buf,
+                              int32_t direction);
+
 /* ------------------------------------------------------------------------ */
 /* batched QAOA-MaxCut (qaoa.rs:125-201 over many graphs / parameter sets)    */
 /* ------------------------------------------------------------------------ */

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(HERE, "libruqu_cuda.so")
 RQ_F32, RQ_F64 = 0, 1
 RQ_QAOA_GRAD_ADJOINT, RQ_QAOA_GRAD_SHIFT = 0, 1
 RQ_VQE_GRAD_NONE, RQ_VQE_GRAD_SHIFT, RQ_VQE_GRAD_ADJOINT = 0, 1, 2
+RQ_HALF_PACK, RQ_HALF_UNPACK = 0, 1
 RQ_EXEC_AUTO, RQ_EXEC_PER_GATE, RQ_EXEC_SWEEP, RQ_EXEC_SWEEP_TC, RQ_EXEC_SWEEP_TC_FAST = 0, 1, 2, 3, 4
 
 (RQ_OK, RQ_ERR_QUBIT_LIMIT_EXCEEDED, RQ_ERR_INVALID_QUBIT_INDEX, RQ_ERR_MEMORY_ALLOCATION,
@@ -68,6 +69,7 @@ SIGNATURES = {
     "rq_state_apply_noisy": (C.c_int, [_vp, _P(RqGate), _u64, _P(RqNoiseModel), _P(RqMeasurement), _u64, _P(_u64)]),
     "rq_state_negate_amplitudes": (C.c_int, [_vp, _P(_u64), _u64]),
     "rq_state_negate_all_except": (C.c_int, [_vp, _u64]),
+    "rq_state_half_copy": (C.c_int, [_vp, _u32, _u32, _vp, _i32]),
     "rq_state_apply_1q_matrix": (C.c_int, [_vp, _u32, _P(_dbl)]),
     "rq_state_apply_2q_matrix": (C.c_int, [_vp, _u32, _u32, _P(_dbl)]),
     "rq_state_measure": (C.c_int, [_vp, _u32, _P(RqMeasurement)]),

@@ -702,6 +702,23 @@ int rq_state_negate_amplitudes(rq_state* s, const uint64_t* indices, uint64_t co
     return RQ_OK;
 }
 
+int rq_state_half_copy(rq_state* s, uint32_t qubit, uint32_t value, void* device_buf, int32_t direction) {
+    if (!s || !device_buf) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (qubit >= s->nq)
+        return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "invalid qubit index " + std::to_string(qubit) + " for " +
+                                                        std::to_string(s->nq) + "-qubit system");
+    if (value > 1) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "value must be 0 or 1");
+    if (direction != RQ_HALF_PACK && direction != RQ_HALF_UNPACK)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "direction must be RQ_HALF_PACK or RQ_HALF_UNPACK");
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, device_buf) != cudaSuccess || at.type != cudaMemoryTypeDevice) {
+        cudaGetLastError();
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "the buffer must be device memory");
+    }
+    RQ_TRY(set_device(s));
+    return rq::half_copy(s, qubit, value, device_buf, direction == RQ_HALF_UNPACK ? 1 : 0);
+}
+
 int rq_state_negate_all_except(rq_state* s, uint64_t keep) {
     if (!s) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null state");
     RQ_TRY(set_device(s));

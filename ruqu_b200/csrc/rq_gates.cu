@@ -231,6 +231,20 @@ __global__ void k_negate_list(typename C2<T>::t* __restrict__ a, const uint64_t*
     }
 }
 
+// one half of the amplitudes (bit q == v), in the order of the other bits, to / from a
+// contiguous buffer: the exchange step of a state split over ranks by its top qubits
+template <typename T>
+__global__ void k_half_copy(typename C2<T>::t* __restrict__ a, typename C2<T>::t* __restrict__ buf, uint64_t half,
+                            uint32_t q, uint32_t v, int unpack) {
+    const uint64_t lo = (1ull << q) - 1;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < half;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t idx = ((i & ~lo) << 1) | ((uint64_t)v << q) | (i & lo);
+        if (unpack) a[idx] = buf[i];
+        else buf[i] = a[idx];
+    }
+}
+
 template <typename T>
 __global__ void k_basis(typename C2<T>::t* __restrict__ a, uint64_t n, uint64_t index) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -335,6 +349,13 @@ int gate_cz(rq_state* s, uint32_t q1, uint32_t q2) {
     uint64_t ng = s->n >> 2;
     if (s->prec == RQ_F32) RQ_LAUNCH(k_cz<float>, ng, (float2*)s->amps, ng, q1, q2);
     else RQ_LAUNCH(k_cz<double>, ng, (double2*)s->amps, ng, q1, q2);
+    return RQ_OK;
+}
+
+int half_copy(rq_state* s, uint32_t q, uint32_t v, void* buf, int unpack) {
+    const uint64_t half = s->n >> 1;
+    if (s->prec == RQ_F32) RQ_LAUNCH(k_half_copy<float>, half, (float2*)s->amps, (float2*)buf, half, q, v, unpack);
+    else RQ_LAUNCH(k_half_copy<double>, half, (double2*)s->amps, (double2*)buf, half, q, v, unpack);
     return RQ_OK;
 }
 

@@ -76,6 +76,7 @@ int gate_swap(rq_state* s, uint32_t q1, uint32_t q2);
 int gate_cz(rq_state* s, uint32_t q1, uint32_t q2);
 int scale_all(rq_state* s, double f);
 int negate_except(rq_state* s, uint64_t keep);
+int half_copy(rq_state* s, uint32_t q, uint32_t v, void* device_buf, int unpack);
 int negate_list(rq_state* s, const uint64_t* dev_idx, uint64_t count);   // distinct indices < 2^n
 int collapse(rq_state* s, uint32_t q, int keep_one, double nf);
 int upload_f64(rq_state* s, const double* dev_interleaved);   // device f64 -> state

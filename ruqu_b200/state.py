@@ -188,6 +188,13 @@ class QuantumState:
         idx = np.ascontiguousarray(np.asarray(indices, dtype=np.uint64).reshape(-1))
         check(lib.rq_state_negate_amplitudes(self._h, idx.ctypes.data_as(C.POINTER(C.c_uint64)), idx.size))
 
+    def half_copy(self, qubit: int, value: int, device_ptr: int, unpack: bool = False) -> None:
+        """Copy the amplitudes whose bit `qubit` equals `value` (in the order of the other
+        bits) to the device buffer at device_ptr, or back from it (unpack=True): the
+        exchange step of a distributed state.  Runs on this state's stream."""
+        check(lib.rq_state_half_copy(self._h, int(qubit), int(value), C.c_void_p(int(device_ptr)),
+                                     _capi.RQ_HALF_UNPACK if unpack else _capi.RQ_HALF_PACK))
+
     def negate_all_except(self, keep: int = 0) -> None:
         """amps[i] = -amps[i] for every i != keep, on the device (grover.rs:144-153)."""
         check(lib.rq_state_negate_all_except(self._h, int(keep)))
