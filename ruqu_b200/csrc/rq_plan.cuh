@@ -299,17 +299,6 @@ inline std::vector<Sweep> plan_sweeps_lookahead(const std::vector<PGate>& gates,
     return out;
 }
 
-// The sweep plan: both planners, keeping the one with fewer sweeps (each sweep is a full
-// read and write of the state); first-come on a tie.  A gate qubit that stays outside a
-// sweep's local set is uniform over each tile, for CUDA-core and tensor-core plans alike.
-inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c,
-                                      bool all_slots = false) {
-    (void)all_slots;
-    auto a = plan_sweeps_first_come(gates, n, m, c);
-    auto b = plan_sweeps_lookahead(gates, n, m, c);
-    return b.size() < a.size() ? b : a;
-}
-
 constexpr int DENSE_MAX_VQ_PLAN = 4;   // qubits outside the tile per tensor-core phase (2^4 image variants)
 
 struct PhasePlan {
@@ -456,6 +445,103 @@ inline std::vector<PhasePlan> plan_phases(const Sweep& sw, uint32_t rb, bool all
     auto a = plan_phases_first_come(sw, rb, all_slots);
     auto b = plan_phases_lookahead(sw, rb, all_slots);
     return (!b.empty() && b.size() < a.size()) ? b : a;
+}
+
+// Gates the fixed local set L takes, as a sweep (1-qubit runs fused), marking them taken.
+inline Sweep take_sweep(const std::vector<PGate>& gates, std::vector<char>& taken, size_t first, uint64_t L,
+                        uint32_t n, uint32_t m) {
+    Sweep sw;
+    sw.L = L;
+    std::vector<int> last(n, -1);
+    uint64_t blocked = 0;
+    for (size_t k = first; k < gates.size(); ++k) {
+        if (taken[k]) continue;
+        const PGate& g = gates[k];
+        const uint64_t qm = qmask(g);
+        if ((qm & blocked) || (needs(g, false) & ~L)) {
+            blocked |= qm;
+            continue;
+        }
+        taken[k] = 1;
+        if (is_1q(g.type) && last[g.q0] >= 0 && is_1q(sw.ops[last[g.q0]].type)) {
+            fuse_into(sw.ops[last[g.q0]], g);
+        } else {
+            sw.ops.push_back(g);
+            const int idx = (int)sw.ops.size() - 1;
+            for (uint32_t q = 0; q < n; ++q)
+                if ((qm >> q) & 1) last[q] = idx;
+        }
+    }
+    for (uint32_t q = 0; q < n && (uint32_t)__builtin_popcountll(sw.L) < m; ++q) sw.L |= 1ull << q;
+    return sw;
+}
+
+// Tensor-core sweep cost model: a launch costs about SWEEP_COST + PHASE_COST x its phases
+// (least-squares fit of the per-launch times of a 30-qubit f32 circuit's 14 sweeps with
+// 1-14 phases: 1.79 ms + 1.91 ms per phase, residuals < 0.8 ms; both terms scale with
+// the state size, so only their ratio matters here).
+constexpr double SWEEP_COST = 1.79, PHASE_COST = 1.91;
+
+inline double plan_cost(std::vector<Sweep> sweeps, uint32_t n, uint32_t m, uint32_t rb) {
+    double c = 0.0;
+    for (auto& sw : sweeps) {
+        for (uint32_t q = 0; q < n && (uint32_t)__builtin_popcountll(sw.L) < m; ++q) sw.L |= 1ull << q;
+        c += SWEEP_COST + PHASE_COST * (double)plan_phases(sw, rb, true).size();
+    }
+    return c;
+}
+
+// Cost-aware local sets for tensor-core plans: each sweep takes the candidate set that
+// maximises (gates it runs) x rate - (its launch cost), rate = the cost per gate of a
+// reference plan, so a set that runs many gates but needs many phases can lose to one
+// that runs slightly fewer in fewer phases.
+inline std::vector<Sweep> plan_sweeps_costed(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c,
+                                             uint32_t rb, double rate) {
+    std::vector<Sweep> out;
+    std::vector<char> taken(gates.size(), 0);
+    size_t first = 0;
+    while (first < gates.size()) {
+        double best = -1e300;
+        uint64_t bestL = 0;
+        bool found = false;
+        for (uint64_t L : sweep_candidates(gates, taken, first, n, m, c)) {
+            std::vector<char> t2 = taken;
+            Sweep sw = take_sweep(gates, t2, first, L, n, m);
+            if (sw.ops.empty()) continue;
+            int got = 0;
+            for (size_t k = first; k < gates.size(); ++k) got += (t2[k] && !taken[k]) ? 1 : 0;
+            const double score = rate * got - (SWEEP_COST + PHASE_COST * (double)plan_phases(sw, rb, true).size());
+            if (score > best) {
+                best = score;
+                bestL = L;
+                found = true;
+            }
+        }
+        if (!found) return {};   // no progress (cannot happen with the first-come candidate): give up
+        Sweep sw = take_sweep(gates, taken, first, bestL, n, m);
+        sw.L = bestL;
+        out.push_back(std::move(sw));
+        while (first < gates.size() && taken[first]) ++first;
+    }
+    return out;
+}
+
+// The sweep plan.  CUDA-core plans: the first-come and lookahead plans, keeping the one
+// with fewer sweeps (each sweep is a full read and write of the state; first-come on a
+// tie).  Tensor-core plans (all_slots, five register slots): also the cost-aware plan,
+// keeping the plan of least modelled cost.  A gate qubit that stays outside a sweep's
+// local set is uniform over each tile, for CUDA-core and tensor-core plans alike.
+inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c,
+                                      bool all_slots = false) {
+    auto a = plan_sweeps_first_come(gates, n, m, c);
+    auto b = plan_sweeps_lookahead(gates, n, m, c);
+    auto best = b.size() < a.size() ? b : a;
+    if (!all_slots || gates.empty()) return best;
+    const uint32_t rb = 5;
+    const double cost_best = plan_cost(best, n, m, rb);
+    auto d = plan_sweeps_costed(gates, n, m, c, rb, cost_best / (double)gates.size());
+    if (!d.empty() && plan_cost(d, n, m, rb) < cost_best) return d;
+    return best;
 }
 
 inline bool to_pgates(const rq_gate* gates, uint64_t n, std::vector<PGate>& out) {

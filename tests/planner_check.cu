@@ -1,7 +1,7 @@
 // Host check of the sweep and phase planners of rq_plan.cuh (no GPU needed).
 //
-// Random circuits are planned with every planner combination (first-come and
-// lookahead sweeps, first-come and lookahead phases, CUDA-core and tensor-core
+// Random circuits are planned with every planner combination (first-come,
+// lookahead and cost-aware sweeps, first-come and lookahead phases, CUDA-core and tensor-core
 // slot rules); the planned ops are applied in plan order (sweep, phase, op) to a
 // state vector in double precision, which must equal the gates applied in list
 // order.  The planners' own rules are checked on the way: every op's required
@@ -107,10 +107,13 @@ int main() {
         for (auto& v : want) v = Cx(nd(r), nd(r));
         const std::vector<Cx> start = want;
         for (const auto& g : pg) apply(want, g);
-        for (int sp = 0; sp < 3; ++sp) {
+        for (int sp = 0; sp < 5; ++sp) {
             std::vector<Sweep> sweeps = sp == 0 ? plan_sweeps_first_come(pg, n, m, c)
                                       : sp == 1 ? plan_sweeps_lookahead(pg, n, m, c)
-                                                : plan_sweeps(pg, n, m, c);
+                                      : sp == 2 ? plan_sweeps(pg, n, m, c)
+                                      : sp == 3 ? plan_sweeps(pg, n, m, c, true)
+                                                : plan_sweeps_costed(pg, n, m, c, 5, 0.05);
+            if (sweeps.empty() && !pg.empty()) return fail("no sweep plan", trial);
             for (int pp = 0; pp < 3; ++pp)
                 for (int tc = 0; tc < 2; ++tc) {
                     const uint32_t rb = tc ? 5 : (trial % 2 ? 5 : 4);
