@@ -406,6 +406,11 @@ RQ_API int rq_qaoa_batch_optimize_precond(rq_qaoa_batch* b, uint32_t steps, cons
                                           double* gammas, double* betas, const double* target, double rtol,
                                           double* energies, uint32_t* steps_taken);
 
+/* The convergence rule of run_qaoa (qaoa.rs:266-269) for both optimizers of this batch:
+ * an instance stops (as when it meets its target) once its energy changed by less than
+ * tol since the previous step.  tol = 0 (the default) turns it off; run_qaoa uses 1e-6. */
+RQ_API int rq_qaoa_batch_set_convergence(rq_qaoa_batch* b, double tol);
+
 /* Final amplitudes of one circuit of the last run (2^n interleaved doubles);
  * only circuits of the last memory wave of that run are still held. */
 RQ_API int rq_qaoa_batch_state(rq_qaoa_batch* b, uint64_t circuit, double* interleaved);

@@ -90,6 +90,7 @@ SIGNATURES = {
     "rq_qaoa_batch_gradient": (C.c_int, [_vp, _P(_dbl), _P(_dbl), _P(_dbl), _P(_dbl)]),
     "rq_qaoa_batch_optimize_precond": (C.c_int, [_vp, _u32, _P(_dbl), _dbl, _P(_dbl), _P(_dbl), _P(_dbl), _dbl,
                                                  _P(_dbl), _P(_u32)]),
+    "rq_qaoa_batch_set_convergence": (C.c_int, [_vp, _dbl]),
     "rq_qaoa_batch_last_ms": (C.c_int, [_vp, _P(C.c_float)]),
     "rq_qaoa_batch_set_state_budget": (C.c_int, [_vp, _u64]),
     "rq_qaoa_batch_destroy": (C.c_int, [_vp]),

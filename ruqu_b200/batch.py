@@ -121,6 +121,11 @@ class QaoaBatch:
         self.nsets = 1
         return g, b, e, st
 
+    def set_convergence(self, tol: float) -> None:
+        """run_qaoa's convergence rule (qaoa.rs:266-269) for optimize / optimize_precond: an
+        instance stops once its energy changed by less than tol in a step (0 turns it off)."""
+        check(lib.rq_qaoa_batch_set_convergence(self._h, float(tol)))
+
     def state(self, circuit: int) -> np.ndarray:
         n = self.graphs[circuit // self.nsets][0]
         out = np.empty(2 << n)

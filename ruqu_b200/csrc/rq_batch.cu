@@ -1151,6 +1151,7 @@ struct rq_qaoa_batch {
     uint32_t last_wave_n = 0;
     float last_ms = 0.f;
     size_t state_budget = (size_t)24 << 30;
+    double conv_tol = 0.0;                 // optimizers: stop an instance when |E - E_prev| < conv_tol (0: off)
 };
 
 namespace {
@@ -1620,7 +1621,7 @@ __global__ void k_qaoa_precond(const double* __restrict__ energy, const uint32_t
                                double* __restrict__ alpha, double* __restrict__ eprev,
                                const double* __restrict__ target, double rtol, uint32_t* __restrict__ done,
                                double* __restrict__ elast, int final_eval, const double* __restrict__ grad,
-                               const uint32_t* __restrict__ step_dev) {
+                               const uint32_t* __restrict__ step_dev, double conv) {
     const uint32_t step = *step_dev;
     const uint32_t P2 = 2 * p;
     for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < nact; a += gridDim.x * blockDim.x) {
@@ -1629,6 +1630,10 @@ __global__ void k_qaoa_precond(const double* __restrict__ energy, const uint32_t
         const double e = energy[a];
         elast[i] = e;
         if (target && e >= target[i] * (1.0 - rtol)) {
+            done[i] = step + 1;
+            continue;
+        }
+        if (conv > 0.0 && fabs(e - eprev[i]) < conv) {   // run_qaoa's convergence rule (qaoa.rs:266-269)
             done[i] = step + 1;
             continue;
         }
@@ -1655,7 +1660,8 @@ __global__ void k_qaoa_adam(const double* __restrict__ energy, const uint32_t* _
                             uint32_t p, uint32_t nsets, double* __restrict__ theta, double* __restrict__ m,
                             double* __restrict__ v, double lr, uint32_t step, const double* __restrict__ target,
                             double rtol, uint32_t* __restrict__ done, double* __restrict__ elast, int final_eval,
-                            const double* __restrict__ grad, const uint32_t* __restrict__ step_dev) {
+                            const double* __restrict__ grad, const uint32_t* __restrict__ step_dev,
+                            double* __restrict__ eprev, double conv) {
     if (step_dev) step = *step_dev;   // graph replays: the step counter lives on the device
     for (uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < nact; a += gridDim.x * blockDim.x) {
         const uint32_t i = act[a];
@@ -1666,6 +1672,11 @@ __global__ void k_qaoa_adam(const double* __restrict__ energy, const uint32_t* _
             done[i] = step + 1;
             continue;
         }
+        if (conv > 0.0 && fabs(e[0] - eprev[i]) < conv) {   // run_qaoa's convergence rule (qaoa.rs:266-269)
+            done[i] = step + 1;
+            continue;
+        }
+        eprev[i] = e[0];
         if (final_eval) continue;
         const double b1 = 0.9, b2 = 0.999, eps = 1e-8;
         const double c1 = 1.0 - pow(b1, (double)(step + 1)), c2 = 1.0 - pow(b2, (double)(step + 1));
@@ -1810,10 +1821,10 @@ int optimize_impl(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, d
     if (rc == RQ_OK) rc = dalloc_b(&d_done, ninst);
     if (rc == RQ_OK) rc = dalloc_b(&d_act, ninst);
     if (rc == RQ_OK) rc = dalloc_b(&d_step, 1);
+    if (rc == RQ_OK) rc = dalloc_b(&d_eprev, ninst);
     if (precond) {
         if (rc == RQ_OK) rc = dalloc_b(&d_pre, (size_t)ninst * P2 * P2);
         if (rc == RQ_OK) rc = dalloc_b(&d_alpha, ninst);
-        if (rc == RQ_OK) rc = dalloc_b(&d_eprev, ninst);
     }
     if (rc != RQ_OK) { cleanup(); return rc; }
     std::vector<double> pre_run, alpha_init, eprev_init;
@@ -1823,11 +1834,13 @@ int optimize_impl(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, d
             std::memcpy(&pre_run[(size_t)r * P2 * P2], precond + (size_t)inst_order[r] * P2 * P2,
                         (size_t)P2 * P2 * sizeof(double));
         alpha_init.assign(ninst, alpha0);
-        eprev_init.assign(ninst, -1e300);
         cudaMemcpyAsync(d_pre, pre_run.data(), pre_run.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream);
         cudaMemcpyAsync(d_alpha, alpha_init.data(), ninst * sizeof(double), cudaMemcpyHostToDevice, b->stream);
-        cudaMemcpyAsync(d_eprev, eprev_init.data(), ninst * sizeof(double), cudaMemcpyHostToDevice, b->stream);
     }
+    // the previous step's energy of every instance (damping, convergence rule): none yet
+    eprev_init.assign(ninst, -1e300);
+    cudaMemcpyAsync(d_eprev, eprev_init.data(), ninst * sizeof(double), cudaMemcpyHostToDevice, b->stream);
+    const double conv = b->conv_tol;
     // active set: run-order instances still optimising, their circuits' instance map, and per-class counts
     std::vector<uint32_t> act(ninst), ci;
     for (uint32_t r = 0; r < ninst; ++r) act[r] = r;
@@ -1865,12 +1878,13 @@ int optimize_impl(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, d
         if (precond)
             k_qaoa_precond<<<rq::grid_for(nact, TPB, sms), TPB, 0, b->stream>>>(
                 b->d_energy, d_act, nact, p, d_th, d_pre, d_alpha, d_eprev, target ? d_tg : nullptr, rtol, d_done,
-                d_el, final_eval ? 1 : 0, b->d_grad, d_step);
+                d_el, final_eval ? 1 : 0, b->d_grad, d_step, conv);
         else
             k_qaoa_adam<<<rq::grid_for(nact, TPB, sms), TPB, 0, b->stream>>>(b->d_energy, d_act, nact, p, nsets, d_th,
                                                                           d_m, d_v, lr, 0, target ? d_tg : nullptr,
                                                                           rtol, d_done, d_el, final_eval ? 1 : 0,
-                                                                          adj ? b->d_grad : nullptr, d_step);
+                                                                          adj ? b->d_grad : nullptr, d_step, d_eprev,
+                                                                          conv);
         k_step_inc<<<1, 32, 0, b->stream>>>(d_step);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return rq::cuda_fail(e, "optimizer kernels");
@@ -1906,7 +1920,7 @@ int optimize_impl(rq_qaoa_batch* b, uint32_t steps, double lr, double* gammas, d
     polled:
         if (rc != RQ_OK) break;
         cudaError_t e = cudaSuccess;
-        if (target && step < steps && (step % 2 == 1)) {
+        if ((target || conv > 0.0) && step < steps && (step % 2 == 1)) {
             // drop the instances that met their target from the next steps' launches; the
             // rest keep their slots' math (every circuit's energy is independent of the batch)
             e = cudaMemcpyAsync(dn.data(), d_done, ninst * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
@@ -1966,6 +1980,13 @@ int rq_qaoa_batch_optimize_precond(rq_qaoa_batch* b, uint32_t steps, const doubl
     if (!(alpha > 0.0)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "alpha must be positive");
     return optimize_impl(b, steps, 0.0, gammas, betas, target, rtol, RQ_QAOA_GRAD_ADJOINT, precond, alpha, energies,
                          steps_taken);
+}
+
+int rq_qaoa_batch_set_convergence(rq_qaoa_batch* b, double tol) {
+    if (!b) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (!(tol >= 0.0)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "tolerance must be >= 0");
+    b->conv_tol = tol;
+    return RQ_OK;
 }
 
 int rq_qaoa_batch_state(rq_qaoa_batch* b, uint64_t circuit, double* interleaved) {

@@ -189,3 +189,60 @@ def test_learned_curvature_pipeline_beats_plain():
     _, _, e_wp, st_wp = hb.optimize_precond(pg, pb, warm.preconditioners(held), steps, 0.8, target=target, rtol=1e-5)
     assert np.mean(e_wp >= target * (1 - 1e-5)) >= 0.9
     assert np.median(st_wp) < 0.5 * np.median(st_ramp), (np.median(st_wp), np.median(st_ramp))
+
+
+def test_convergence_rule_preconditioned_matches_host_loop():
+    """run_qaoa's rule (qaoa.rs:266-269): an instance stops once its energy changed by less
+    than tol in a step; the preconditioned device loop against the same loop on the host."""
+    graphs = _graphs(5, [8, 10, 12], 8)
+    p, steps, tol = 2, 12, 1e-3
+    g0, b0 = linear_ramp(p)
+    G, B = np.tile(g0, (5, 1)), np.tile(b0, (5, 1))
+    r = np.random.default_rng(3)
+    A = r.normal(size=(5, 2 * p, 2 * p))
+    P = 0.01 * (np.einsum('kij,klj->kil', A, A) + np.eye(2 * p))
+    qb = QaoaBatch(graphs, p, "f64")
+    qb.set_convergence(tol)
+    g, b, e, st = qb.optimize_precond(G, B, P, steps, 0.8)
+    th = np.concatenate([G, B], axis=1)
+    alpha = np.full(5, 0.8)
+    eprev = np.full(5, -1e300)
+    done = np.zeros(5, dtype=int)
+    elast = np.zeros(5)
+    for t in range(steps + 1):
+        en, gr = qb.gradient(th[:, :p], th[:, p:])
+        for k in range(5):
+            if done[k]:
+                continue
+            elast[k] = en[k]
+            if abs(en[k] - eprev[k]) < tol:
+                done[k] = t + 1
+                continue
+            if t == steps:
+                continue
+            if en[k] < eprev[k]:
+                alpha[k] *= 0.5
+            eprev[k] = en[k]
+            th[k] += alpha[k] * (P[k] @ gr[k])
+    assert (st < steps).any()                      # the rule stopped someone early
+    assert np.max(np.abs(g - th[:, :p])) < 1e-12 and np.max(np.abs(b - th[:, p:])) < 1e-12
+    assert np.max(np.abs(e - elast)) < 1e-12
+    assert np.array_equal(st, np.where(done > 0, done - 1, steps))
+
+
+def test_convergence_rule_adam_stops_at_the_first_small_change():
+    graphs = _graphs(6, [8, 10], 9)
+    p, steps, lr, tol = 2, 14, 0.05, 2e-3
+    g0, b0 = linear_ramp(p)
+    G, B = np.tile(g0, (6, 1)), np.tile(b0, (6, 1))
+    qb = QaoaBatch(graphs, p, "f64")
+    energy = np.stack([qb.optimize(G, B, s, lr)[2] for s in range(steps + 1)])   # energy after s updates
+    qb.set_convergence(tol)
+    _, _, e, st = qb.optimize(G, B, steps, lr)
+    qb.set_convergence(0.0)
+    for i in range(6):
+        small = [s for s in range(1, steps + 1) if abs(energy[s, i] - energy[s - 1, i]) < tol]
+        want = small[0] if small else steps
+        assert st[i] == want, (i, st[i], want)
+        assert abs(e[i] - energy[want, i]) < 1e-12
+    assert (st < steps).any()
