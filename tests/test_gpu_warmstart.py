@@ -232,11 +232,13 @@ def test_convergence_rule_preconditioned_matches_host_loop():
 
 def test_convergence_rule_adam_stops_at_the_first_small_change():
     graphs = _graphs(6, [8, 10], 9)
-    p, steps, lr, tol = 2, 14, 0.05, 2e-3
+    p, steps, lr = 2, 14, 0.05
     g0, b0 = linear_ramp(p)
     G, B = np.tile(g0, (6, 1)), np.tile(b0, (6, 1))
     qb = QaoaBatch(graphs, p, "f64")
     energy = np.stack([qb.optimize(G, B, s, lr)[2] for s in range(steps + 1)])   # energy after s updates
+    # a tolerance that half of the steps' energy changes fall below, so some instances stop early
+    tol = float(np.median(np.abs(np.diff(energy, axis=0))))
     qb.set_convergence(tol)
     _, _, e, st = qb.optimize(G, B, steps, lr)
     qb.set_convergence(0.0)
