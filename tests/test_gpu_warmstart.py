@@ -6,7 +6,6 @@ oracle's evaluate_qaoa_cost (qaoa.rs:179-201); the warm start is checked
 end to end on small graphs: training reduces the loss and warm-started
 instances reach the plain optimizer's energy in fewer steps.
 """
-import math
 
 import numpy as np
 import pytest

@@ -8,7 +8,6 @@ import os
 import re
 
 import numpy as np
-import pytest
 
 import oracle
 import ruqu_b200 as rq
