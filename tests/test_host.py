@@ -36,6 +36,25 @@ def test_library_exports_every_declared_symbol():
     assert set(names) <= set(_capi.SIGNATURES), set(names) - set(_capi.SIGNATURES)
 
 
+def test_abi_header_compiles_as_c_and_cpp(tmp_path):
+    """include/*.h is the drop-in boundary for C and C++ callers (and Rust / cgo binding
+    generators): it must compile on its own as C99 and as C++11, warning-free."""
+    import shutil
+    import subprocess
+    for cc, std, ext in (("gcc", "-std=c99", "c"), ("g++", "-std=c++11", "cpp")):
+        exe = shutil.which(cc)
+        if exe is None:
+            continue
+        for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+            if not h.endswith(".h"):
+                continue
+            src = tmp_path / f"use_{h}.{ext}"
+            src.write_text(f'#include "{h}"\nint main(void) {{ return 0; }}\n')
+            r = subprocess.run([exe, std, "-Wall", "-Wextra", "-Werror", "-fsyntax-only",
+                                "-I" + os.path.join(ROOT, "include"), str(src)], capture_output=True, text=True)
+            assert r.returncode == 0, (cc, h, r.stderr)
+
+
 def test_host_uniform_matches_oracle_and_numpy():
     for seed, stream in ((0, 0), (42, 0), (2**63 + 5, 3), (17, 1)):
         u = rng.uniforms(seed, stream, 0, 9)
