@@ -380,7 +380,8 @@ def small_circuit_leg(with_cpu):
     (seed 0), then <Z_i> for every qubit and 4096 shots (a full simulator run with its
     read-out).  Device time through the public API (state created, gates applied from the
     host list, results back on the host), gates/s, per-layer GB/s; beside it the oracle's
-    scalar f64 reference kernels on the same circuit (gate application only)."""
+    scalar f64 reference kernels on the same circuit (gate application only), one thread
+    and the OpenMP restatement of the reference's parallel kernels on all host cores."""
     import torch
 
     import ruqu_b200 as rq
@@ -417,6 +418,15 @@ def small_circuit_leg(with_cpu):
         out["cpu_baseline"] = {"ms": cpu_s * 1e3, "cores": 1, "kind": "port",
                                "sample": "the same %d gates on the oracle's scalar f64 reference kernels" % len(gates)}
         out["speedup_vs_cpu"] = cpu_s * 1e3 / min(ms)
+        # the reference's parallel kernels (rayon, simd.rs:270-377) restated with OpenMP on all host cores
+        o2 = oracle.OracleState(n, oracle.RQ_F64, 0)
+        t0 = time.perf_counter()
+        o2.apply(gates, parallel=True)
+        par_s = time.perf_counter() - t0
+        out["cpu_parallel"] = {"ms": par_s * 1e3, "cores": oracle.num_threads(), "kind": "port",
+                               "sample": "the same gates on the oracle's OpenMP restatement of the reference's "
+                                         "parallel kernels"}
+        out["speedup_vs_cpu_parallel"] = par_s * 1e3 / min(ms)
     return out
 
 
