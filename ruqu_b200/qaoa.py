@@ -86,6 +86,40 @@ def evaluate_qaoa_cost(graph: Graph, gammas, betas, seed=None, precision="f64") 
     return cost
 
 
+WASM_MAX_QUBITS = 25
+
+
+def qaoa_maxcut(num_nodes: int, edges_flat, p: int, gammas, betas, seed=None, precision: str = "f64") -> dict:
+    """ruqu-wasm's qaoa_maxcut by semantics (crates/ruqu-wasm/src/lib.rs:408-500): a graph
+    from flattened (u, v) pairs with unit weights, the QAOA circuit of build_qaoa_circuit,
+    one run_with_config, then {"probabilities": all 2^n probabilities, "expected_cut":
+    sum over the listed pairs of (1 - <Z_u Z_v>) / 2}.  The same argument checks (at most
+    25 nodes, p angles each, an even number of node indices), raised as ValueError; the
+    <ZZ> of all pairs come from one device call."""
+    if num_nodes > WASM_MAX_QUBITS:
+        raise ValueError(f"Qubit limit exceeded: {num_nodes} requested, max {WASM_MAX_QUBITS} in WASM")
+    gammas = list(gammas)
+    betas = list(betas)
+    if len(gammas) != p:
+        raise ValueError(f"gammas length mismatch: expected {p} (p), got {len(gammas)}")
+    if len(betas) != p:
+        raise ValueError(f"betas length mismatch: expected {p} (p), got {len(betas)}")
+    edges_flat = [int(x) for x in edges_flat]
+    if len(edges_flat) % 2:
+        raise ValueError("edges_flat must contain an even number of elements (pairs of node indices)")
+    graph = Graph(num_nodes)
+    pairs = list(zip(edges_flat[0::2], edges_flat[1::2]))
+    for u, v in pairs:
+        graph.add_edge(u, v, 1.0)
+    res = Simulator.run_with_config(build_qaoa_circuit(graph, gammas, betas), SimConfig(seed=seed, precision=precision))
+    probs = res.state.probabilities()
+    zz = res.state.expectation_values([PauliString([(u, PauliOp.Z), (v, PauliOp.Z)]) for u, v in pairs]) if pairs else []
+    expected_cut = 0.0
+    for z in zz:
+        expected_cut += 0.5 * (1.0 - z)
+    return {"probabilities": probs, "expected_cut": float(expected_cut)}
+
+
 def _best_index(probs: np.ndarray) -> int:
     """Iterator::max_by semantics: the last of equal maxima (qaoa.rs:249-255)."""
     mx = probs.max()
