@@ -54,7 +54,7 @@ def _args():
     ap.add_argument("--layers", type=int, default=20)
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32")
-    ap.add_argument("--mode", choices=["auto", "per_gate", "sweep", "tc", "tc_fast"], default="auto")
+    ap.add_argument("--mode", choices=["auto", "per_gate", "sweep", "tc", "tc_fast", "tc16"], default="auto")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-qaoa", action="store_true", help="skip the batched QAOA leg")
@@ -137,25 +137,57 @@ def _dist():
     return world()
 
 
-def cpu_baseline_sample(a, parallel: bool, gates_in_sample: int = 4):
-    """Time the oracle (restated reference kernels) on the first gates of the same circuit.
-    Returns (GB/s, seconds, cores, sample description)."""
+def _gate_kinds(gates):
+    """(one-qubit gates, two-qubit gates) of a gate list."""
+    one = [g for g in gates if g[0] != 12]
+    two = [g for g in gates if g[0] == 12]
+    return one, two
+
+
+def cpu_circuit_time(a, parallel: bool, n_one: int, n_two: int, st=None, start: int = 0):
+    """Time n_one one-qubit gates and n_two CNOTs of the benchmark circuit on the oracle
+    (the restated reference kernels, one pass over the state per gate), each gate timed on
+    its own, and extrapolate to the whole circuit: circuit seconds = (#1q gates) x mean 1q
+    time + (#CNOTs) x mean CNOT time.  Returns (circuit seconds, timed seconds, cores, the
+    state, per-kind mean seconds)."""
     import oracle
     from ruqu_b200 import workloads
-    gates = workloads.random_layer_circuit(a.qubits, a.layers, a.seed)[:gates_in_sample]
-    prec = oracle.RQ_F32 if a.precision == "f32" else oracle.RQ_F64
-    st = oracle.OracleState(a.qubits, prec, 0)
-    elem = 8 if a.precision == "f32" else 16
-    S = (1 << a.qubits) * elem
-    nbytes = sum(S if g[0] == 12 else 2 * S for g in gates)
-    t0 = time.perf_counter()
-    st.apply(gates, parallel=parallel)
-    dt = time.perf_counter() - t0
+    gates = workloads.random_layer_circuit(a.qubits, a.layers, a.seed)
+    one, two = _gate_kinds(gates)
+    if st is None:
+        prec = oracle.RQ_F32 if a.precision == "f32" else oracle.RQ_F64
+        st = oracle.OracleState(a.qubits, prec, 0)
+    t_one, t_two = [], []
+    for k in range(n_one):
+        g = one[(start * n_one + k) % len(one)]
+        t0 = time.perf_counter()
+        st.apply([g], parallel=parallel)
+        t_one.append(time.perf_counter() - t0)
+    for k in range(n_two):
+        g = two[(start * n_two + k) % len(two)]
+        t0 = time.perf_counter()
+        st.apply([g], parallel=parallel)
+        t_two.append(time.perf_counter() - t0)
+    m1 = sum(t_one) / max(1, len(t_one))
+    m2 = sum(t_two) / max(1, len(t_two))
+    circuit_s = len(one) * m1 + len(two) * m2
     cores = oracle.num_threads() if parallel else 1
-    desc = (f"first {len(gates)} gates of the {a.qubits}-qubit circuit on a {a.precision} state, "
-            f"{'OpenMP restatement of the reference parallel kernels' if parallel else 'scalar reference kernels'}"
-            f", {cores} thread(s)")
-    return nbytes / dt / 1e9, dt, cores, desc
+    return circuit_s, sum(t_one) + sum(t_two), cores, st, (m1, m2)
+
+
+def cpu_baseline_sample(a, parallel: bool):
+    """The CPU baseline of the GPU arm: the oracle's scalar reference kernels (1 thread) on
+    two one-qubit gates and one CNOT of the benchmark circuit, extrapolated to the whole
+    circuit; reported in the GPU arm's own unit (per-layer bytes / circuit time).
+    Returns (GB/s, circuit seconds, timed seconds, cores, sample description)."""
+    S = (1 << a.qubits) * (8 if a.precision == "f32" else 16)
+    layer_bytes = S + 2 * S * a.layers
+    circuit_s, timed_s, cores, _, (m1, m2) = cpu_circuit_time(a, parallel, 2, 1)
+    desc = (f"2 one-qubit gates and 1 CNOT of the {a.qubits}-qubit circuit on a {a.precision} state, each one "
+            f"pass of the {'OpenMP restatement of the reference parallel kernels' if parallel else 'scalar reference kernels'}"
+            f" ({cores} thread(s)); mean {m1 * 1e3:.0f} ms per 1q gate, {m2 * 1e3:.0f} ms per CNOT; circuit time "
+            f"extrapolated by gate counts; value = (S + 2S x layers) / circuit time, the GPU arm's byte count")
+    return layer_bytes / circuit_s / 1e9, circuit_s, timed_s, cores, desc
 
 
 def qaoa_batch_leg(a, ws, rank, with_cpu):
@@ -368,10 +400,16 @@ _NCU_BYTES_PER_TILE = {"k_sweep_tc": (537.133824e6 + 487.704576e6) / 2 ** 13,
                        "k_sweep": (537.2e6 + 485.1e6) / 2 ** 13}
 
 
+_EXECUTED_AS = {1: "unfused per-gate kernels", 2: "CUDA-core sweeps", 3: "tensor-core sweeps (3xTF32)",
+                4: "tensor-core sweeps (one TF32 pass)", 5: "tensor-core sweeps (3xFP16 split)"}
+_KERNEL_OF = {2: "k_sweep (multi-gate sweep)", 3: "k_sweep_tc (tensor-core sweep, 3xTF32)",
+              4: "k_sweep_tc (tensor-core sweep, one TF32 pass)", 5: "k_sweep_tc16 (tensor-core sweep, 3xFP16)"}
+
+
 def _traffic_per_launch(a, stats):
-    if a.precision != "f32":
+    kern = {2: "k_sweep", 3: "k_sweep_tc", 4: "k_sweep_tc", 5: "k_sweep_tc16"}.get(stats["exec_mode"])
+    if a.precision != "f32" or kern not in _NCU_BYTES_PER_TILE or stats["local_qubits"] != 13:
         return None
-    kern = "k_sweep_tc" if stats["dense_ops"] else "k_sweep"
     return _NCU_BYTES_PER_TILE[kern] * 2 ** (a.qubits - 13)
 
 
@@ -499,7 +537,8 @@ def variants_leg(a, garr):
     ref.synchronize()
     out = {"value_bytes_per_run": layer_bytes, "reference": "complex f64 CUDA-core sweep of the same circuit"}
     for name, mode in (("unfused_per_gate", rq.RQ_EXEC_PER_GATE), ("sweep_cuda_cores", rq.RQ_EXEC_SWEEP),
-                       ("tensor_core_3xtf32", rq.RQ_EXEC_SWEEP_TC), ("tensor_core_tf32", rq.RQ_EXEC_SWEEP_TC_FAST)):
+                       ("tensor_core_3xtf32", rq.RQ_EXEC_SWEEP_TC), ("tensor_core_tf32", rq.RQ_EXEC_SWEEP_TC_FAST),
+                       ("tensor_core_3xfp16", rq.RQ_EXEC_SWEEP_TC16)):
         st = rq.QuantumState(a.qubits, 0, "f32")
         plan = rq.Plan(st, garr, mode)
         _, sptr = st.device_pointer()
@@ -524,38 +563,48 @@ def variants_leg(a, garr):
 
 
 def run_reference(a):
+    """The reference arm: the oracle's OpenMP restatement of the reference's parallel
+    kernels (one pass over the state per gate, the reference's execution model) on all host
+    cores.  Each step times a bounded sample of the benchmark circuit (3 one-qubit gates and
+    1 CNOT, in circuit order, each gate timed on its own); the circuit time is extrapolated
+    from the per-kind mean gate times and the gate counts, and `value` is the GPU arm's
+    per-layer byte count (S + 2S x layers) over that circuit time, so the two arms' values
+    divide to the ratio of their circuit times.  Imports nothing that loads the CUDA library."""
     ws, rank, _ = _dist()
     if rank != 0:
         return
     import oracle
     from ruqu_b200 import workloads
     gates = workloads.random_layer_circuit(a.qubits, a.layers, a.seed)
+    one, two = _gate_kinds(gates)
     prec = oracle.RQ_F32 if a.precision == "f32" else oracle.RQ_F64
     st = oracle.OracleState(a.qubits, prec, 0)
-    elem = 8 if a.precision == "f32" else 16
-    S = (1 << a.qubits) * elem
-    per_step = 4
-    pos = 0
-    times, nbytes = [], []
+    S = (1 << a.qubits) * (8 if a.precision == "f32" else 16)
+    layer_bytes = S + 2 * S * a.layers
+    t1, t2, step_s = [], [], []
     for it in range(a.warmup + a.steps):
-        chunk = [gates[(pos + k) % len(gates)] for k in range(per_step)]
-        pos += per_step
-        b = sum(S if g[0] == 12 else 2 * S for g in chunk)
-        t0 = time.perf_counter()
-        st.apply(chunk, parallel=True)
-        dt = time.perf_counter() - t0
+        _, timed, cores, st, (m1, m2) = cpu_circuit_time(a, True, 3, 1, st=st, start=it)
         if it >= a.warmup:
-            times.append(dt)
-            nbytes.append(b)
-    value = sum(nbytes) / sum(times) / 1e9
+            t1.append(m1)
+            t2.append(m2)
+            step_s.append(timed)
+    m1 = sum(t1) / len(t1)
+    m2 = sum(t2) / len(t2)
+    circuit_s = len(one) * m1 + len(two) * m2
+    value = layer_bytes / circuit_s / 1e9
     cores = oracle.num_threads()
-    sample = (f"{per_step} consecutive gates of the {a.qubits}-qubit circuit per step on a {a.precision} state, "
-              f"one pass over the state per gate (the reference's execution model)")
+    sample = (f"per step 3 one-qubit gates and 1 CNOT of the {a.qubits}-qubit circuit on a {a.precision} state, "
+              f"one pass over the state per gate (the reference's execution model), OpenMP restatement of the "
+              f"reference's parallel kernels; circuit time extrapolated from the mean per-kind gate times "
+              f"({m1 * 1e3:.1f} ms per 1q gate, {m2 * 1e3:.1f} ms per CNOT) x ({len(one)}, {len(two)}) gates")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
-        "warmup": a.warmup, "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+        "warmup": a.warmup, "ms_per_step": 1e3 * sum(step_s) / len(step_s), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": a.precision, "data": "synthetic",
-        "config": {"workload": _workload_desc(a), "l2": "state larger than L2"},
+        "config": {"workload": _workload_desc(a), "l2": "state larger than L2",
+                   "value_bytes_per_circuit": layer_bytes, "circuit_ms": circuit_s * 1e3,
+                   "circuit_ms_kind": "extrapolated from the timed gate sample",
+                   "ms_per_step_is": "timed sample of 4 gates per step"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -582,7 +631,7 @@ def run_ours(a):
     torch.cuda.set_device(local)
 
     mode = {"auto": rq.RQ_EXEC_AUTO, "per_gate": rq.RQ_EXEC_PER_GATE, "sweep": rq.RQ_EXEC_SWEEP,
-            "tc": rq.RQ_EXEC_SWEEP_TC, "tc_fast": rq.RQ_EXEC_SWEEP_TC_FAST}[a.mode]
+            "tc": rq.RQ_EXEC_SWEEP_TC, "tc_fast": rq.RQ_EXEC_SWEEP_TC_FAST, "tc16": rq.RQ_EXEC_SWEEP_TC16}[a.mode]
     gates = workloads.random_layer_circuit(a.qubits, a.layers, a.seed)
     garr = gates_to_array(gates)
     state = rq.QuantumState(a.qubits, 0, a.precision)
@@ -684,8 +733,9 @@ def run_ours(a):
 
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
-        v, secs, cores, desc = cpu_baseline_sample(a, parallel=False)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc, "seconds": secs}
+        v, circuit_s, secs, cores, desc = cpu_baseline_sample(a, parallel=False)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc, "seconds": secs,
+               "circuit_ms": circuit_s * 1e3}
 
     if rank == 0:
         ref_layer_bytes = workloads.random_layer_bytes(a.qubits, a.layers, elem) + S
@@ -698,13 +748,15 @@ def run_ours(a):
                        "sweeps_per_step": stats["sweeps"], "launches_per_step": 1 + stats["launches"],
                        "phases_per_step": stats["phases"], "device_ops_per_step": stats["ops"],
                        "dense_tensor_core_ops_per_step": stats["dense_ops"],
-                       "executed_as": "tensor-core sweeps (3xTF32)" if stats["dense_ops"] else "CUDA-core sweeps",
+                       "executed_as": _EXECUTED_AS.get(stats["exec_mode"], str(stats["exec_mode"])),
+                       "local_qubits": stats["local_qubits"],
                        "value_bytes_per_step": layer_bytes, "plan_hbm_bytes_per_step": step_bytes,
+                       "circuit_ms": total_ms / a.steps,
                        "layers_per_s": ws * a.layers * a.steps / (total_ms / 1e3),
                        "ms_init": init_ms / a.steps, "ms_gates": plan_ms / a.steps,
                        "unfused_reference_bytes_per_step": ref_layer_bytes},
-            "roofline": {"bound": "hbm", "kernel": "k_sweep_tc (tensor-core sweep)" if stats["dense_ops"]
-                         else "k_sweep (multi-gate sweep)", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": _KERNEL_OF.get(stats["exec_mode"], "k_sweep (multi-gate sweep)"),
+                         "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg_launch_ms,
                          "traffic": _traffic_per_launch(a, stats)},

@@ -114,8 +114,13 @@ typedef enum rq_exec_mode {
     RQ_EXEC_SWEEP_TC = 3,  /* sweeps whose per-phase gate runs are fused into dense
                               32x32 unitaries applied on the tensor cores as
                               3xTF32 MMAs (complex f32 states, >= 12 qubits)     */
-    RQ_EXEC_SWEEP_TC_FAST = 4  /* as RQ_EXEC_SWEEP_TC with one TF32 MMA pass
+    RQ_EXEC_SWEEP_TC_FAST = 4, /* as RQ_EXEC_SWEEP_TC with one TF32 MMA pass
                                   (10-bit operand mantissas)                     */
+    RQ_EXEC_SWEEP_TC16 = 5     /* as RQ_EXEC_SWEEP_TC with the dense ops as three
+                                  FP16 MMA passes (hi*hi + hi*lo + lo*hi of
+                                  per-tile-scaled amplitudes and 2^14-scaled
+                                  unitaries, FP32 accumulation): FP32-level
+                                  accuracy at twice the TF32 tensor rate        */
 } rq_exec_mode;
 
 typedef struct rq_state rq_state;   /* opaque: device-resident amplitudes */
@@ -130,6 +135,8 @@ typedef struct rq_plan_stats {
     uint64_t ops;         /* device ops after 1-qubit fusion                    */
     uint64_t hbm_bytes;   /* algorithmic HBM bytes per execution                */
     uint64_t dense_ops;   /* dense 32x32 unitaries on the tensor cores          */
+    uint64_t exec_mode;   /* rq_exec_mode the plan runs (RQ_EXEC_AUTO resolved)  */
+    uint64_t local_qubits;/* qubits per tile of a sweep (0: per-gate)            */
 } rq_plan_stats;
 
 /* ------------------------------------------------------------------------ */
@@ -183,6 +190,19 @@ RQ_API int rq_state_device_ptr(const rq_state* s, void** out_ptr, void** out_str
 
 /* Block the host until all work queued on the state's stream is done. */
 RQ_API int rq_state_synchronize(rq_state* s);
+
+/* Test hook, no counterpart in the reference: the number of polls a
+ * tensor-core kernel (the sweeps of RQ_EXEC_SWEEP_TC / _FAST / _TC16 and the
+ * BF16 GEMM) makes on an mbarrier before its wait counts as expired, on the
+ * current device; RQ_WAIT_LIMIT_DEFAULT restores the default.  With 0 polls
+ * the waits run out at once: the kernel sets its error flag, waits (with the
+ * default limit) for its copies and MMAs in flight, frees its tensor memory
+ * and returns; the next read-back of the state (rq_state_synchronize,
+ * rq_state_download, an expectation, probabilities or samples) -- or the
+ * GEMM call itself -- reports RQ_ERR_TIMEOUT and clears the flag, and the
+ * state's handle stays usable (its amplitudes are not: reset or upload). */
+#define RQ_WAIT_LIMIT_DEFAULT 0xFFFFFFFFu
+RQ_API int rq_debug_set_wait_limit(uint32_t polls);
 
 /* ------------------------------------------------------------------------ */
 /* gates (state.rs:158-276)                                                  */
@@ -294,12 +314,16 @@ RQ_API int rq_state_expectation_hamiltonian(rq_state* s, const double* coeffs,
  *   - at most RQ_NOALLOC_MAX_STRINGS strings per call; more is rejected with
  *     RQ_ERR_INVALID_ARGUMENT and nothing runs;
  *   - the first call on a device looks up the scratch address for that device
- *     (with the device current); make that first call before any stream
- *     capture;
- *   - every call shares the one scratch array, so calls that overlap on the
- *     GPU (other streams, other host threads) race: serialise them;
+ *     (with the device current), and so does the first call after the
+ *     device's context was re-created (cudaDeviceReset); make that first call
+ *     before any stream capture;
+ *   - every call shares the one scratch array and keeps nothing from earlier
+ *     calls (each call writes every partial it reads), so calls that overlap
+ *     on the GPU (other streams, other host threads) race: serialise them;
  *   - runs on `stream` (a cudaStream_t, NULL = the legacy default stream) on
- *     the current device and returns after the results are in out[] (host).
+ *     the current device; it blocks the host: it copies the sums back and
+ *     synchronises `stream` before it returns with the results in out[];
+ *   - a NULL `ops` with a non-empty string is rejected (RQ_ERR_INVALID_ARGUMENT).
  * It calls no cudaMalloc / cudaFree and no allocating library routine. */
 #define RQ_NOALLOC_MAX_STRINGS 128u
 #define RQ_NOALLOC_MAX_BLOCKS 1024u

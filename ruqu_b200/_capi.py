@@ -15,7 +15,7 @@ RQ_F32, RQ_F64 = 0, 1
 RQ_QAOA_GRAD_ADJOINT, RQ_QAOA_GRAD_SHIFT = 0, 1
 RQ_VQE_GRAD_NONE, RQ_VQE_GRAD_SHIFT, RQ_VQE_GRAD_ADJOINT = 0, 1, 2
 RQ_HALF_PACK, RQ_HALF_UNPACK = 0, 1
-RQ_EXEC_AUTO, RQ_EXEC_PER_GATE, RQ_EXEC_SWEEP, RQ_EXEC_SWEEP_TC, RQ_EXEC_SWEEP_TC_FAST = 0, 1, 2, 3, 4
+RQ_EXEC_AUTO, RQ_EXEC_PER_GATE, RQ_EXEC_SWEEP, RQ_EXEC_SWEEP_TC, RQ_EXEC_SWEEP_TC_FAST, RQ_EXEC_SWEEP_TC16 = range(6)
 
 (RQ_OK, RQ_ERR_QUBIT_LIMIT_EXCEEDED, RQ_ERR_INVALID_QUBIT_INDEX, RQ_ERR_MEMORY_ALLOCATION,
  RQ_ERR_INVALID_STATE_VECTOR, RQ_ERR_CIRCUIT, RQ_ERR_CUDA, RQ_ERR_TIMEOUT, RQ_ERR_INVALID_ARGUMENT) = range(9)
@@ -40,7 +40,8 @@ class RqPauliOp(C.Structure):
 
 class RqPlanStats(C.Structure):
     _fields_ = [("gates", C.c_uint64), ("launches", C.c_uint64), ("sweeps", C.c_uint64), ("phases", C.c_uint64),
-                ("ops", C.c_uint64), ("hbm_bytes", C.c_uint64), ("dense_ops", C.c_uint64)]
+                ("ops", C.c_uint64), ("hbm_bytes", C.c_uint64), ("dense_ops", C.c_uint64),
+                ("exec_mode", C.c_uint64), ("local_qubits", C.c_uint64)]
 
 
 # name -> (restype, argtypes); every symbol here is declared in include/ruqu_cuda.h
@@ -64,6 +65,7 @@ SIGNATURES = {
     "rq_state_precision": (C.c_int, [_vp, _P(_i32)]),
     "rq_state_device_ptr": (C.c_int, [_vp, _P(_vp), _P(_vp)]),
     "rq_state_synchronize": (C.c_int, [_vp]),
+    "rq_debug_set_wait_limit": (C.c_int, [_u32]),
     "rq_state_apply": (C.c_int, [_vp, _P(RqGate), _u64, _P(RqMeasurement), _u64, _P(_u64)]),
     "rq_state_apply_mode": (C.c_int, [_vp, _P(RqGate), _u64, _i32, _P(RqMeasurement), _u64, _P(_u64)]),
     "rq_state_apply_noisy": (C.c_int, [_vp, _P(RqGate), _u64, _P(RqNoiseModel), _P(RqMeasurement), _u64, _P(_u64)]),

@@ -353,7 +353,7 @@ int rq_device_count(int32_t* out) {
 
 int rq_plan_create(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out) {
     if (!s || !out || (!gates && n)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
-    if (mode < RQ_EXEC_AUTO || mode > RQ_EXEC_SWEEP_TC_FAST)
+    if (mode < RQ_EXEC_AUTO || mode > RQ_EXEC_SWEEP_TC16)
         return rq::fail(RQ_ERR_INVALID_ARGUMENT, "bad execution mode");
     for (uint64_t k = 0; k < n; ++k) {
         RQ_TRY(validate_gate(s, gates[k]));
@@ -429,8 +429,12 @@ int rq_state_device_ptr(const rq_state* s, void** out_ptr, void** out_stream) {
 int rq_state_synchronize(rq_state* s) {
     if (!s) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null state");
     RQ_TRY(set_device(s));
-    RQ_CUDA(cudaStreamSynchronize(s->stream));
-    return RQ_OK;
+    return rq::sync_checked(s);
+}
+
+int rq_debug_set_wait_limit(uint32_t polls) {
+    RQ_TRY(rq::tc_set_wait_polls(polls));
+    return rq::mma_set_wait_polls(polls);
 }
 
 }  // extern "C"
@@ -500,7 +504,7 @@ extern "C" {
 int rq_state_apply_mode(rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_measurement* out,
                         uint64_t cap, uint64_t* nout) {
     if (!s || (!gates && n)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
-    if (mode < RQ_EXEC_AUTO || mode > RQ_EXEC_SWEEP_TC_FAST)
+    if (mode < RQ_EXEC_AUTO || mode > RQ_EXEC_SWEEP_TC16)
         return rq::fail(RQ_ERR_INVALID_ARGUMENT, "bad execution mode");
     RQ_TRY(set_device(s));
     for (uint64_t k = 0; k < n; ++k) RQ_TRY(validate_gate(s, gates[k]));
@@ -642,6 +646,7 @@ int rq_state_expectation_value(rq_state* s, const rq_pauli_op* ops, uint32_t nop
 int rq_state_expectation_batch(rq_state* s, const rq_pauli_op* ops, const uint32_t* offsets, uint32_t nstrings,
                                double* out) {
     if (!s || (!out && nstrings) || (!offsets && nstrings)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (nstrings && !ops && offsets[nstrings] > offsets[0]) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
     std::vector<rq::PauliMask> masks(nstrings);
     for (uint32_t k = 0; k < nstrings; ++k) {
         if (offsets[k + 1] < offsets[k]) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "offsets must be non-decreasing");
@@ -744,8 +749,7 @@ int rq_state_download(rq_state* s, double* out) {
     size_t bytes = s->n * 2 * sizeof(double);
     if (s->prec == RQ_F64) {
         RQ_CUDA(cudaMemcpyAsync(out, s->amps, bytes, cudaMemcpyDeviceToHost, s->stream));
-        RQ_CUDA(cudaStreamSynchronize(s->stream));
-        return RQ_OK;
+        return rq::sync_checked(s);
     }
     double* d = nullptr;
     RQ_CUDA(cudaMallocAsync((void**)&d, bytes, s->stream));
@@ -755,8 +759,7 @@ int rq_state_download(rq_state* s, double* out) {
     cudaFreeAsync(d, s->stream);
     RQ_TRY(rc);
     RQ_CUDA(e);
-    RQ_CUDA(cudaStreamSynchronize(s->stream));
-    return RQ_OK;
+    return rq::sync_checked(s);
 }
 
 int rq_state_upload(rq_state* s, const double* in) {

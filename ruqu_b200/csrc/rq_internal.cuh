@@ -113,8 +113,12 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
 // with 13 or 12 local qubits): tensor-core passes (0 or 3) and tile shape (m, 0 = default),
 // cached per (device, qubits, gate structure)
 int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes, uint32_t* m);
-// the tensor-core passes a mode asks for (0: none)
-inline int tc_passes_of(int32_t mode) { return mode == RQ_EXEC_SWEEP_TC ? 3 : mode == RQ_EXEC_SWEEP_TC_FAST ? 1 : 0; }
+// the tensor-core arithmetic a mode asks for: 0 none, 3 = 3xTF32, 1 = one TF32 pass,
+// TC_F16 = three FP16 passes (RQ_EXEC_SWEEP_TC16)
+constexpr int TC_F16 = 16;
+inline int tc_passes_of(int32_t mode) {
+    return mode == RQ_EXEC_SWEEP_TC ? 3 : mode == RQ_EXEC_SWEEP_TC_FAST ? 1 : mode == RQ_EXEC_SWEEP_TC16 ? TC_F16 : 0;
+}
 int plan_launch(rq_state* s, const rq_plan* p);
 void plan_free(rq_plan* p);
 rq_plan_stats plan_stats(const rq_plan* p);
@@ -122,7 +126,17 @@ bool plan_fits(const rq_plan* p, const rq_state* s);
 int apply_one_gate(rq_state* s, const rq_gate& g);   // per-gate kernels (rq_capi.cu)
 
 // ---- tensor-core GEMM (rq_mlp.cu) -------------------------------------------
+// read-and-clear of the GEMM kernels' expired-wait flag on the current device
 int mma_timeout_flag(int* out);
+// polls before an mbarrier wait counts as expired (0: the default), current device
+int mma_set_wait_polls(uint32_t polls);
+// the tensor-core sweeps' equivalents (rq_sweep.cu)
+int tc_timeout_flag(int* out);
+int tc_set_wait_polls(uint32_t polls);
+// synchronise the state's stream, then report (and clear) an expired tensor-core wait as
+// RQ_ERR_TIMEOUT: the read-back paths call this, so a sweep that gave up is never read as
+// if it had finished
+int sync_checked(rq_state* s);
 
 }  // namespace rq
 

@@ -1,6 +1,6 @@
 // rq_mlp.cu -- BF16 tensor-core (tcgen05) GEMMs and the warm-start MLP.
 //
-// The warm start for QAOA angles is a small MLP (276 -> 256 -> 256 -> 8, ReLU,
+// The warm start for QAOA angles is a small MLP (325 -> 256 -> 256 -> 8, ReLU,
 // BF16 weights and activations, FP32 accumulation).  It has no counterpart in
 // the reference (whose run_qaoa always starts from gamma = beta = 0.5,
 // qaoa.rs:221-222); it is trained on angles the batched simulator optimises.
@@ -62,10 +62,15 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 
+// polls before a main-path wait counts as expired (rq_debug_set_wait_limit); the clean-up
+// wait after an expiry always uses WAIT_POLLS
+constexpr uint32_t WAIT_POLLS = 1u << 26;
+__device__ uint32_t g_mma_wait_polls = WAIT_POLLS;
+
 // bounded wait for the mbarrier phase `parity`; false on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t polls = WAIT_POLLS) {
     const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < (1u << 26); ++it) {
+    for (uint32_t it = 0; it < polls; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -172,13 +177,18 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(GemmArgs g) {
                          : "memory");
         }
         // the chunk's MMAs must finish before the buffers are overwritten (and before the epilogue)
-        if (!mbar_wait(&mbar, phase)) {
+        if (!mbar_wait(&mbar, phase, g_mma_wait_polls)) {
             timed_out = 1;
         }
         phase ^= 1u;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         __syncthreads();
-        if (timed_out) break;
+        if (timed_out) {
+            // the MMAs of this chunk may still be in flight: let them land (bounded) before the
+            // shared and tensor memory they use are released
+            if (tid == 0) mbar_wait(&mbar, phase ^ 1u);
+            break;
+        }
     }
 
     if (!timed_out) {
@@ -251,9 +261,16 @@ int gemm_bf16(cudaStream_t stream, const __nv_bfloat16* A, int lda, const __nv_b
 }
 
 int mma_timeout_flag(int* out) {
-    int v = 0;
+    int v = 0, zero = 0;
     RQ_CUDA(cudaMemcpyFromSymbol(&v, g_mma_timeout, sizeof(int)));
+    if (v) RQ_CUDA(cudaMemcpyToSymbol(g_mma_timeout, &zero, sizeof(int)));
     *out = v;
+    return RQ_OK;
+}
+
+int mma_set_wait_polls(uint32_t polls) {
+    const uint32_t v = polls == RQ_WAIT_LIMIT_DEFAULT ? WAIT_POLLS : polls;
+    RQ_CUDA(cudaMemcpyToSymbol(g_mma_wait_polls, &v, sizeof(v)));
     return RQ_OK;
 }
 

@@ -710,6 +710,17 @@ inline void build_program(std::vector<Sweep>& sweeps, uint32_t nq, uint32_t m, u
 constexpr int DENSE_FLOATS = 64 * 64;          // one 64x64 operand image
 constexpr int DENSE_IMAGE_FLOATS = 2 * DENSE_FLOATS;
 
+// FP16 operand images (RQ_EXEC_SWEEP_TC16): the same B, scaled by 2^DENSE_F16_SCALE_LOG2,
+// split into an FP16 high part h = fp16(B') and low part l = fp16(B' - h) (both rounded to
+// nearest even from the f64 product), each 64x64 in the no-swizzle K-major core-matrix
+// layout of 16-bit elements: element (c, k) at byte (c/8)*1024 + (k/8)*128 + (c%8)*16 +
+// (k%8)*2; high part then low part, 8 KB each.
+constexpr int DENSE_F16_SCALE_LOG2 = 14;
+constexpr int DENSE_F16_WORDS = 64 * 64;       // 32-bit words per image (two 8 KB parts)
+
+enum DenseFormat : int { DENSE_TF32 = 0, DENSE_F16 = 1 };
+inline size_t dense_image_words(int fmt) { return fmt == DENSE_F16 ? DENSE_F16_WORDS : DENSE_IMAGE_FLOATS; }
+
 // v <- op(v) on a 32-vector of register amplitudes (the kernel's op semantics); u0 / u1
 // are the values of q0 / q1 when they are not register slots (uniform over a tile)
 inline void apply_op32(const SwOp& o, const double* mt, double* v /* 64: re, im interleaved */, int u0 = 0,
@@ -795,6 +806,51 @@ inline void dense_image(const std::vector<double>& U /* 32 x 32 complex, [col][i
         }
 }
 
+// IEEE binary16 bits of x, rounded to nearest even (subnormals kept; |x| < 65520 here)
+inline uint16_t f16_bits(double x) {
+    const uint16_t sign = std::signbit(x) ? 0x8000u : 0u;
+    const double a = std::fabs(x);
+    if (a == 0.0) return sign;
+    if (a >= 65520.0) return (uint16_t)(sign | 0x7C00u);
+    int e = 0;
+    const double m = std::frexp(a, &e);   // a = m * 2^e, m in [0.5, 1)
+    int E = e - 1;                        // a = (2m) * 2^E
+    if (E < -14) return (uint16_t)(sign | (uint16_t)std::nearbyint(a * 16777216.0));   // units of 2^-24
+    double q = std::nearbyint(m * 2048.0);   // 11 significant bits, in [1024, 2048]
+    if (q == 2048.0) { q = 1024.0; E += 1; }
+    if (E > 15) return (uint16_t)(sign | 0x7C00u);
+    return (uint16_t)(sign | (uint16_t)(((E + 15) << 10) | ((int)q - 1024)));
+}
+
+inline double f16_value(uint16_t h) {
+    const int e = (h >> 10) & 0x1F, f = h & 0x3FF;
+    double v = e == 0 ? std::ldexp((double)f, -24) : std::ldexp((double)(1024 + f), e - 25);
+    return (h & 0x8000u) ? -v : v;
+}
+
+inline size_t dense_offset16(int c, int k) {   // in 16-bit elements
+    return (size_t)(c / 8) * 512 + (size_t)(k / 8) * 64 + (size_t)(c % 8) * 8 + (size_t)(k % 8);
+}
+
+inline void dense_image_f16(const std::vector<double>& U /* as dense_image */, uint32_t* out_words) {
+    uint16_t* out = reinterpret_cast<uint16_t*>(out_words);
+    const double sc = std::ldexp(1.0, DENSE_F16_SCALE_LOG2);
+    for (int col = 0; col < 32; ++col)
+        for (int i = 0; i < 32; ++i) {
+            const double ur = U[(size_t)col * 64 + 2 * i], ui = U[(size_t)col * 64 + 2 * i + 1];
+            const double vals[2][2] = {{ur, -ui}, {ui, ur}};
+            for (int rp = 0; rp < 2; ++rp)
+                for (int r = 0; r < 2; ++r) {
+                    const double x = vals[rp][r] * sc;
+                    const uint16_t hi = f16_bits(x);
+                    const uint16_t lo = f16_bits(x - f16_value(hi));
+                    const size_t off = dense_offset16(2 * i + rp, 2 * col + r);
+                    out[off] = hi;
+                    out[DENSE_F16_WORDS + off] = lo;
+                }
+        }
+}
+
 // Tensor-core plans: every phase becomes one OP_DENSE.  Gate qubits that are register
 // slots index the 32-dimensional space; the other gate qubits are outside the sweep's local
 // set (the phase planner makes every local gate qubit a slot), so their values are fixed
@@ -815,7 +871,9 @@ __host__ __device__ inline uint32_t dense_vq(const SwOp& o, int j) {
 }
 
 inline bool fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& phases, std::vector<SwOp>& ops,
-                       const std::vector<double>& mats, std::vector<float>& images, uint64_t* ndense) {
+                       const std::vector<double>& mats, std::vector<uint32_t>& images, uint64_t* ndense,
+                       int fmt = DENSE_TF32) {
+    const size_t words = dense_image_words(fmt);
     std::vector<SwOp> out;
     std::vector<uint32_t> sweep_of(phases.size(), 0);
     for (size_t d = 0; d < descs.size(); ++d) {
@@ -883,7 +941,7 @@ inline bool fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& ph
         ++*ndense;
     }
     // build the images (the products in f64 and their TF32 split) on the host's cores
-    images.assign(nimg * DENSE_IMAGE_FLOATS, 0.0f);
+    images.assign(nimg * words, 0u);
     auto work = [&](size_t j0, size_t j1) {
         std::vector<double> U(32 * 64);
         for (size_t jj = j0; jj < j1; ++jj) {
@@ -902,7 +960,8 @@ inline bool fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& ph
                     apply_op32(op, mats.data() + 2 * (size_t)op.mat, v, val(op.q0), val(op.q1));
                 }
             }
-            dense_image(U, images.data() + jb.slot * DENSE_IMAGE_FLOATS);
+            if (fmt == DENSE_F16) dense_image_f16(U, images.data() + jb.slot * words);
+            else dense_image(U, reinterpret_cast<float*>(images.data() + jb.slot * words));
         }
     };
     const size_t nt = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), (jobs.size() + 15) / 16));

@@ -261,7 +261,7 @@ int finish(rq_state* s, unsigned nblocks, unsigned stride, unsigned nout, double
     RQ_CUDA(cudaGetLastError());
     RQ_TRY(rq::ensure_hbuf(s, nout));
     RQ_CUDA(cudaMemcpyAsync(s->hbuf, dout, nout * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
-    RQ_CUDA(cudaStreamSynchronize(s->stream));
+    RQ_TRY(rq::sync_checked(s));
     for (unsigned k = 0; k < nout; ++k) host[k] = s->hbuf[k];
     return RQ_OK;
 }
@@ -420,18 +420,47 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 double* g_noalloc_addr[kMaxDevices] = {nullptr};
+unsigned long long g_noalloc_ctx[kMaxDevices] = {0};   // context the address belongs to
+
+// Unique id of the current CUDA context (cuCtxGetId, reached through the runtime's
+// driver entry points so the library needs no libcuda link); 0 when unavailable.
+unsigned long long current_context_id() {
+    using GetCurrent = int (*)(void**);
+    using GetId = int (*)(void*, unsigned long long*);
+    static GetCurrent get_current = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+                       q == cudaDriverEntryPointSuccess ? reinterpret_cast<GetCurrent>(f) : nullptr;
+    }();
+    static GetId get_id = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        return cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+                       q == cudaDriverEntryPointSuccess ? reinterpret_cast<GetId>(f) : nullptr;
+    }();
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
 
 // Device address of g_noalloc_scratch on the current device.  In host code
 // the array's name is only a host-side stand-in, so the address is looked up
-// once per device, with that device current, and cached.
+// with that device current, once per device and context: the first call on a
+// device (and the first call after its context was re-created, for example by
+// cudaDeviceReset, which reloads the module and can move the array) looks it
+// up; later calls reuse it.
 int noalloc_scratch_address(int device, double** out) {
     if (device < 0 || device >= kMaxDevices) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "device index out of range");
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[device]) {
+    const unsigned long long ctx = current_context_id();
+    if (!g_noalloc_addr[device] || ctx == 0 || ctx != g_noalloc_ctx[device]) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return rq::cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
         g_noalloc_addr[device] = static_cast<double*>(p);
+        g_noalloc_ctx[device] = ctx;
     }
     *out = g_noalloc_addr[device];
     return RQ_OK;
@@ -454,6 +483,7 @@ extern "C" int rq_expectation_batch_noalloc(const void* device_amps, uint32_t nu
                                                      std::to_string(RQ_NOALLOC_MAX_STRINGS) + " Pauli strings per call, got " +
                                                      std::to_string(nstrings));
     if (nstrings == 0) return RQ_OK;
+    if (!ops && offsets[nstrings] > offsets[0]) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
     // Pauli strings in mask form (same rules as rq_state_expectation_batch)
     std::vector<rq::PauliMask> terms(nstrings);
     for (uint32_t k = 0; k < nstrings; ++k) {

@@ -171,8 +171,7 @@ int sample(rq_state* s, const uint32_t* qubits, uint32_t nqm, uint64_t base_seed
     cudaFreeAsync(dout, s->stream);
     RQ_CUDA(le);
     RQ_CUDA(ce);
-    RQ_CUDA(cudaStreamSynchronize(s->stream));
-    return RQ_OK;
+    return rq::sync_checked(s);
 }
 
 }  // namespace rq

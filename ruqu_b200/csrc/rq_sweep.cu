@@ -21,6 +21,8 @@
 #include "rq_internal.cuh"
 #include "rq_plan.cuh"
 
+#include <cuda_fp16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -492,6 +494,10 @@ constexpr uint32_t B_LBO = 128;    // bytes between core matrices along K
 constexpr uint32_t COL_D = 0;   // accumulator columns [0, 64 * halves); A follows at col_a = 64 * halves
 
 __device__ int g_tc_timeout = 0;
+// polls of an mbarrier before a main-path wait counts as expired (rq_debug_set_wait_limit);
+// the clean-up waits after an expiry always use WAIT_POLLS
+constexpr uint32_t WAIT_POLLS = 1u << 24;
+__device__ uint32_t g_tc_wait_polls = WAIT_POLLS;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -507,9 +513,9 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
 // TF32 x TF32 -> F32, both operands K-major, M = 128, N = 64
 constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
 
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t polls = WAIT_POLLS) {
     const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < (1u << 24); ++it) {
+    for (uint32_t it = 0; it < polls; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -615,7 +621,7 @@ __device__ __forceinline__ bool commit_wait(TcCtx& c, uint32_t tid) {
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                          smem_u32(c.bar))
                      : "memory");
-    const bool late = !mbar_wait(c.bar, c.parity);
+    const bool late = !mbar_wait(c.bar, c.parity, g_tc_wait_polls);
     c.parity ^= 1u;
     if (__syncthreads_or(late)) {
         c.failed = true;
@@ -634,7 +640,7 @@ __device__ __forceinline__ void dense_op(TcCtx& c, float2* reg, uint32_t tid, ui
     const uint32_t halves = nthreads / 128;
     store_a(c, reg, c.tmem + lane_base + c.col_a + half_col, false);
     // the image copy started at the phase start
-    const bool late = !mbar_wait(c.ibar, c.iparity);
+    const bool late = !mbar_wait(c.ibar, c.iparity, g_tc_wait_polls);
     c.iparity ^= 1u;
     if (__syncthreads_or(late)) {
         c.failed = true;
@@ -819,6 +825,331 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc(float2* __restrict__ amps, 
 }
 
 // ---------------------------------------------------------------------------
+// FP16-split tensor-core sweeps (RQ_EXEC_SWEEP_TC16)
+// ---------------------------------------------------------------------------
+//
+// Same tiles, phases and register rows as k_sweep_tc, with the dense 32x32 op
+// computed as three FP16 MMA passes, D = Ah*Bh + Ah*Bl + Al*Bh, accumulated in
+// FP32 (kind::f16 runs at twice the TF32 rate, and both A parts fit in tensor
+// memory at once, so a phase is one MMA round trip instead of two):
+//
+// * amplitudes are scaled per tile by a power of two 2^s chosen from the
+//   tile's norm (computed in the tile's first phase; the sweep's ops are
+//   unitary on the tile, so the norm bounds every amplitude of every phase):
+//   |a| * 2^s < 2^15 keeps the FP16 high parts inside the FP16 range, and a
+//   small tile gets a large s, so nothing drops into FP16 subnormals early;
+// * a thread's scaled amplitude x splits into h = x rounded to 11 significant
+//   bits (exact in FP16) and l = x - h (exact in FP32, then rounded to FP16):
+//   the split keeps ~22 bits, and the dropped Al*Bl term is ~2^-22 relative,
+//   the same as 3xTF32;
+// * the images hold U * 2^14 as FP16 high and low parts (host-built, f64);
+//   outputs are scaled back by 2^-14 between phases (the tile stays scaled by
+//   2^s) and by 2^-(s+14) in the last phase;
+// * tensor memory per 128-row half: accumulator (64 columns), A high part (32
+//   columns of FP16 pairs: column i = amplitude i, real part in the low 16
+//   bits) and A low part (32 columns);
+// * each half is issued by its own thread (warp 4h, lane 0) with its own
+//   completion mbarrier, so one half's MMAs overlap the other half's
+//   conversion; the CTA meets once per phase (the shared-memory exchange);
+// * operand images are double-buffered: while a phase's MMAs run, the next
+//   phase's image (or the next tile's first image) is already being copied.
+namespace tc16 {
+
+constexpr uint32_t IMG_BYTES = DENSE_F16_WORDS * 4u;   // 16 KB: high + low part
+constexpr uint32_t PART_BYTES = IMG_BYTES / 2;
+constexpr uint32_t B_SBO = 1024;   // bytes between 8-row groups (8 core matrices along K)
+constexpr uint32_t B_LBO = 128;    // bytes between core matrices along K
+// FP16 x FP16 -> F32, both operands K-major, M = 128, N = 64
+constexpr uint32_t IDESC = (1u << 4) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
+    d |= (uint64_t)(B_LBO >> 4) << 16;
+    d |= (uint64_t)(B_SBO >> 4) << 32;
+    d |= (uint64_t)1 << 46;   // sm_100 descriptor version; no swizzle, base offset 0
+    return d;
+}
+
+__device__ __forceinline__ float pow2f(int k) { return __int_as_float((k + 127) << 23); }   // |k| <= 126
+
+__device__ __forceinline__ uint32_t pack_f16x2(float lo_elem, float hi_elem) {
+    const __half2 h = __floats2half2_rn(lo_elem, hi_elem);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+__device__ __forceinline__ void st16u(uint32_t taddr, const uint32_t* v) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+        ::"r"(taddr), "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+        "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+        : "memory");
+}
+
+__device__ __forceinline__ void mma(uint32_t d, uint32_t a, uint64_t bdesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(d), "r"(a), "l"(bdesc), "r"(IDESC), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+__device__ __forceinline__ void start_copy(uint32_t dst, const void* src, uint64_t* bar) {
+    const uint32_t b = tc::smem_u32(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(IMG_BYTES) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(IMG_BYTES), "r"(b)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bar_half(uint32_t half) {   // the 128 threads of one half
+    asm volatile("bar.sync %0, 128;" ::"r"(1u + half) : "memory");
+}
+
+}  // namespace tc16
+
+__global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps, const SweepDesc d,
+                                                     const PhaseDesc* __restrict__ phases,
+                                                     const SwOp* __restrict__ ops,
+                                                     const uint32_t* __restrict__ images, uint64_t ntiles) {
+    using VV = float4;
+    constexpr int NR = 32;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const uint32_t tile_elems = 1u << d.m;
+    float2* sm = reinterpret_cast<float2*>(smem_raw);
+    unsigned char* img = reinterpret_cast<unsigned char*>(sm + tile_elems);   // two image buffers
+    PhaseDesc* sph = reinterpret_cast<PhaseDesc*>(img + 2 * tc16::IMG_BYTES);
+    const uint32_t nph = d.phase_end - d.phase_begin;
+    const uint32_t op0 = phases[d.phase_begin].op_begin, nops = phases[d.phase_end - 1].op_end - op0;
+    SwOp* sop = reinterpret_cast<SwOp*>(sph + nph);
+    __shared__ __align__(8) uint64_t mbar[2], ibar[2];
+    __shared__ uint32_t tmem_base;
+    __shared__ float wsum[8];
+    __shared__ int half_failed[2];
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t T_ = blockDim.x;
+    const uint32_t warp = tid >> 5, half = warp >> 2;
+    for (uint32_t k = tid; k < nph * (uint32_t)(sizeof(PhaseDesc) / 16); k += T_)
+        reinterpret_cast<uint4*>(sph)[k] = reinterpret_cast<const uint4*>(phases + d.phase_begin)[k];
+    for (uint32_t k = tid; k < nops; k += T_) sop[k] = ops[op0 + k];
+    const uint32_t ncols = 128u * (T_ / 128u);
+    if (tid < 32) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(&tmem_base)),
+                     "r"(ncols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int k = 0; k < 2; ++k) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc::smem_u32(&mbar[k])), "r"(1u) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc::smem_u32(&ibar[k])), "r"(1u) : "memory");
+            half_failed[k] = 0;
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base;
+    const PhaseDesc* lph = sph - d.phase_begin;
+    const SwOp* lop = sop - op0;
+    const uint32_t polls = tc::g_tc_wait_polls;
+
+    const uint64_t cmask = (1ull << d.c) - 1;
+    uint64_t dep_tid = 0;
+    {
+        const uint64_t x = (uint64_t)tid * 2;
+        dep_tid = x & cmask;
+        for (uint32_t b = d.c; b < d.m; ++b)
+            if ((x >> b) & 1ull) dep_tid |= 1ull << d.local_global[b];
+    }
+    const uint32_t stid = swz<float>(tid * 2);
+    auto tile_base = [&](uint64_t tile) {
+        uint64_t b = 0;
+        for (uint32_t k = 0; k < d.nonlocal_count; ++k)
+            if ((tile >> k) & 1ull) b |= 1ull << d.nonlocal[k];
+        return b;
+    };
+    // the operand image of phase p for a tile at `base` (its variant: the tile's values of the
+    // phase's qubits outside the tile)
+    auto image_of = [&](uint64_t base, uint32_t p) {
+        const SwOp& op = lop[lph[p].op_begin];
+        uint32_t var = 0;
+        for (int j = 0; j < dense_nvq(op); ++j) var |= (uint32_t)((base >> dense_vq(op, j)) & 1ull) << j;
+        return images + (size_t)(op.mat + var) * DENSE_F16_WORDS;
+    };
+
+    // thread 0 issues every image copy; copies into buffer b complete phases of ibar[b]
+    uint32_t issued[2] = {0u, 0u};   // (thread 0) copies issued into each buffer
+    uint32_t step = 0;               // (tile, phase) steps run by this CTA
+    bool failed = false;
+    bool committed = false;          // (issuing threads) MMAs of the current step in flight
+    const uint32_t col_h = half * 128u;
+    const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
+
+    uint64_t tile = blockIdx.x;
+    uint64_t base = tile < ntiles ? tile_base(tile) : 0;
+    if (tid == 0 && tile < ntiles) {
+        tc16::start_copy(tc::smem_u32(img), image_of(base, d.phase_begin), &ibar[0]);
+        issued[0] = 1;
+    }
+    for (; tile < ntiles && !failed; tile += gridDim.x) {
+        const uint64_t next = tile + gridDim.x;
+        const uint64_t nbase = next < ntiles ? tile_base(next) : 0;
+        issue_tile<float>(sm, amps, d, base, dep_tid, stid);
+        cp_async_commit();
+        cp_async_wait0();
+        __syncthreads();
+        float in_scale = 1.f, mid_scale = tc16::pow2f(-DENSE_F16_SCALE_LOG2), last_scale = 1.f;
+        for (uint32_t p = d.phase_begin; p < d.phase_end; ++p, ++step) {
+            const uint32_t buf = step & 1u;
+            const PhaseDesc& ph = lph[p];
+            // the next step's image into the other buffer (its previous MMAs finished last step)
+            if (tid == 0) {
+                const bool more = p + 1 < d.phase_end;
+                if (more || next < ntiles) {
+                    tc16::start_copy(tc::smem_u32(img + (buf ^ 1u) * tc16::IMG_BYTES),
+                                     more ? image_of(base, p + 1) : image_of(nbase, d.phase_begin), &ibar[buf ^ 1u]);
+                    ++issued[buf ^ 1u];
+                }
+            }
+            uint32_t ebase = 0;
+            for (uint32_t b = 0; b < ph.nt; ++b)
+                if ((tid >> b) & 1u) ebase |= 1u << ph.tbit_local[b];
+            const uint32_t sb = swz<float>(ebase);
+            auto addr = [&](int i, const uint32_t* S) {
+                uint32_t a = sb;
+#pragma unroll
+                for (int k = 0; k < 5; ++k)
+                    if ((i >> k) & 1) a ^= S[k];
+                return a;
+            };
+            float2 reg[NR];
+            {
+                uint32_t S[5];
+#pragma unroll
+                for (int k = 0; k < 5; ++k) S[k] = ph.slut[1 << k];
+#pragma unroll
+                for (int i = 0; i < NR; ++i) reg[i] = sm[addr(i, S)];
+            }
+            if (p == d.phase_begin) {
+                // the tile's norm -> its scale 2^s with |a| * 2^s < 2^15
+                float acc = 0.f;
+#pragma unroll
+                for (int i = 0; i < NR; ++i) acc = fmaf(reg[i].x, reg[i].x, fmaf(reg[i].y, reg[i].y, acc));
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+                if ((tid & 31u) == 0) wsum[warp] = acc;
+                __syncthreads();
+                float n2 = 0.f;
+                for (uint32_t w = 0; w < T_ / 32u; ++w) n2 += wsum[w];
+                int sc = 0;
+                if (n2 > 0.f && n2 < 3.0e38f) {
+                    const int E = (int)((__float_as_uint(n2) >> 23) & 0xFFu) - 127;   // n2 in [2^E, 2^(E+1))
+                    sc = 15 - ((E + 2) >> 1);                                         // sqrt(n2) < 2^((E+2)>>1)
+                    sc = max(-100, min(100, sc));
+                }
+                in_scale = tc16::pow2f(sc);
+                last_scale = tc16::pow2f(-(sc + DENSE_F16_SCALE_LOG2));
+            }
+            const float xs = p == d.phase_begin ? in_scale : 1.f;
+            // A high and low parts into this thread's tensor-memory lane
+            {
+                const uint32_t ta = tmem + lane_base + col_h + 64u;
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    uint32_t hw[16], lw[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const float x = reg[16 * c + j].x * xs, y = reg[16 * c + j].y * xs;
+                        const float hx = tc::to_tf32(x), hy = tc::to_tf32(y);
+                        hw[j] = tc16::pack_f16x2(hx, hy);
+                        lw[j] = tc16::pack_f16x2(x - hx, y - hy);
+                    }
+                    tc16::st16u(ta + 16u * c, hw);
+                    tc16::st16u(ta + 32u + 16u * c, lw);
+                }
+                asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            }
+            tc16::bar_half(half);
+            const uint32_t mpar = step & 1u;
+            if ((tid & 127u) == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                if (tc::mbar_wait(&ibar[buf], (step >> 1) & 1u, polls)) {
+                    const uint32_t bh = tc::smem_u32(img + buf * tc16::IMG_BYTES), bl = bh + tc16::PART_BYTES;
+                    const uint32_t dt = tmem + col_h, ah = tmem + col_h + 64u, al = tmem + col_h + 96u;
+#pragma unroll
+                    for (uint32_t ks = 0; ks < 4; ++ks) tc16::mma(dt, ah + 8u * ks, tc16::sdesc(bh + 256u * ks), ks > 0);
+#pragma unroll
+                    for (uint32_t ks = 0; ks < 4; ++ks) tc16::mma(dt, ah + 8u * ks, tc16::sdesc(bl + 256u * ks), 1u);
+#pragma unroll
+                    for (uint32_t ks = 0; ks < 4; ++ks) tc16::mma(dt, al + 8u * ks, tc16::sdesc(bh + 256u * ks), 1u);
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     tc::smem_u32(&mbar[half]))
+                                 : "memory");
+                    committed = true;
+                } else {
+                    // the image never landed: release this half's waiters and give up
+                    half_failed[half] = 1;
+                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(&mbar[half])) : "memory");
+                }
+            }
+            if (!tc::mbar_wait(&mbar[half], mpar, polls)) failed = true;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (half_failed[half]) failed = true;
+            const bool last = p + 1 == d.phase_end;
+            const float os = last ? last_scale : mid_scale;
+            {
+                const uint32_t taddr = tmem + lane_base + col_h;
+                tc::ld16(taddr, reg);
+                tc::ld16(taddr + 16, reg + 8);
+                tc::ld16(taddr + 32, reg + 16);
+                tc::ld16(taddr + 48, reg + 24);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                uint32_t S[5];
+#pragma unroll
+                for (int k = 0; k < 5; ++k) S[k] = ph.slut[1 << k];
+#pragma unroll
+                for (int i = 0; i < NR; ++i) sm[addr(i, S)] = make_float2(reg[i].x * os, reg[i].y * os);
+            }
+            if (__syncthreads_or(failed)) {
+                failed = true;
+                break;
+            }
+            committed = false;
+        }
+        if (failed) break;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const uint32_t se = stid ^ d.sgj[j];
+            const uint64_t g = base | dep_tid | d.gj[j];
+            const float2 a = sm[se], b = sm[se ^ 1u];
+            __stcs(reinterpret_cast<VV*>(amps + g), make_float4(a.x, a.y, b.x, b.y));
+        }
+        __syncthreads();
+        base = nbase;
+    }
+    if (failed) {
+        if (tid == 0) tc::g_tc_timeout = 1;
+        // let everything still in flight land before the shared and tensor memory are released
+        if ((tid & 127u) == 0 && committed) tc::mbar_wait(&mbar[half], step & 1u);
+        if (tid == 0)
+            for (uint32_t b = 0; b < 2; ++b)
+                if (issued[b]) tc::mbar_wait(&ibar[b], (issued[b] - 1u) & 1u);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid < 32) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host planner
 // ---------------------------------------------------------------------------
 
@@ -923,6 +1254,7 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
             if (gates[k].kind != RQ_GATE_BARRIER) P->gates.push_back(gates[k]);
         P->stats.gates = P->gates.size();
         P->stats.launches = P->gates.size();
+        P->stats.exec_mode = RQ_EXEC_PER_GATE;
         for (auto& g : P->gates) {
             uint64_t b = 2 * S;
             if (g.kind == RQ_GATE_CNOT || g.kind == RQ_GATE_SWAP) b = S;
@@ -953,11 +1285,11 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
     std::vector<SwOp> ops;
     std::vector<double> mats;
     build_program(sweeps, nq, m, c, rb, s->prec == RQ_F32 ? 2 : 1, P->descs, phases, ops, mats, tcp);
-    std::vector<float> images;
+    std::vector<uint32_t> images;
     uint64_t ndense = 0;
     if (tcp) {
         // images resident in shared memory next to one tile
-        if (!fuse_dense(P->descs, phases, ops, mats, images, &ndense)) {
+        if (!fuse_dense(P->descs, phases, ops, mats, images, &ndense, tc_passes == TC_F16 ? DENSE_F16 : DENSE_TF32)) {
             delete P;
             return fail(RQ_ERR_CIRCUIT, "tensor-core plan: a phase touches more than 5 qubits outside the tile");
         }
@@ -975,9 +1307,9 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
     P->off_ops = (P->off_ph + phases.size() * sizeof(PhaseDesc) + 255) & ~size_t(255);
     P->off_mat = (P->off_ops + ops.size() * sizeof(SwOp) + 255) & ~size_t(255);
     P->off_img = (P->off_mat + mats.size() * mat_elem + 255) & ~size_t(255);
-    size_t total = P->off_img + images.size() * sizeof(float);
+    size_t total = P->off_img + images.size() * sizeof(uint32_t);
     std::vector<unsigned char> host(total);
-    if (!images.empty()) std::memcpy(host.data() + P->off_img, images.data(), images.size() * sizeof(float));
+    if (!images.empty()) std::memcpy(host.data() + P->off_img, images.data(), images.size() * sizeof(uint32_t));
     std::memcpy(host.data() + P->off_ph, phases.data(), phases.size() * sizeof(PhaseDesc));
     std::memcpy(host.data() + P->off_ops, ops.data(), ops.size() * sizeof(SwOp));
     if (s->prec == RQ_F32) {
@@ -1004,6 +1336,9 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
     P->stats.ops = ops.size();
     P->stats.dense_ops = ndense;
     P->stats.hbm_bytes = 2 * S * P->descs.size();
+    P->stats.exec_mode = !tcp ? RQ_EXEC_SWEEP : tc_passes == TC_F16 ? RQ_EXEC_SWEEP_TC16
+                                               : tc_passes == 1 ? RQ_EXEC_SWEEP_TC_FAST : RQ_EXEC_SWEEP_TC;
+    P->stats.local_qubits = m;
     *out = P;
     return RQ_OK;
 }
@@ -1082,8 +1417,11 @@ int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes
         rq_plan* plan;
         float ms;
     };
-    std::vector<Cand> cands = {{0, 0, nullptr, 0.f}, {3, 0, nullptr, 0.f}};
-    if (m == 13 && s->nq > 13) cands.push_back({3, 12, nullptr, 0.f});
+    std::vector<Cand> cands = {{0, 0, nullptr, 0.f}, {3, 0, nullptr, 0.f}, {TC_F16, 0, nullptr, 0.f}};
+    if (m == 13 && s->nq > 13) {
+        cands.push_back({3, 12, nullptr, 0.f});
+        cands.push_back({TC_F16, 12, nullptr, 0.f});
+    }
     for (auto& c : cands)
         if (plan_build(s, gates, n, RQ_EXEC_SWEEP, &c.plan, c.passes, 2, c.m) != RQ_OK) {
             if (c.passes == 0) {   // the CUDA-core plan is the reference point
@@ -1122,6 +1460,35 @@ int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes
     return RQ_OK;
 }
 
+// FP16-split tensor-core sweeps: shared memory = tile | two operand images | the sweep's
+// phase and op descriptors; resident CTAs per SM by registers (128 per thread), shared
+// memory (228 KB per SM, 1 KB reserved per CTA) and tensor memory (512 columns per SM).
+static int launch_tc16(rq_state* s, const rq_plan* P, const PhaseDesc* ph, const SwOp* op) {
+    const uint32_t* img = reinterpret_cast<const uint32_t*>(P->dev + P->off_img);
+    const unsigned threads = 1u << (P->descs.front().m - 5);
+    const PhaseDesc* hph = P->host_phases.data();
+    auto smem_of = [&](const SweepDesc& d) {
+        const size_t nph = d.phase_end - d.phase_begin;
+        const size_t nops = hph[d.phase_end - 1].op_end - hph[d.phase_begin].op_begin;
+        return P->smem + 2 * (size_t)tc16::IMG_BYTES + nph * sizeof(PhaseDesc) + nops * sizeof(SwOp);
+    };
+    size_t smem_max = 0;
+    for (const auto& d : P->descs) smem_max = std::max(smem_max, smem_of(d));
+    const int by_regs = 65536 / (128 * (int)threads);
+    const int by_smem = (int)((228u * 1024u) / (smem_max + 1024u + 128u));
+    const int by_tmem = (int)(512u / (128u * (threads / 128u)));
+    const int per_sm = std::min(by_regs, std::min(by_smem, by_tmem));
+    if (per_sm < 1) return fail(RQ_ERR_CUDA, "FP16 tensor-core sweep kernel does not fit on an SM");
+    const unsigned grid = (unsigned)std::min<uint64_t>(P->ntiles, (uint64_t)per_sm * rq::num_sms(s->device));
+    for (const auto& d : P->descs) {
+        const size_t smem = smem_of(d);
+        RQ_CUDA(cudaFuncSetAttribute(k_sweep_tc16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_sweep_tc16<<<grid, threads, smem, s->stream>>>((float2*)s->amps, d, ph, op, img, P->ntiles);
+        RQ_CUDA(cudaGetLastError());
+    }
+    return RQ_OK;
+}
+
 int plan_launch(rq_state* s, const rq_plan* P) {
     if (P->mode == RQ_EXEC_PER_GATE) {
         for (const auto& g : P->gates) RQ_TRY(apply_one_gate(s, g));
@@ -1130,6 +1497,7 @@ int plan_launch(rq_state* s, const rq_plan* P) {
     const PhaseDesc* ph = reinterpret_cast<const PhaseDesc*>(P->dev + P->off_ph);
     const SwOp* op = reinterpret_cast<const SwOp*>(P->dev + P->off_ops);
     const void* mt = P->dev + P->off_mat;
+    if (P->tc_passes == TC_F16) return launch_tc16(s, P, ph, op);
     if (P->tc_passes > 0) {
         const float* img = reinterpret_cast<const float*>(P->dev + P->off_img);
         const size_t img_bytes = (P->tc_passes > 1 ? DENSE_IMAGE_FLOATS : DENSE_FLOATS) * sizeof(float);
@@ -1177,6 +1545,28 @@ void plan_free(rq_plan* P) {
 }
 
 rq_plan_stats plan_stats(const rq_plan* p) { return p->stats; }
+
+int tc_timeout_flag(int* out) {
+    int v = 0, zero = 0;
+    RQ_CUDA(cudaMemcpyFromSymbol(&v, tc::g_tc_timeout, sizeof(int)));
+    if (v) RQ_CUDA(cudaMemcpyToSymbol(tc::g_tc_timeout, &zero, sizeof(int)));
+    *out = v;
+    return RQ_OK;
+}
+
+int sync_checked(rq_state* s) {
+    RQ_CUDA(cudaStreamSynchronize(s->stream));
+    int to = 0;
+    RQ_TRY(tc_timeout_flag(&to));
+    if (to) return fail(RQ_ERR_TIMEOUT, "a tensor-core sweep's bounded device wait expired; the state is invalid");
+    return RQ_OK;
+}
+
+int tc_set_wait_polls(uint32_t polls) {
+    const uint32_t v = polls == RQ_WAIT_LIMIT_DEFAULT ? tc::WAIT_POLLS : polls;
+    RQ_CUDA(cudaMemcpyToSymbol(tc::g_tc_wait_polls, &v, sizeof(v)));
+    return RQ_OK;
+}
 
 bool plan_fits(const rq_plan* p, const rq_state* s) {
     return p->nq == s->nq && p->prec == s->prec && p->device == s->device;

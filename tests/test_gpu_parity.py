@@ -6,6 +6,7 @@ complex f32 states (at up to 20 qubits); expectation values and energies
 shot bitstrings, cut values and histograms bit-exact.
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -314,13 +315,76 @@ def test_sweep_equals_per_gate_24q_f32():
     assert abs(b.norm_sq() - 1) < 1e-4
 
 
-def test_26q_f64_against_oracle():
-    """Random-layer circuit at 26 qubits (seed 1), f64 GPU vs the oracle (its
-    multi-core kernels compute each amplitude exactly like the scalar ones)."""
-    n, layers = 26, 3
+class _DeviceArray:
+    def __init__(self, ptr, count, typestr):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def _device_amplitudes(state, n, prec):
+    """The state's amplitudes as a complex torch tensor on the device (no host copy)."""
+    import torch
+    ptr, _ = state.device_pointer()
+    state.synchronize()
+    t = torch.as_tensor(_DeviceArray(ptr, 2 << n, "<f4" if prec == "f32" else "<f8"), device="cuda")
+    return torch.view_as_complex(t.view(-1, 2))
+
+
+def _golden_26q():
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "random_layers_26q_seed1.npz")
+    return np.load(path)
+
+
+@pytest.mark.parametrize("prec,mode", [("f64", rq.RQ_EXEC_SWEEP), ("f64", rq.RQ_EXEC_PER_GATE),
+                                       ("f32", rq.RQ_EXEC_SWEEP_TC), ("f32", rq.RQ_EXEC_SWEEP_TC16)])
+def test_26q_20_layers_against_oracle_fixture(prec, mode):
+    """The config's oracle check at 26 qubits: the 20-layer, seed-1 random-layer circuit
+    (1,300 gates) against the oracle's f64 state (tests/golden/random_layers_26q_seed1.npz,
+    made by make_random_layers_26q.py): 16,384 sampled amplitudes, <Z_q> of every qubit and
+    the norms of 256 blocks of 2^18 amplitudes.  Tolerances: f64 (CUDA-core sweeps and the
+    unfused per-gate kernels) 1e-12 on amplitudes and 1e-10 on the sums; f32 through the
+    tensor-core sweeps (3xTF32 and the FP16 split) 1e-5 on amplitudes and on the sums."""
+    import torch
+    f = _golden_26q()
+    n, layers, seed = (int(x) for x in f["meta"])
+    gates = workloads.random_layer_circuit(n, layers, seed)
+    g = QuantumState(n, 0, prec)
+    g.apply_gates(gates, mode)
+    a = _device_amplitudes(g, n, prec)
+    idx = torch.as_tensor(f["indices"], device="cuda")
+    got = a[idx].to(torch.complex128).cpu().numpy()
+    amp_tol, sum_tol = (1e-12, 1e-10) if prec == "f64" else (1e-5, 1e-5)
+    assert float(np.max(np.abs(got - f["amps"]))) < amp_tol
+    p = a.real.double() ** 2 + a.imag.double() ** 2
+    blocks = p.view(256, -1).sum(dim=1).cpu().numpy()
+    assert float(np.max(np.abs(blocks - f["blocks"]))) < sum_tol
+    z = []
+    for q in range(n):
+        v = p.view(-1, 2, 1 << q)
+        z.append(float(v[:, 0, :].sum() - v[:, 1, :].sum()))
+    assert float(np.max(np.abs(np.array(z) - f["z"]))) < sum_tol
+
+
+@pytest.mark.parametrize("mode", [rq.RQ_EXEC_SWEEP_TC, rq.RQ_EXEC_SWEEP_TC16])
+def test_30q_tensor_core_f32_against_f64_sweep(mode):
+    """The benchmark circuit itself (30 qubits, 20 layers, seed 1): the f32 tensor-core
+    sweeps against the complex f64 CUDA-core sweep of the same circuit (the oracle would
+    take hours at 2^30 amplitudes; the f64 sweep is pinned to it at 26 qubits above), max-abs
+    over all 2^30 amplitudes below 1e-6 and the norm within 1e-6."""
+    import torch
+    n, layers = 30, 20
     gates = workloads.random_layer_circuit(n, layers, 1)
-    o = oracle.OracleState(n, oracle.RQ_F64, 0)
-    o.apply(gates, parallel=True)
-    g = QuantumState(n, 0, "f64")
-    g.apply_gates(gates)
-    assert _maxdiff(g, o) < 1e-12
+    ref = QuantumState(n, 0, "f64")
+    ref.apply_gates(gates, rq.RQ_EXEC_SWEEP)
+    g = QuantumState(n, 0, "f32")
+    g.apply_gates(gates, mode)
+    a = _device_amplitudes(g, n, "f32")
+    b = _device_amplitudes(ref, n, "f64")
+    worst, norm = 0.0, 0.0
+    chunk = 1 << 26
+    for k in range(0, 1 << n, chunk):
+        x = a[k:k + chunk].to(torch.complex128)
+        worst = max(worst, float((x - b[k:k + chunk]).abs().max()))
+        norm += float((x.real ** 2 + x.imag ** 2).sum())
+    assert worst < 1e-6, worst
+    assert abs(norm - 1.0) < 1e-6

@@ -1,10 +1,12 @@
-"""Tensor-core sweeps (RQ_EXEC_SWEEP_TC / _FAST) vs the oracle (needs a GPU).
+"""Tensor-core sweeps (RQ_EXEC_SWEEP_TC / _FAST / _TC16) vs the oracle (needs a GPU).
 
-Each phase's slot-local gate run is one dense 32x32 complex unitary applied as
-TF32 MMAs on the tensor cores.  3xTF32 keeps FP32-level accuracy: amplitudes
-max-abs 1e-5 against the oracle's f64 state (the f32 bar), as the CUDA-core
-sweep.  One TF32 pass carries 10-bit operand mantissas: its bar is 1e-4
-max-abs at up to 20 qubits, and the norm stays within 1e-3.
+Each phase's slot-local gate run is one dense 32x32 complex unitary applied on
+the tensor cores: as 3xTF32 MMAs (RQ_EXEC_SWEEP_TC), one TF32 pass (_FAST), or
+three FP16 passes of per-tile-scaled high/low splits (_TC16).  3xTF32 and the
+FP16 split keep FP32-level accuracy: amplitudes max-abs 1e-5 against the
+oracle's f64 state (the f32 bar), as the CUDA-core sweep.  One TF32 pass
+carries 10-bit operand mantissas: its bar is 1e-4 max-abs at up to 20 qubits,
+and the norm stays within 1e-3.
 """
 import math
 
@@ -38,12 +40,16 @@ def _oracle_f64(n, gates):
     return o.amplitudes()
 
 
+MODES = [rq.RQ_EXEC_SWEEP_TC, rq.RQ_EXEC_SWEEP_TC16]
+
+
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("n", [12, 13, 14, 17])
-def test_tc_random_layers_match_oracle(n):
+def test_tc_random_layers_match_oracle(n, mode):
     gates = workloads.random_layer_circuit(n, 8, n)
     ref = _oracle_f64(n, gates)
     g = QuantumState(n, 0, "f32")
-    plan = rq.Plan(g, gates, rq.RQ_EXEC_SWEEP_TC)
+    plan = rq.Plan(g, gates, mode)
     st = plan.stats()
     assert st["dense_ops"] > 0
     plan.execute(g)
@@ -51,13 +57,14 @@ def test_tc_random_layers_match_oracle(n):
     assert err < 1e-5, err
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("n", [12, 15, 18])
-def test_tc_mixed_gates_match_oracle(n):
+def test_tc_mixed_gates_match_oracle(n, mode):
     """Every gate kind, controls and diagonals on thread bits (deferred past the dense op)."""
     gates = _mixed_circuit(n, 400, 100 + n)
     ref = _oracle_f64(n, gates)
     g = QuantumState(n, 0, "f32")
-    g.apply_gates(gates, rq.RQ_EXEC_SWEEP_TC)
+    g.apply_gates(gates, mode)
     assert float(np.max(np.abs(g.state_vector() - ref))) < 1e-5
 
 
@@ -75,13 +82,56 @@ def test_tc_fast_20q_random_layers():
     assert float(np.max(np.abs(h.state_vector() - ref))) < 1e-5
 
 
-def test_tc_plan_replays_and_equals_cuda_sweep_24q():
+def test_tc16_20q_random_layers_config1_circuit():
+    """The 20-qubit, 40-layer, seed-0 random-layer circuit on complex f32 with the FP16-split
+    dense ops: max-abs 1e-5 against the oracle's f64 amplitudes, norm within 1e-5."""
+    n = 20
+    gates = workloads.random_layer_circuit(n, 40, 0)
+    ref = _oracle_f64(n, gates)
+    g = QuantumState(n, 0, "f32")
+    plan = rq.Plan(g, gates, rq.RQ_EXEC_SWEEP_TC16)
+    assert plan.stats()["dense_ops"] > 0
+    plan.execute(g)
+    v = g.state_vector()
+    assert float(np.max(np.abs(v - ref))) < 1e-5
+    assert abs(float(np.vdot(v, v).real) - 1.0) < 1e-5
+
+
+def test_tc16_scales_each_tile_unnormalised_and_tiny_tiles():
+    """The FP16 split scales every tile by a power of two from its norm: a state of norm 40
+    (amplitudes far outside the FP16 range once scaled for a unit state) and a state whose
+    upper half is 1e-30 of its lower half both keep FP32-level relative accuracy."""
+    n = 16
+    gates = workloads.random_layer_circuit(n, 6, 9)
+    r = np.random.default_rng(3)
+    for kind in ("large", "tiny"):
+        a = r.normal(size=1 << n) + 1j * r.normal(size=1 << n)
+        a /= np.linalg.norm(a)
+        if kind == "large":
+            a *= 40.0
+        else:
+            a[1 << (n - 1):] *= 1e-30
+        o = oracle.OracleState.from_amplitudes(a, n, oracle.RQ_F64)
+        o.apply(gates)
+        ref = o.amplitudes()
+        g = QuantumState.from_amplitudes(a, n, "f32")
+        g.apply_gates(gates, rq.RQ_EXEC_SWEEP_TC16)
+        v = g.state_vector()
+        scale = float(np.max(np.abs(ref)))
+        assert float(np.max(np.abs(v - ref))) < 1e-5 * scale, kind
+        if kind == "tiny":   # the tiles of the small half, relative to their own size
+            lo = slice(1 << (n - 1), None)
+            assert float(np.max(np.abs(v[lo] - ref[lo]))) < 1e-5 * float(np.max(np.abs(ref[lo])))
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_tc_plan_replays_and_equals_cuda_sweep_24q(mode):
     n = 24
     gates = workloads.random_layer_circuit(n, 6, 5)
     a = QuantumState(n, 0, "f32")
     b = QuantumState(n, 0, "f32")
     pa = rq.Plan(a, gates, rq.RQ_EXEC_SWEEP)
-    pb = rq.Plan(b, gates, rq.RQ_EXEC_SWEEP_TC)
+    pb = rq.Plan(b, gates, mode)
     for _ in range(2):
         a.reset()
         b.reset()

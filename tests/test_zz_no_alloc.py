@@ -61,6 +61,45 @@ def test_noalloc_matches_allocating_entry_point(prec):
     assert rc3 == 0 and np.max(np.abs(got3 - want1[:7])) < TOL[prec]
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("n", [1, 2])
+def test_noalloc_small_states_where_most_blocks_get_no_work(prec, n):
+    """With 2 or 4 amplitudes nearly every reduction block has no element: each still
+    writes a zero partial, so the sums never pick up what an earlier call left in the
+    shared scratch (a 16-qubit call first fills it with non-zero partials)."""
+    big = QuantumState(16, 0, prec)
+    big.apply_gates(workloads.random_layer_circuit(16, 2, 4))
+    bptr, bstream = big.device_pointer()
+    big.synchronize()
+    fill = _strings(16, 64, 5)
+    rc0, _ = _noalloc(bptr, 16, prec, fill, bstream)
+    assert rc0 == 0, _capi.last_error()
+    st = QuantumState(n, 0, prec)
+    st.apply_gates([(9, 0, 0, 0.7), (10, n - 1, 0, 1.3)])   # Ry(0.7) q0, Rz(1.3) q(n-1)
+    ptr, stream = st.device_pointer()
+    st.synchronize()
+    strings = [[], [(0, 3)], [(0, 1)], [(0, 2)], [(n - 1, 3)], [(0, 1), (n - 1, 3)]]
+    for _ in range(2):
+        rc, got = _noalloc(ptr, n, prec, strings, stream)
+        assert rc == 0, _capi.last_error()
+        want = st.expectation_values(strings)
+        assert np.max(np.abs(got - want)) < TOL[prec]
+
+
+def test_noalloc_rejects_null_ops_for_non_empty_strings():
+    n = 4
+    st = QuantumState(n, 0, "f64")
+    ptr, stream = st.device_pointer()
+    st.synchronize()
+    off = np.array([0, 1], dtype=np.uint32)
+    out = np.full(1, np.nan)
+    rc = _capi.lib.rq_expectation_batch_noalloc(
+        C.c_void_p(ptr), n, _capi.RQ_F64, None, off.ctypes.data_as(C.POINTER(C.c_uint32)), 1,
+        out.ctypes.data_as(C.POINTER(C.c_double)), C.c_void_p(stream))
+    assert rc == _capi.RQ_ERR_INVALID_ARGUMENT
+    assert np.isnan(out).all()
+
+
 def test_noalloc_rejects_more_strings_than_its_scratch_holds():
     n = 10
     st = QuantumState(n, 0, "f64")
