@@ -833,11 +833,16 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc(float2* __restrict__ amps, 
 // FP32 (kind::f16 runs at twice the TF32 rate, and both A parts fit in tensor
 // memory at once, so a phase is one MMA round trip instead of two):
 //
-// * amplitudes are scaled per tile by a power of two 2^s chosen from the
-//   tile's norm (computed in the tile's first phase; the sweep's ops are
-//   unitary on the tile, so the norm bounds every amplitude of every phase):
-//   |a| * 2^s < 2^15 keeps the FP16 high parts inside the FP16 range, and a
-//   small tile gets a large s, so nothing drops into FP16 subnormals early;
+// * amplitudes are scaled per tile by a power of two 2^s chosen in the tile's
+//   first phase from its largest component M: the tile's norm is at most
+//   2^(m/2) M, the ops are unitary on the tile, so no component of any phase
+//   exceeds that norm, and 2^(m/2) M 2^s <= 2^15 keeps every FP16 high part
+//   in range; a small tile gets a large s, so nothing drops into FP16
+//   subnormals early;
+// * the last phase restores the tile's norm (measured on the scaled inputs in
+//   the first phase): the phases are unitary on the tile, and the tensor
+//   cores' FP32 accumulation rounds partial sums toward zero, which would
+//   otherwise shrink every amplitude by ~1e-7 per phase;
 // * a thread's scaled amplitude x splits into h = x rounded to 11 significant
 //   bits (exact in FP16) and l = x - h (exact in FP32, then rounded to FP16):
 //   the split keeps ~22 bits, and the dropped Al*Bl term is ~2^-22 relative,
@@ -925,7 +930,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
     SwOp* sop = reinterpret_cast<SwOp*>(sph + nph);
     __shared__ __align__(8) uint64_t mbar[2], ibar[2];
     __shared__ uint32_t tmem_base;
-    __shared__ float wsum[8];
+    __shared__ float wmax[8], wsum[8], wsum2[8];
     __shared__ int half_failed[2];
 
     const uint32_t tid = threadIdx.x;
@@ -1035,25 +1040,27 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
                 for (int i = 0; i < NR; ++i) reg[i] = sm[addr(i, S)];
             }
             if (p == d.phase_begin) {
-                // the tile's norm -> its scale 2^s with |a| * 2^s < 2^15
-                float acc = 0.f;
+                // the tile's largest component M < 2^(E+1) bounds its norm by 2^(m/2) M, and the
+                // norm bounds every component of every later phase (unitary on the tile): the
+                // scale 2^s with 2^(m/2) M 2^s <= 2^15 keeps all FP16 high parts in range
+                float mx = 0.f;
 #pragma unroll
-                for (int i = 0; i < NR; ++i) acc = fmaf(reg[i].x, reg[i].x, fmaf(reg[i].y, reg[i].y, acc));
+                for (int i = 0; i < NR; ++i) mx = fmaxf(mx, fmaxf(fabsf(reg[i].x), fabsf(reg[i].y)));
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
-                if ((tid & 31u) == 0) wsum[warp] = acc;
+                for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
+                if ((tid & 31u) == 0) wmax[warp] = mx;
                 __syncthreads();
-                float n2 = 0.f;
-                for (uint32_t w = 0; w < T_ / 32u; ++w) n2 += wsum[w];
+                for (uint32_t w = 0; w < T_ / 32u; ++w) mx = fmaxf(mx, wmax[w]);
                 int sc = 0;
-                if (n2 > 0.f && n2 < 3.0e38f) {
-                    const int E = (int)((__float_as_uint(n2) >> 23) & 0xFFu) - 127;   // n2 in [2^E, 2^(E+1))
-                    sc = 15 - ((E + 2) >> 1);                                         // sqrt(n2) < 2^((E+2)>>1)
-                    sc = max(-100, min(100, sc));
+                if (mx > 0.f && mx < 3.0e38f) {
+                    const int E = (int)((__float_as_uint(mx) >> 23) & 0xFFu) - 127;   // mx in [2^E, 2^(E+1))
+                    sc = max(-100, min(100, 14 - E - (int)((d.m + 1) / 2)));
                 }
                 in_scale = tc16::pow2f(sc);
                 last_scale = tc16::pow2f(-(sc + DENSE_F16_SCALE_LOG2));
             }
+            const bool first = p == d.phase_begin;
+            float n2 = 0.f;   // first phase: this thread's part of the scaled tile's norm^2
             const float xs = p == d.phase_begin ? in_scale : 1.f;
             // A high and low parts into this thread's tensor-memory lane
             {
@@ -1064,6 +1071,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
                         const float x = reg[16 * c + j].x * xs, y = reg[16 * c + j].y * xs;
+                        if (first) n2 = fmaf(x, x, fmaf(y, y, n2));
                         const float hx = tc::to_tf32(x), hy = tc::to_tf32(y);
                         hw[j] = tc16::pack_f16x2(hx, hy);
                         lw[j] = tc16::pack_f16x2(x - hx, y - hy);
@@ -1074,6 +1082,11 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
                 asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             }
+            if (first) {   // per-warp sums; read in the last phase, after this phase's CTA barrier
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) n2 += __shfl_xor_sync(0xFFFFFFFFu, n2, o);
+                if ((tid & 31u) == 0) wsum[warp] = n2;
+            }
             tc16::bar_half(half);
             const uint32_t mpar = step & 1u;
             if ((tid & 127u) == 0) {
@@ -1081,12 +1094,14 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
                 if (tc::mbar_wait(&ibar[buf], (step >> 1) & 1u, polls)) {
                     const uint32_t bh = tc::smem_u32(img + buf * tc16::IMG_BYTES), bl = bh + tc16::PART_BYTES;
                     const uint32_t dt = tmem + col_h, ah = tmem + col_h + 64u, al = tmem + col_h + 96u;
+                    // the small correction products first, then the large one on top of them:
+                    // fewer additions into a large running sum, where the accumulator rounds
 #pragma unroll
-                    for (uint32_t ks = 0; ks < 4; ++ks) tc16::mma(dt, ah + 8u * ks, tc16::sdesc(bh + 256u * ks), ks > 0);
+                    for (uint32_t ks = 0; ks < 4; ++ks) tc16::mma(dt, al + 8u * ks, tc16::sdesc(bh + 256u * ks), ks > 0);
 #pragma unroll
                     for (uint32_t ks = 0; ks < 4; ++ks) tc16::mma(dt, ah + 8u * ks, tc16::sdesc(bl + 256u * ks), 1u);
 #pragma unroll
-                    for (uint32_t ks = 0; ks < 4; ++ks) tc16::mma(dt, al + 8u * ks, tc16::sdesc(bh + 256u * ks), 1u);
+                    for (uint32_t ks = 0; ks < 4; ++ks) tc16::mma(dt, ah + 8u * ks, tc16::sdesc(bh + 256u * ks), 1u);
                     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                      tc::smem_u32(&mbar[half]))
                                  : "memory");
@@ -1101,7 +1116,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (half_failed[half]) failed = true;
             const bool last = p + 1 == d.phase_end;
-            const float os = last ? last_scale : mid_scale;
+            float os = last ? last_scale : mid_scale;
             {
                 const uint32_t taddr = tmem + lane_base + col_h;
                 tc::ld16(taddr, reg);
@@ -1110,6 +1125,23 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
                 tc::ld16(taddr + 48, reg + 24);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                if (last) {
+                    // the phases are unitary on the tile: give it back the norm it was loaded with
+                    float acc = 0.f;
+#pragma unroll
+                    for (int i = 0; i < NR; ++i) acc = fmaf(reg[i].x, reg[i].x, fmaf(reg[i].y, reg[i].y, acc));
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+                    if ((tid & 31u) == 0) wsum2[warp] = acc;
+                    __syncthreads();
+                    float out2 = 0.f, in2 = 0.f;
+                    for (uint32_t w = 0; w < T_ / 32u; ++w) {
+                        out2 += wsum2[w];
+                        in2 += wsum[w];
+                    }
+                    in2 *= (float)(1u << (2 * DENSE_F16_SCALE_LOG2));   // outputs carry the images' 2^14 too
+                    if (out2 > 0.f && in2 > 0.f && out2 < 3.0e38f && in2 < 3.0e38f) os *= sqrtf(in2 / out2);
+                }
                 uint32_t S[5];
 #pragma unroll
                 for (int k = 0; k < 5; ++k) S[k] = ph.slut[1 << k];
