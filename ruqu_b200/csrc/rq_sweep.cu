@@ -912,6 +912,50 @@ __device__ __forceinline__ void bar_half(uint32_t half) {   // the 128 threads o
     asm volatile("bar.sync %0, 128;" ::"r"(1u + half) : "memory");
 }
 
+// index of the lowest set bit of 1 <= g < 32 (the Gray-code bit that flips at step g)
+__host__ __device__ constexpr int ctz5(int g) { return (g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : (g & 8) ? 3 : 4; }
+
+// packed FP32x2 arithmetic (one instruction for both lanes of a complex value)
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+    float2 r;
+    asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    float2 r;
+    asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    float2 r;
+    asm("{.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mov.b64 rc, {%6, %7};\n\tfma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return r;
+}
+
+// bounded wait that lets the thread sleep until the phase completes (or 20 us pass) between
+// polls, so waiting warps take no issue slots from the working ones
+__device__ __forceinline__ bool wait_sleep(uint64_t* bar, uint32_t parity, uint32_t polls) {
+    const uint32_t a = tc::smem_u32(bar);
+    for (uint32_t it = 0; it < polls; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity), "r"(20000u)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 }  // namespace tc16
 
 __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps, const SweepDesc d,
@@ -960,7 +1004,8 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
     const uint32_t tmem = tmem_base;
     const PhaseDesc* lph = sph - d.phase_begin;
     const SwOp* lop = sop - op0;
-    const uint32_t polls = tc::g_tc_wait_polls;
+    // each poll may sleep up to 20 us: 2^-7 of the polls of the spinning kernels (~2.6 s in all)
+    const uint32_t hpolls = tc::g_tc_wait_polls >> 7;
 
     const uint64_t cmask = (1ull << d.c) - 1;
     uint64_t dep_tid = 0;
@@ -1007,7 +1052,8 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
         cp_async_commit();
         cp_async_wait0();
         __syncthreads();
-        float in_scale = 1.f, mid_scale = tc16::pow2f(-DENSE_F16_SCALE_LOG2), last_scale = 1.f;
+        const float mid_scale = tc16::pow2f(-DENSE_F16_SCALE_LOG2);
+        float last_scale = 1.f;
         for (uint32_t p = d.phase_begin; p < d.phase_end; ++p, ++step) {
             const uint32_t buf = step & 1u;
             const PhaseDesc& ph = lph[p];
@@ -1020,26 +1066,35 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
                     ++issued[buf ^ 1u];
                 }
             }
+            const bool first = p == d.phase_begin;
+            const bool last = p + 1 == d.phase_end;
+            // this thread's row: thread bit b sits at local bit tbit_local[b]
             uint32_t ebase = 0;
-            for (uint32_t b = 0; b < ph.nt; ++b)
-                if ((tid >> b) & 1u) ebase |= 1u << ph.tbit_local[b];
-            const uint32_t sb = swz<float>(ebase);
-            auto addr = [&](int i, const uint32_t* S) {
-                uint32_t a = sb;
+            {
+                const uint32_t* tb = reinterpret_cast<const uint32_t*>(ph.tbit_local);
+                const uint32_t w0 = tb[0], w1 = tb[1];
 #pragma unroll
-                for (int k = 0; k < 5; ++k)
-                    if ((i >> k) & 1) a ^= S[k];
-                return a;
-            };
+                for (uint32_t b = 0; b < 8; ++b) {
+                    const uint32_t lb = ((b < 4 ? w0 : w1) >> (8 * (b & 3u))) & 0xFFu;
+                    if (b < ph.nt && ((tid >> b) & 1u)) ebase |= 1u << lb;
+                }
+            }
+            const uint32_t sb = swz<float>(ebase);
+            // register i sits at sb ^ (XOR of S[k] over the set bits k of i); visiting the
+            // registers in Gray-code order makes each address one XOR from the previous one
+            uint32_t S[5];
+#pragma unroll
+            for (int k = 0; k < 5; ++k) S[k] = ph.slut[1 << k];
             float2 reg[NR];
             {
-                uint32_t S[5];
+                uint32_t a = sb;
 #pragma unroll
-                for (int k = 0; k < 5; ++k) S[k] = ph.slut[1 << k];
-#pragma unroll
-                for (int i = 0; i < NR; ++i) reg[i] = sm[addr(i, S)];
+                for (int g = 0; g < NR; ++g) {
+                    if (g) a ^= S[tc16::ctz5(g)];
+                    reg[g ^ (g >> 1)] = sm[a];
+                }
             }
-            if (p == d.phase_begin) {
+            if (first) {
                 // the tile's largest component M < 2^(E+1) bounds its norm by 2^(m/2) M, and the
                 // norm bounds every component of every later phase (unitary on the tile): the
                 // scale 2^s with 2^(m/2) M 2^s <= 2^15 keeps all FP16 high parts in range
@@ -1056,13 +1111,20 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
                     const int E = (int)((__float_as_uint(mx) >> 23) & 0xFFu) - 127;   // mx in [2^E, 2^(E+1))
                     sc = max(-100, min(100, 14 - E - (int)((d.m + 1) / 2)));
                 }
-                in_scale = tc16::pow2f(sc);
                 last_scale = tc16::pow2f(-(sc + DENSE_F16_SCALE_LOG2));
+                const float2 s2 = make_float2(tc16::pow2f(sc), tc16::pow2f(sc));
+                float2 n2 = make_float2(0.f, 0.f);   // the scaled tile's norm^2, this thread's part
+#pragma unroll
+                for (int i = 0; i < NR; ++i) {
+                    reg[i] = tc16::mul2(reg[i], s2);
+                    n2 = tc16::fma2(reg[i], reg[i], n2);
+                }
+                float n = n2.x + n2.y;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xFFFFFFFFu, n, o);
+                if ((tid & 31u) == 0) wsum[warp] = n;   // read at the tile's store, after later CTA barriers
             }
-            const bool first = p == d.phase_begin;
-            float n2 = 0.f;   // first phase: this thread's part of the scaled tile's norm^2
-            const float xs = p == d.phase_begin ? in_scale : 1.f;
-            // A high and low parts into this thread's tensor-memory lane
+            // A high part h = fp16(x) and low part fp16(x - h) into this thread's tensor-memory lane
             {
                 const uint32_t ta = tmem + lane_base + col_h + 64u;
 #pragma unroll
@@ -1070,11 +1132,11 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
                     uint32_t hw[16], lw[16];
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
-                        const float x = reg[16 * c + j].x * xs, y = reg[16 * c + j].y * xs;
-                        if (first) n2 = fmaf(x, x, fmaf(y, y, n2));
-                        const float hx = tc::to_tf32(x), hy = tc::to_tf32(y);
-                        hw[j] = tc16::pack_f16x2(hx, hy);
-                        lw[j] = tc16::pack_f16x2(x - hx, y - hy);
+                        const float2 x = reg[16 * c + j];
+                        const __half2 h = __float22half2_rn(x);
+                        const __half2 l = __float22half2_rn(tc16::sub2(x, __half22float2(h)));
+                        hw[j] = *reinterpret_cast<const uint32_t*>(&h);
+                        lw[j] = *reinterpret_cast<const uint32_t*>(&l);
                     }
                     tc16::st16u(ta + 16u * c, hw);
                     tc16::st16u(ta + 32u + 16u * c, lw);
@@ -1082,16 +1144,11 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
                 asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             }
-            if (first) {   // per-warp sums; read in the last phase, after this phase's CTA barrier
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) n2 += __shfl_xor_sync(0xFFFFFFFFu, n2, o);
-                if ((tid & 31u) == 0) wsum[warp] = n2;
-            }
             tc16::bar_half(half);
             const uint32_t mpar = step & 1u;
             if ((tid & 127u) == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                if (tc::mbar_wait(&ibar[buf], (step >> 1) & 1u, polls)) {
+                if (tc16::wait_sleep(&ibar[buf], (step >> 1) & 1u, hpolls)) {
                     const uint32_t bh = tc::smem_u32(img + buf * tc16::IMG_BYTES), bl = bh + tc16::PART_BYTES;
                     const uint32_t dt = tmem + col_h, ah = tmem + col_h + 64u, al = tmem + col_h + 96u;
                     // the small correction products first, then the large one on top of them:
@@ -1112,11 +1169,9 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
                     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(&mbar[half])) : "memory");
                 }
             }
-            if (!tc::mbar_wait(&mbar[half], mpar, polls)) failed = true;
+            if (!tc16::wait_sleep(&mbar[half], mpar, hpolls)) failed = true;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (half_failed[half]) failed = true;
-            const bool last = p + 1 == d.phase_end;
-            float os = last ? last_scale : mid_scale;
             {
                 const uint32_t taddr = tmem + lane_base + col_h;
                 tc::ld16(taddr, reg);
@@ -1125,28 +1180,23 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
                 tc::ld16(taddr + 48, reg + 24);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                 asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                if (last) {
-                    // the phases are unitary on the tile: give it back the norm it was loaded with
-                    float acc = 0.f;
+                if (last) {   // the tile's output norm^2, this thread's part (see the store)
+                    float2 o2 = make_float2(0.f, 0.f);
 #pragma unroll
-                    for (int i = 0; i < NR; ++i) acc = fmaf(reg[i].x, reg[i].x, fmaf(reg[i].y, reg[i].y, acc));
+                    for (int i = 0; i < NR; ++i) o2 = tc16::fma2(reg[i], reg[i], o2);
+                    float o = o2.x + o2.y;
 #pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
-                    if ((tid & 31u) == 0) wsum2[warp] = acc;
-                    __syncthreads();
-                    float out2 = 0.f, in2 = 0.f;
-                    for (uint32_t w = 0; w < T_ / 32u; ++w) {
-                        out2 += wsum2[w];
-                        in2 += wsum[w];
-                    }
-                    in2 *= (float)(1u << (2 * DENSE_F16_SCALE_LOG2));   // outputs carry the images' 2^14 too
-                    if (out2 > 0.f && in2 > 0.f && out2 < 3.0e38f && in2 < 3.0e38f) os *= sqrtf(in2 / out2);
+                    for (int k = 16; k > 0; k >>= 1) o += __shfl_xor_sync(0xFFFFFFFFu, o, k);
+                    if ((tid & 31u) == 0) wsum2[warp] = o;
                 }
-                uint32_t S[5];
+                const float os = last ? last_scale : mid_scale;
+                const float2 os2 = make_float2(os, os);
+                uint32_t a = sb;
 #pragma unroll
-                for (int k = 0; k < 5; ++k) S[k] = ph.slut[1 << k];
-#pragma unroll
-                for (int i = 0; i < NR; ++i) sm[addr(i, S)] = make_float2(reg[i].x * os, reg[i].y * os);
+                for (int g = 0; g < NR; ++g) {
+                    if (g) a ^= S[tc16::ctz5(g)];
+                    sm[a] = tc16::mul2(reg[g ^ (g >> 1)], os2);
+                }
             }
             if (__syncthreads_or(failed)) {
                 failed = true;
@@ -1155,11 +1205,25 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
             committed = false;
         }
         if (failed) break;
+        // The phases are unitary on the tile, so its norm is what it was when loaded; the
+        // tensor cores' FP32 accumulation rounds partial sums toward zero and would shrink it
+        // by ~1e-7 per phase.  The store gives the tile its loaded norm back.
+        float fix = 1.f;
+        {
+            float in2 = 0.f, out2 = 0.f;
+            for (uint32_t w = 0; w < T_ / 32u; ++w) {
+                in2 += wsum[w];
+                out2 += wsum2[w];
+            }
+            in2 *= (float)(1u << (2 * DENSE_F16_SCALE_LOG2));   // the outputs carry the images' 2^14 too
+            if (out2 > 0.f && in2 > 0.f && out2 < 3.0e38f && in2 < 3.0e38f) fix = sqrtf(in2 / out2);
+        }
+        const float2 fix2 = make_float2(fix, fix);
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const uint32_t se = stid ^ d.sgj[j];
             const uint64_t g = base | dep_tid | d.gj[j];
-            const float2 a = sm[se], b = sm[se ^ 1u];
+            const float2 a = tc16::mul2(sm[se], fix2), b = tc16::mul2(sm[se ^ 1u], fix2);
             __stcs(reinterpret_cast<VV*>(amps + g), make_float4(a.x, a.y, b.x, b.y));
         }
         __syncthreads();
