@@ -45,13 +45,15 @@ struct __align__(16) SwOp {
 
 struct __align__(16) PhaseDesc {
     uint32_t slut[1 << RBMAX];   // swz(lut[i]) for the state's element size
+    uint16_t tsw[8];             // FP16 tensor-core plans: swz16 of thread bit b's local offset
     uint32_t op_begin, op_end;
     uint32_t nt;                 // number of thread bits
-    uint8_t tbit_local[16];      // thread bit b -> local bit index
-    uint8_t tbit_global[16];     // thread bit b -> global qubit
+    uint8_t tbit_local[12];      // thread bit b -> local bit index (nt <= MMAX - 4)
+    uint8_t tbit_global[12];     // thread bit b -> global qubit
     uint16_t lut[1 << RBMAX];    // register index -> local offset
     uint8_t slot_global[RBMAX];  // register slot -> global qubit
 };
+static_assert(sizeof(PhaseDesc) == 256, "phase descriptors are copied in 16-byte units");
 
 struct SweepDesc {
     uint32_t n, m, c;
@@ -609,6 +611,63 @@ inline uint32_t swz_host(uint32_t e, uint32_t cb) {
     uint32_t r = e >> cb;
     uint32_t f = r ^ (r >> cb) ^ (r >> (2 * cb)) ^ (r >> (3 * cb));
     return e ^ (f & ((1u << cb) - 1));
+}
+
+// Shared-memory layout of the FP16 tensor-core sweeps (complex f32, at most 13 local bits):
+// element e is stored at swz16(e) = e ^ g(e), where local bits 0..3 address the 16 8-byte
+// units of a 128-byte row and every higher local bit b flips the unit index by its own
+// 4-bit pattern SWZ16_ROW[b - 4].  All 13 patterns (with 1, 2, 4, 8 for bits 0..3) are
+// distinct and non-zero, so any 8 local bits span all 16 units: a phase can always give its
+// warp lanes 5 thread bits whose patterns span the units, and then the 32 8-byte accesses of
+// a warp fall on every bank exactly twice (two wavefronts, no conflict), whichever 5 local
+// bits the phase keeps in registers.
+// SWZ16_ROW nibble k = the pattern of local bit 4 + k: 3, 5, 6, 9, 10, 12, 7, 11, 13
+constexpr uint64_t SWZ16_ROW = 0xDB7CA9653ull;
+
+__host__ __device__ inline uint32_t swz16(uint32_t e) {
+    uint32_t g = 0;
+    for (int b = 0; b < 9; ++b)
+        if ((e >> (4 + b)) & 1u) g ^= (uint32_t)(SWZ16_ROW >> (4 * b)) & 15u;
+    return e ^ g;
+}
+
+inline uint32_t swz16_unit(uint32_t local_bit) { return swz16(1u << local_bit) & 15u; }
+
+// Re-table a tensor-core program for the FP16 sweep kernel: slot and vector offsets under
+// swz16, and per phase an order of the thread bits whose first five (the warp lanes) span all
+// 16 bank units (a greedy basis, lowest local bits first), with the thread bits' swizzled
+// offsets in tsw.
+inline void retable_f16(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& phases, uint32_t rb) {
+    for (auto& d : descs) {
+        const uint32_t t = d.m - rb;
+        for (uint32_t j = 0; j < (1u << rb) / 2; ++j) d.sgj[j] = swz16(j * (1u << t) * 2u);
+    }
+    for (auto& ph : phases) {
+        for (uint32_t i = 0; i < (1u << rb); ++i) ph.slut[i] = swz16(ph.lut[i]);
+        const uint32_t nt = ph.nt;
+        std::vector<uint32_t> order, rest;
+        uint32_t span[16] = {0};   // reduced basis by leading bit
+        for (uint32_t b = 0; b < nt; ++b) {
+            uint32_t v = swz16_unit(ph.tbit_local[b]);
+            for (int k = 3; k >= 0 && v; --k)
+                if ((v >> k) & 1u) {
+                    if (span[k]) v ^= span[k];
+                    else { span[k] = v; v = 0; order.push_back(b); break; }
+                }
+            if (order.empty() || order.back() != b) rest.push_back(b);
+        }
+        for (uint32_t b : rest) order.push_back(b);
+        uint8_t tl[12], tg[12];
+        for (uint32_t b = 0; b < nt; ++b) {
+            tl[b] = ph.tbit_local[order[b]];
+            tg[b] = ph.tbit_global[order[b]];
+        }
+        for (uint32_t b = 0; b < nt; ++b) {
+            ph.tbit_local[b] = tl[b];
+            ph.tbit_global[b] = tg[b];
+        }
+        for (uint32_t b = 0; b < 8; ++b) ph.tsw[b] = b < nt ? (uint16_t)swz16(1u << ph.tbit_local[b]) : 0;
+    }
 }
 
 // Flatten sweeps into kernel tables: one SweepDesc per sweep, PhaseDescs,

@@ -964,7 +964,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
                                                      const uint32_t* __restrict__ images, uint64_t ntiles) {
     using VV = float4;
     constexpr int NR = 32;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t tile_elems = 1u << d.m;
     float2* sm = reinterpret_cast<float2*>(smem_raw);
     unsigned char* img = reinterpret_cast<unsigned char*>(sm + tile_elems);   // two image buffers
@@ -1015,7 +1015,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
         for (uint32_t b = d.c; b < d.m; ++b)
             if ((x >> b) & 1ull) dep_tid |= 1ull << d.local_global[b];
     }
-    const uint32_t stid = swz<float>(tid * 2);
+    const uint32_t stid = swz16(tid * 2);   // the FP16 kernel's layout (retable_f16)
     auto tile_base = [&](uint64_t tile) {
         uint64_t b = 0;
         for (uint32_t k = 0; k < d.nonlocal_count; ++k)
@@ -1068,18 +1068,16 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
             }
             const bool first = p == d.phase_begin;
             const bool last = p + 1 == d.phase_end;
-            // this thread's row: thread bit b sits at local bit tbit_local[b]
-            uint32_t ebase = 0;
+            // this thread's row: thread bit b sits at local bit tbit_local[b], whose swizzled
+            // offset is tsw[b] (the layout is XOR-linear)
+            uint32_t sb = 0;
             {
-                const uint32_t* tb = reinterpret_cast<const uint32_t*>(ph.tbit_local);
-                const uint32_t w0 = tb[0], w1 = tb[1];
+                const uint4 t4 = *reinterpret_cast<const uint4*>(ph.tsw);
+                const uint32_t tw[4] = {t4.x, t4.y, t4.z, t4.w};
 #pragma unroll
-                for (uint32_t b = 0; b < 8; ++b) {
-                    const uint32_t lb = ((b < 4 ? w0 : w1) >> (8 * (b & 3u))) & 0xFFu;
-                    if (b < ph.nt && ((tid >> b) & 1u)) ebase |= 1u << lb;
-                }
+                for (uint32_t b = 0; b < 8; ++b)
+                    if ((tid >> b) & 1u) sb ^= (tw[b >> 1] >> (16 * (b & 1u))) & 0xFFFFu;
             }
-            const uint32_t sb = swz<float>(ebase);
             // register i sits at sb ^ (XOR of S[k] over the set bits k of i); visiting the
             // registers in Gray-code order makes each address one XOR from the previous one
             uint32_t S[5];
@@ -1394,6 +1392,7 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
                 delete P;
                 return fail(RQ_ERR_CIRCUIT, "tensor-core plan: a phase is not one dense op");
             }
+        if (tc_passes == TC_F16) retable_f16(P->descs, phases, rb);
         P->tc_passes = tc_passes;
         P->mode = RQ_EXEC_SWEEP_TC;
     }

@@ -163,6 +163,62 @@ int main() {
                 }
         }
     }
+    // The FP16 sweep kernel's shared-memory layout (swz16, retable_f16): a bijection on a
+    // 13-bit tile; after re-tabling, every phase's (thread, register) pairs still cover the
+    // tile exactly once, and the five lane bits of every phase span all 16 bank units (the
+    // 32 8-byte accesses of a warp hit each bank exactly twice).
+    {
+        std::vector<int> hit(1u << 13, 0);
+        for (uint32_t e = 0; e < (1u << 13); ++e) ++hit[swz16(e)];
+        for (int h : hit)
+            if (h != 1) return fail("swz16 is not a bijection", -1);
+        for (int t2 = 0; t2 < 40; ++t2) {
+            const uint32_t n = 16 + (uint32_t)(t2 % 5), m = 13, c = 5, rb = 5;
+            const auto circ = random_circuit(n, r, t2 % 2 == 0);
+            std::vector<PGate> pg;
+            if (!to_pgates(circ.data(), circ.size(), pg)) return fail("to_pgates", t2);
+            auto sweeps = plan_sweeps(pg, n, m, c, true);
+            std::vector<SweepDesc> descs;
+            std::vector<PhaseDesc> phases;
+            std::vector<SwOp> ops;
+            std::vector<double> mats;
+            build_program(sweeps, n, m, c, rb, 2, descs, phases, ops, mats, true);
+            const std::vector<PhaseDesc> before = phases;
+            retable_f16(descs, phases, rb);
+            for (size_t pi = 0; pi < phases.size(); ++pi) {
+                const PhaseDesc& ph = phases[pi];
+                uint64_t set_a = 0, set_b = 0;
+                for (uint32_t b = 0; b < ph.nt; ++b) {
+                    set_a |= 1ull << ph.tbit_local[b];
+                    set_b |= 1ull << before[pi].tbit_local[b];
+                }
+                if (set_a != set_b || ph.nt != 8) return fail("retable changed the thread bits", t2);
+                uint32_t basis[4] = {0, 0, 0, 0};
+                int rank = 0;
+                for (uint32_t b = 0; b < 5; ++b) {
+                    uint32_t v = swz16(1u << ph.tbit_local[b]) & 15u;
+                    for (int k = 3; k >= 0 && v; --k)
+                        if ((v >> k) & 1u) {
+                            if (basis[k]) v ^= basis[k];
+                            else { basis[k] = v; ++rank; v = 0; }
+                        }
+                }
+                if (rank != 4) return fail("lane bits do not span the banks", t2);
+                std::vector<int> cover(1u << m, 0);
+                for (uint32_t tid = 0; tid < 256; ++tid) {
+                    uint32_t sb = 0;
+                    for (uint32_t b = 0; b < 8; ++b)
+                        if ((tid >> b) & 1u) sb ^= ph.tsw[b];
+                    for (uint32_t i = 0; i < 32; ++i) ++cover[sb ^ ph.slut[i]];
+                }
+                for (int v : cover)
+                    if (v != 1) return fail("retabled phase does not cover the tile once", t2);
+            }
+            for (const auto& d : descs)
+                for (uint32_t j = 0; j < 16; ++j)
+                    if (d.sgj[j] != swz16(j * (1u << 8) * 2u)) return fail("sgj not under swz16", t2);
+        }
+    }
     std::printf("ok %d plans\n", trials);
     return 0;
 }
