@@ -207,19 +207,49 @@ def qaoa_batch_leg(a, ws, rank, with_cpu):
     bet = np.array([x["betas"] for x in mine])
     qb = QaoaBatch(graphs, 4, "f32")
     qb.run(gam, bet, shots=1024, seed=11)            # warm-up (allocation, first launches)
-    ms, wall = [], []
+    ms, wall, profs = [], [], []
     for _ in range(3):
         t0 = time.perf_counter()
         out = qb.run(gam, bet, shots=1024, seed=11)
         wall.append(time.perf_counter() - t0)
         ms.append(qb.last_ms())
+        profs.append(qb.last_profile())
     dev_ms = min(ms)
+    prof = profs[int(np.argmin(ms))]
+    peak, peak_kind = _peak()
+    sweep_gbs = prof["sweep_bytes"] / (prof["sweep_ms"] / 1e3) / 1e9
+    sample_gbs = prof["sample_bytes"] / (prof["sample_ms"] / 1e3) / 1e9
     res = {"workload": "batched QAOA-MaxCut, %d random 3-regular graphs, n in {12..24}, p=4, f32 states, "
                        "1024 shots each, best cut" % a.qaoa_instances,
            "circuits_per_rank": len(mine), "device_ms": dev_ms, "wall_ms": 1e3 * min(wall),
            "evals_per_s": len(mine) * ws / (dev_ms / 1e3),
            "evals_per_s_e2e": len(mine) * ws / min(wall),
-           "mean_energy": float(np.mean(out["energies"])), "mean_best_cut": float(np.mean(out["best_cut"]))}
+           "mean_energy": float(np.mean(out["energies"])), "mean_best_cut": float(np.mean(out["best_cut"])),
+           "roofline": {"bound": "hbm", "kernel": "k_batch_sweep (all size classes and waves)",
+                        "achieved": sweep_gbs, "peak": peak, "unit": "GB/s", "frac": sweep_gbs / peak,
+                        "peak_kind": peak_kind, "bytes": prof["sweep_bytes"], "kernel_ms": prof["sweep_ms"],
+                        "bytes_definition": "per circuit and sweep: S written by the initialising sweep, 2S "
+                                            "(read + write) for every other sweep; S = 2^n x 8 B"},
+           "sampling": {"kernels": "k_leaf_fold / k_fold / k_sample (1024 shots per circuit)",
+                        "achieved_gbs": sample_gbs, "bytes": prof["sample_bytes"], "kernel_ms": prof["sample_ms"],
+                        "frac": sample_gbs / peak},
+           "device_ms_outside_kernels": dev_ms - prof["sweep_ms"] - prof["sample_ms"]}
+    # exact gradients of the same circuits: forward sweeps, then k_batch_adjoint over psi and lambda
+    qb.gradient(gam, bet)
+    gms, gprofs = [], []
+    for _ in range(3):
+        qb.gradient(gam, bet)
+        gms.append(qb.last_ms())
+        gprofs.append(qb.last_profile())
+    gp = gprofs[int(np.argmin(gms))]
+    res["adjoint_gradient"] = {
+        "device_ms": min(gms), "gradients_per_s": len(mine) * ws / (min(gms) / 1e3),
+        "roofline": {"bound": "hbm", "kernel": "k_batch_adjoint (psi and lambda through the reversed program)",
+                     "achieved": gp["adjoint_bytes"] / (gp["adjoint_ms"] / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": gp["adjoint_bytes"] / (gp["adjoint_ms"] / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
+                     "bytes": gp["adjoint_bytes"], "kernel_ms": gp["adjoint_ms"],
+                     "bytes_definition": "per circuit and backward sweep: read + write of psi and lambda (4S), "
+                                         "3S for the sweep that builds lambda = C psi instead of loading it"}}
     if with_cpu:
         import oracle
         t_by_n = {}
@@ -253,26 +283,46 @@ def vqe_batch_leg(a, ws, rank, with_cpu):
     params = shard(workloads.vqe_parameter_sets(a.vqe_sets, n * depth, 4), rank, ws)
     vb = VqeBatch(n, depth, coeffs, strings, "f32")
     vb.run(params[:2], gradient=True)           # warm-up
-    ms, wall = [], []
+    ms, wall, profs = [], [], []
     for _ in range(2):
         t0 = time.perf_counter()
         e, g = vb.run(params, gradient=True)
         wall.append(time.perf_counter() - t0)
         ms.append(vb.last_ms())
+        profs.append(vb.last_profile())
+    prof = profs[int(np.argmin(ms))]
     circuits = len(params) * (1 + 2 * n * depth)
     # the same energies and gradients by the adjoint pass (one forward, lambda = H psi, one backward)
     vb.run(params[:2], gradient="adjoint")
-    ams = []
+    ams, aprofs = [], []
     for _ in range(3):
         ea, ga = vb.run(params, gradient="adjoint")
         ams.append(vb.last_ms())
+        aprofs.append(vb.last_profile())
+    aprof = aprofs[int(np.argmin(ams))]
+    peak, peak_kind = _peak()
     scale = float(np.sum(np.abs(coeffs)))
     res = {"workload": "batched VQE, 16 qubits, 200-term Pauli Hamiltonian, depth-8 Ry+CZ ansatz, %d parameter "
                        "sets x 257 parameter-shift circuits, f32 states" % a.vqe_sets,
            "circuits_per_rank": circuits, "device_ms": min(ms), "wall_ms": 1e3 * min(wall),
            "circuits_per_s": circuits * ws / (min(ms) / 1e3), "mean_energy": float(np.mean(e)),
            "gradient_sets_per_s_shift": len(params) * ws / (min(ms) / 1e3),
+           "roofline": {"bound": "hbm", "kernel": "k_batch_sweep (ansatz evolution of all 131,584 circuits)",
+                        "achieved": prof["sweep_bytes"] / (prof["sweep_ms"] / 1e3) / 1e9, "peak": peak,
+                        "unit": "GB/s",
+                        "frac": prof["sweep_bytes"] / (prof["sweep_ms"] / 1e3) / 1e9 / peak,
+                        "peak_kind": peak_kind, "bytes": prof["sweep_bytes"], "kernel_ms": prof["sweep_ms"],
+                        "note": "waves of ~96 MB of states are sized to stay in L2, so these bytes are mostly "
+                                "L2 traffic: a fraction above 1 of the HBM copy peak is possible and expected"},
+           "energy_pass": {"kernel": "k_vqe_energy_tiles", "flops": prof["energy_flops"],
+                           "kernel_ms": prof["energy_ms"],
+                           "achieved_tflops": prof["energy_flops"] / (prof["energy_ms"] / 1e3) / 1e12,
+                           "flops_definition": "8 per Pauli string and amplitude: one complex product "
+                                               "conj(a[i^x]) a[i] and its FP64 accumulation (CUDA cores, FP32 "
+                                               "products, FP64 sums; no measured peak for this mix)"},
            "adjoint": {"device_ms": min(ams), "gradient_sets_per_s": len(params) * ws / (min(ams) / 1e3),
+                       "kernel_ms": aprof["adjoint_ms"], "bytes": aprof["adjoint_bytes"],
+                       "achieved_gbs": aprof["adjoint_bytes"] / max(1e-9, aprof["adjoint_ms"] / 1e3) / 1e9,
                        "speedup_vs_shift": min(ms) / min(ams),
                        "max_abs_grad_diff_vs_shift_rel": float(np.max(np.abs(ga - g))) / scale,
                        "energies_identical": bool(np.array_equal(ea, e))}}

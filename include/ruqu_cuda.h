@@ -441,6 +441,13 @@ RQ_API int rq_qaoa_batch_state(rq_qaoa_batch* b, uint64_t circuit, double* inter
 
 /* Device time of the last run (CUDA events around all of its kernels), ms. */
 RQ_API int rq_qaoa_batch_last_ms(const rq_qaoa_batch* b, float* ms);
+/* Device time and algorithmic work of the last rq_qaoa_batch_run / _gradient, by kernel
+ * kind (no counterpart in the reference): out6 = {sweep HBM bytes, sweep ms, sampling
+ * bytes, sampling ms, adjoint bytes, adjoint ms}.  Bytes are algorithmic: per circuit
+ * and sweep, S written by an initialising sweep and 2S for a read and a write otherwise
+ * (two states in the adjoint pass), and per sampled circuit S + 2^n x 16 bytes for the
+ * prefix tree; times are CUDA events around each class's launches. */
+RQ_API int rq_qaoa_batch_last_profile(const rq_qaoa_batch* b, double* out6);
 
 /* Upper bound of state memory per wave (default 24 GiB). */
 RQ_API int rq_qaoa_batch_set_state_budget(rq_qaoa_batch* b, uint64_t bytes);
@@ -480,6 +487,12 @@ RQ_API int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* param
                             int32_t with_gradient, double* energies, double* gradients);
 
 RQ_API int rq_vqe_batch_last_ms(const rq_vqe_batch* b, float* ms);
+/* As rq_qaoa_batch_last_profile for the last rq_vqe_batch_run: {evolution sweep bytes,
+ * evolution ms, energy-pass floating-point operations (8 per string and amplitude),
+ * energy ms, adjoint bytes (the H pass and the backward program over two states),
+ * adjoint ms}.  The waves are sized to stay in L2, so the sweep bytes are mostly L2
+ * traffic.  No counterpart in the reference. */
+RQ_API int rq_vqe_batch_last_profile(const rq_vqe_batch* b, double* out6);
 RQ_API int rq_vqe_batch_destroy(rq_vqe_batch* b);
 
 /* ------------------------------------------------------------------------ */

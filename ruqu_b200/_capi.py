@@ -94,11 +94,13 @@ SIGNATURES = {
                                                  _P(_dbl), _P(_u32)]),
     "rq_qaoa_batch_set_convergence": (C.c_int, [_vp, _dbl]),
     "rq_qaoa_batch_last_ms": (C.c_int, [_vp, _P(C.c_float)]),
+    "rq_qaoa_batch_last_profile": (C.c_int, [_vp, _P(_dbl)]),
     "rq_qaoa_batch_set_state_budget": (C.c_int, [_vp, _u64]),
     "rq_qaoa_batch_destroy": (C.c_int, [_vp]),
     "rq_vqe_batch_create": (C.c_int, [_u32, _u32, _P(_dbl), _P(RqPauliOp), _P(_u32), _u32, _i32, _P(_vp)]),
     "rq_vqe_batch_run": (C.c_int, [_vp, _u32, _P(_dbl), _i32, _P(_dbl), _P(_dbl)]),
     "rq_vqe_batch_last_ms": (C.c_int, [_vp, _P(C.c_float)]),
+    "rq_vqe_batch_last_profile": (C.c_int, [_vp, _P(_dbl)]),
     "rq_vqe_batch_destroy": (C.c_int, [_vp]),
     "rq_gemm_bf16": (C.c_int, [_P(C.c_uint16), _P(C.c_uint16), _i32, _i32, _i32, _P(C.c_float)]),
     "rq_mlp_create": (C.c_int, [_i32, _i32, _i32, _i32, _u64, _P(_vp)]),

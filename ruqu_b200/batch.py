@@ -137,6 +137,13 @@ class QaoaBatch:
         check(lib.rq_qaoa_batch_last_ms(self._h, C.byref(ms)))
         return ms.value
 
+    def last_profile(self) -> dict:
+        """Device time and algorithmic work of the last run / gradient, by kernel kind."""
+        out = np.zeros(6)
+        check(lib.rq_qaoa_batch_last_profile(self._h, _dp(out)))
+        return {"sweep_bytes": out[0], "sweep_ms": out[1], "sample_bytes": out[2], "sample_ms": out[3],
+                "adjoint_bytes": out[4], "adjoint_ms": out[5]}
+
     def set_state_budget(self, nbytes: int) -> None:
         check(lib.rq_qaoa_batch_set_state_budget(self._h, int(nbytes)))
 
@@ -179,6 +186,13 @@ class VqeBatch:
         g = np.empty((nsets, self.P)) if mode else np.empty(1)
         check(lib.rq_vqe_batch_run(self._h, nsets, _dp(p), mode, _dp(e), _dp(g)))
         return (e, g) if mode else e
+
+    def last_profile(self) -> dict:
+        """Device time and algorithmic work of the last run, by kernel kind."""
+        out = np.zeros(6)
+        check(lib.rq_vqe_batch_last_profile(self._h, _dp(out)))
+        return {"sweep_bytes": out[0], "sweep_ms": out[1], "energy_flops": out[2], "energy_ms": out[3],
+                "adjoint_bytes": out[4], "adjoint_ms": out[5]}
 
     def last_ms(self) -> float:
         ms = C.c_float()

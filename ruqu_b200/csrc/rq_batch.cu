@@ -1094,6 +1094,68 @@ __global__ void __launch_bounds__(256) k_vqe_apply_h(const typename C2<T>::t* __
 // ===========================================================================
 // batch object
 // ===========================================================================
+// Device-time and algorithmic-work accounting of one batched run, per kind of kernel
+// (0: forward sweeps, 1: read-out -- QAOA sampling / VQE energies, 2: adjoint passes):
+// events bracket each group of launches on the batch's stream; the sums are read after the
+// run's final synchronisation.  Work is algorithmic: HBM bytes of the sweeps (S written by
+// an initialising sweep, 2S per other sweep and state), the sampling tree's bytes, or the
+// energy pass's floating-point operations.
+struct RunProfile {
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> kind;      // per event pair
+    size_t used = 0;            // events in use
+    bool on = false;            // only the plain runs are profiled (not graph-captured steps)
+    double work[3] = {0, 0, 0};
+    double ms[3] = {0, 0, 0};
+    int begin(cudaStream_t st) {
+        if (!on) return -1;
+        if (used + 2 > ev.size()) {
+            for (int k = 0; k < 2; ++k) {
+                cudaEvent_t e = nullptr;
+                if (cudaEventCreate(&e) != cudaSuccess) return -1;
+                ev.push_back(e);
+            }
+        }
+        cudaEventRecord(ev[used], st);
+        used += 2;
+        return (int)used - 2;
+    }
+    void end(int at, cudaStream_t st, int k, double w) {
+        if (at < 0) return;
+        cudaEventRecord(ev[at + 1], st);
+        kind.push_back(k);
+        work[k] += w;
+    }
+    void start() {
+        on = true;
+        used = 0;
+        kind.clear();
+        for (int k = 0; k < 3; ++k) work[k] = ms[k] = 0.0;
+    }
+    void collect() {   // after the stream has been synchronised
+        on = false;
+        for (size_t i = 0; i < kind.size(); ++i) {
+            float t = 0.f;
+            if (cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]) == cudaSuccess) ms[kind[i]] += t;
+        }
+    }
+    void release() {
+        for (auto e : ev) cudaEventDestroy(e);
+        ev.clear();
+    }
+};
+
+// algorithmic HBM bytes of one circuit's sweeps
+inline double sweep_bytes(const std::vector<SweepDesc>& descs, double state_bytes, double states = 1.0) {
+    double b = 0.0;
+    for (const auto& d : descs) {
+        const bool init = d.flags & (SWEEP_INIT_UNIFORM | SWEEP_INIT_ZERO);
+        b += states * (init ? state_bytes : 2.0 * state_bytes);
+        if (d.flags & SWEEP_INIT_LAMBDA) b -= state_bytes;   // lambda is built, not loaded
+    }
+    return b;
+}
+
 struct QClass {
     uint32_t n = 0, m = 0, c = 0;
     std::vector<uint32_t> insts;            // instances of this size
@@ -1150,6 +1212,7 @@ struct rq_qaoa_batch {
     uint64_t last_wave_first = 0, last_wave_count = 0;
     uint32_t last_wave_n = 0;
     float last_ms = 0.f;
+    RunProfile prof;
     size_t state_budget = (size_t)24 << 30;
     double conv_tol = 0.0;                 // optimizers: stop an instance when |E - E_prev| < conv_tol (0: off)
 };
@@ -1467,6 +1530,7 @@ int rq_qaoa_batch_destroy(rq_qaoa_batch* b) {
                     b->d_best_bits, b->d_best_cut, b->d_states, b->d_epart, b->d_tree, b->d_lam, b->d_gpart,
                     b->d_grad};
     for (void* q : ptrs) if (q) cudaFree(q);
+    b->prof.release();
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -1567,14 +1631,24 @@ int qaoa_launch(rq_qaoa_batch* b, uint32_t nsets, uint32_t shots, uint64_t base_
         }
         for (uint64_t w0 = 0; w0 < kc; w0 += wave) {
             const uint64_t wn = std::min<uint64_t>(wave, kc - w0);
-            if (b->prec == RQ_F32) {
-                RQ_TRY(launch_class<float>(b, K, wn, pos + w0, b->d_states));
-                if (shots) RQ_TRY(sample_class<float>(b, K, wn, pos + w0, b->d_states, shots, base_seed));
-                if (adjoint) RQ_TRY(adjoint_class<float>(b, K, wn, pos + w0, b->d_states, b->d_lam));
-            } else {
-                RQ_TRY(launch_class<double>(b, K, wn, pos + w0, b->d_states));
-                if (shots) RQ_TRY(sample_class<double>(b, K, wn, pos + w0, b->d_states, shots, base_seed));
-                if (adjoint) RQ_TRY(adjoint_class<double>(b, K, wn, pos + w0, b->d_states, b->d_lam));
+            const double sb = (double)state_bytes;
+            int ev = b->prof.begin(b->stream);
+            if (b->prec == RQ_F32) RQ_TRY(launch_class<float>(b, K, wn, pos + w0, b->d_states));
+            else RQ_TRY(launch_class<double>(b, K, wn, pos + w0, b->d_states));
+            b->prof.end(ev, b->stream, 0, (double)wn * sweep_bytes(K.descs, sb));
+            if (shots) {
+                ev = b->prof.begin(b->stream);
+                if (b->prec == RQ_F32) RQ_TRY(sample_class<float>(b, K, wn, pos + w0, b->d_states, shots, base_seed));
+                else RQ_TRY(sample_class<double>(b, K, wn, pos + w0, b->d_states, shots, base_seed));
+                // the tree's leaf level reads the state and writes 2^n doubles; the folds read and
+                // write the levels above once more (the walks touch n entries per shot)
+                b->prof.end(ev, b->stream, 1, (double)wn * (sb + 2.0 * (double)((size_t)1 << K.n) * 8.0));
+            }
+            if (adjoint) {
+                ev = b->prof.begin(b->stream);
+                if (b->prec == RQ_F32) RQ_TRY(adjoint_class<float>(b, K, wn, pos + w0, b->d_states, b->d_lam));
+                else RQ_TRY(adjoint_class<double>(b, K, wn, pos + w0, b->d_states, b->d_lam));
+                b->prof.end(ev, b->stream, 2, (double)wn * sweep_bytes(K.adescs, sb, 2.0));
             }
             b->last_wave_first = pos + w0;
             b->last_wave_count = adjoint ? 0 : wn;   // the backward pass overwrites the final states
@@ -1705,8 +1779,13 @@ int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, co
     RQ_CUDA(cudaSetDevice(b->device));
     const uint64_t ncirc = (uint64_t)b->ninst * nsets;
     RQ_TRY(qaoa_prepare(b, nsets, gammas, betas));
+    b->prof.start();
     RQ_CUDA(cudaEventRecord(b->ev0, b->stream));
-    RQ_TRY(qaoa_launch(b, nsets, shots, base_seed));
+    const int lrc = qaoa_launch(b, nsets, shots, base_seed);
+    if (lrc != RQ_OK) {
+        b->prof.on = false;
+        return lrc;
+    }
     RQ_CUDA(cudaEventRecord(b->ev1, b->stream));
     std::vector<double> e(ncirc);
     RQ_CUDA(cudaMemcpyAsync(e.data(), b->d_energy, ncirc * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
@@ -1720,6 +1799,7 @@ int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, co
     }
     RQ_CUDA(cudaStreamSynchronize(b->stream));
     RQ_CUDA(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+    b->prof.collect();
     for (uint64_t k = 0; k < ncirc; ++k) {
         const uint64_t user = b->order[k];
         energies[user] = e[k];
@@ -1738,14 +1818,20 @@ int rq_qaoa_batch_gradient(rq_qaoa_batch* b, const double* gammas, const double*
     RQ_CUDA(cudaSetDevice(b->device));
     const uint32_t p = b->p, P2 = 2 * p, ninst = b->ninst;
     RQ_TRY(qaoa_prepare(b, 1, gammas, betas));
+    b->prof.start();
     RQ_CUDA(cudaEventRecord(b->ev0, b->stream));
-    RQ_TRY(qaoa_launch(b, 1, 0, 0, nullptr, true));
+    const int lrc = qaoa_launch(b, 1, 0, 0, nullptr, true);
+    if (lrc != RQ_OK) {
+        b->prof.on = false;
+        return lrc;
+    }
     RQ_CUDA(cudaEventRecord(b->ev1, b->stream));
     std::vector<double> e(ninst), g((size_t)ninst * P2);
     RQ_CUDA(cudaMemcpyAsync(e.data(), b->d_energy, ninst * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
     RQ_CUDA(cudaMemcpyAsync(g.data(), b->d_grad, g.size() * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
     RQ_CUDA(cudaStreamSynchronize(b->stream));
     RQ_CUDA(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+    b->prof.collect();
     for (uint32_t k = 0; k < ninst; ++k) {
         const uint64_t user = b->order[k];
         energies[user] = e[k];
@@ -2011,6 +2097,15 @@ int rq_qaoa_batch_state(rq_qaoa_batch* b, uint64_t circuit, double* interleaved)
     return RQ_OK;
 }
 
+int rq_qaoa_batch_last_profile(const rq_qaoa_batch* b, double* out6) {
+    if (!b || !out6) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    for (int k = 0; k < 3; ++k) {
+        out6[2 * k] = b->prof.work[k];
+        out6[2 * k + 1] = b->prof.ms[k];
+    }
+    return RQ_OK;
+}
+
 int rq_qaoa_batch_last_ms(const rq_qaoa_batch* b, float* ms) {
     if (!b || !ms) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
     *ms = b->last_ms;
@@ -2058,6 +2153,7 @@ struct rq_vqe_batch {
     double* d_energy = nullptr;
     size_t energy_cap = 0;
     float last_ms = 0.f;
+    RunProfile prof;
     size_t wave_bytes = (size_t)96 << 20;   // states per wave kept around the L2 size
     // exact gradients: the reversed ansatz as an adjoint program, H as operator strings
     uint32_t am = 0;
@@ -2125,11 +2221,19 @@ int vqe_wave(rq_vqe_batch* b, uint64_t ncirc, uint64_t circ0) {
     if (per_sm < 1) return rq::fail(RQ_ERR_CUDA, "batched sweep kernel does not fit on an SM");
     const int sms = rq::num_sms(b->device);
     const unsigned grid = (unsigned)std::min<uint64_t>(ncirc * b->ntiles, (uint64_t)sms * per_sm);
+    int ev = b->prof.begin(b->stream);
     for (const auto& d : b->descs) {
         kern<<<grid, threads, b->smem, b->stream>>>(d, ph, op, a);
         RQ_CUDA(cudaGetLastError());
     }
-    return vqe_energy<T>(b, ncirc, circ0);
+    const double sb = (double)((size_t)1 << b->n) * sizeof(V);
+    b->prof.end(ev, b->stream, 0, (double)ncirc * sweep_bytes(b->descs, sb));
+    ev = b->prof.begin(b->stream);
+    RQ_TRY(vqe_energy<T>(b, ncirc, circ0));
+    // per string and amplitude: one complex product conj(a[i ^ x]) a[i] (6 flops) and its
+    // FP64 accumulation (2 flops)
+    b->prof.end(ev, b->stream, 1, (double)ncirc * (double)b->nterms * (double)((size_t)1 << b->n) * 8.0);
+    return RQ_OK;
 }
 
 // exact gradients of a wave whose final states vqe_wave left in d_states: lambda = H psi,
@@ -2379,6 +2483,7 @@ int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* params, int3
     }
     RQ_CUDA(cudaMemcpyAsync(b->d_params, params, (size_t)nsets * P * sizeof(double), cudaMemcpyHostToDevice, b->stream));
     const int sms = rq::num_sms(b->device);
+    b->prof.start();
     RQ_CUDA(cudaEventRecord(b->ev0, b->stream));
     if (b->prec == RQ_F32)
         k_vqe_rot<float><<<rq::grid_for(ncirc * P, TPB, sms), TPB, 0, b->stream>>>(b->d_params, ncirc, P, V, (float*)b->d_rot);
@@ -2389,10 +2494,20 @@ int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* params, int3
         const uint64_t wn = std::min<uint64_t>(wave, ncirc - w0);
         if (b->prec == RQ_F32) {
             RQ_TRY(vqe_wave<float>(b, wn, w0));
-            if (adj) RQ_TRY(vqe_adjoint<float>(b, wn, w0));
+            if (adj) {
+                const int ev = b->prof.begin(b->stream);
+                RQ_TRY(vqe_adjoint<float>(b, wn, w0));
+                b->prof.end(ev, b->stream, 2, (double)wn * (2.0 * (double)((size_t)8 << b->n) +
+                                                            sweep_bytes(b->adescs, (double)((size_t)8 << b->n), 2.0)));
+            }
         } else {
             RQ_TRY(vqe_wave<double>(b, wn, w0));
-            if (adj) RQ_TRY(vqe_adjoint<double>(b, wn, w0));
+            if (adj) {
+                const int ev = b->prof.begin(b->stream);
+                RQ_TRY(vqe_adjoint<double>(b, wn, w0));
+                b->prof.end(ev, b->stream, 2, (double)wn * (2.0 * (double)((size_t)16 << b->n) +
+                                                            sweep_bytes(b->adescs, (double)((size_t)16 << b->n), 2.0)));
+            }
         }
     }
     RQ_CUDA(cudaEventRecord(b->ev1, b->stream));
@@ -2403,11 +2518,21 @@ int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* params, int3
                                 b->stream));
     RQ_CUDA(cudaStreamSynchronize(b->stream));
     RQ_CUDA(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+    b->prof.collect();
     for (uint32_t s = 0; s < nsets; ++s) {
         energies[s] = e[(uint64_t)s * V];
         if (with_gradient == RQ_VQE_GRAD_SHIFT)
             for (uint32_t k = 0; k < P; ++k)
                 gradients[(uint64_t)s * P + k] = (e[(uint64_t)s * V + 1 + 2 * k] - e[(uint64_t)s * V + 2 + 2 * k]) / 2.0;
+    }
+    return RQ_OK;
+}
+
+int rq_vqe_batch_last_profile(const rq_vqe_batch* b, double* out6) {
+    if (!b || !out6) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    for (int k = 0; k < 3; ++k) {
+        out6[2 * k] = b->prof.work[k];
+        out6[2 * k + 1] = b->prof.ms[k];
     }
     return RQ_OK;
 }
@@ -2425,6 +2550,7 @@ int rq_vqe_batch_destroy(rq_vqe_batch* b) {
     void* ptrs[] = {b->prog,     b->d_groups, b->d_terms, b->d_gofs,  b->d_part, b->d_params, b->d_rot,
                     b->d_states, b->d_energy, b->aprog,   b->d_hterms, b->d_lam,  b->d_gpart,  b->d_grad};
     for (void* q : ptrs) if (q) cudaFree(q);
+    b->prof.release();
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->stream) cudaStreamDestroy(b->stream);
