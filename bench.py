@@ -447,7 +447,8 @@ def warmstart_leg(a, ws, rank):
 # case of this circuit, per tile; a launch moves every tile once, so the figure
 # scales with the tile count (x16 from 26 to 30 qubits).
 _NCU_BYTES_PER_TILE = {"k_sweep_tc": (537.133824e6 + 487.704576e6) / 2 ** 13,
-                       "k_sweep": (537.2e6 + 485.1e6) / 2 ** 13}
+                       "k_sweep": (537.2e6 + 485.1e6) / 2 ** 13,
+                       "k_sweep_tc16": (537.199360e6 + 484.082176e6) / 2 ** 13}
 
 
 _EXECUTED_AS = {1: "unfused per-gate kernels", 2: "CUDA-core sweeps", 3: "tensor-core sweeps (3xTF32)",

@@ -1050,6 +1050,16 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
         const uint64_t nbase = next < ntiles ? tile_base(next) : 0;
         issue_tile<float>(sm, amps, d, base, dep_tid, stid);
         cp_async_commit();
+        if (next < ntiles) {
+            // Pull the next tile into L2 while this one runs its phases: thread t prefetches the
+            // t-th contiguous run of 2^c amplitudes (local bits c.. of t << c; 2^(m-c) runs, one
+            // per thread), so the next tile's loads hit L2 instead of waiting on HBM.
+            uint64_t g = nbase;
+            const uint32_t x = tid << d.c;
+            for (uint32_t b = d.c; b < d.m; ++b)
+                if ((x >> b) & 1u) g |= 1ull << d.local_global[b];
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(amps + g), "r"(8u << d.c) : "memory");
+        }
         cp_async_wait0();
         __syncthreads();
         const float mid_scale = tc16::pow2f(-DENSE_F16_SCALE_LOG2);
