@@ -59,6 +59,8 @@ def _args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-qaoa", action="store_true", help="skip the batched QAOA leg")
     ap.add_argument("--qaoa-instances", type=int, default=2048)
+    ap.add_argument("--qaoa-sizes", default="12,14,16,18,20,22,24",
+                    help="graph sizes of the batched QAOA leg (the config's n uniform over {12..24})")
     ap.add_argument("--no-vqe", action="store_true", help="skip the batched VQE leg")
     ap.add_argument("--vqe-sets", type=int, default=512)
     ap.add_argument("--no-warm", action="store_true", help="skip the warm-start leg")
@@ -200,7 +202,8 @@ def qaoa_batch_leg(a, ws, rank, with_cpu):
     from ruqu_b200 import workloads
     from ruqu_b200.batch import QaoaBatch
     from ruqu_b200.dist import shard
-    inst = workloads.qaoa_instances(a.qaoa_instances, 2)
+    sizes = tuple(int(x) for x in a.qaoa_sizes.split(","))
+    inst = workloads.qaoa_instances(a.qaoa_instances, 2, n_values=sizes)
     mine = shard(inst, rank, ws)
     graphs = [(x["n"], [(u, v) for u, v, _ in x["edges"]]) for x in mine]
     gam = np.array([x["gammas"] for x in mine])
@@ -219,8 +222,8 @@ def qaoa_batch_leg(a, ws, rank, with_cpu):
     peak, peak_kind = _peak()
     sweep_gbs = prof["sweep_bytes"] / (prof["sweep_ms"] / 1e3) / 1e9
     sample_gbs = prof["sample_bytes"] / (prof["sample_ms"] / 1e3) / 1e9
-    res = {"workload": "batched QAOA-MaxCut, %d random 3-regular graphs, n in {12..24}, p=4, f32 states, "
-                       "1024 shots each, best cut" % a.qaoa_instances,
+    res = {"workload": "batched QAOA-MaxCut, %d random 3-regular graphs, n in {%s}, p=4, f32 states, "
+                       "1024 shots each, best cut" % (a.qaoa_instances, a.qaoa_sizes),
            "circuits_per_rank": len(mine), "device_ms": dev_ms, "wall_ms": 1e3 * min(wall),
            "evals_per_s": len(mine) * ws / (dev_ms / 1e3),
            "evals_per_s_e2e": len(mine) * ws / min(wall),
@@ -253,18 +256,25 @@ def qaoa_batch_leg(a, ws, rank, with_cpu):
     if with_cpu:
         import oracle
         t_by_n = {}
-        for n in (12, 14, 16, 18):
+        present = sorted({x["n"] for x in inst})
+        timed = [n for n in present if n <= 18] or present[:1]
+        for n in timed:
             x = next(y for y in inst if y["n"] == n)
             t0 = time.perf_counter()
             oracle.qaoa_cost(n, x["edges"], x["gammas"], x["betas"])
             t_by_n[n] = time.perf_counter() - t0
-        for n in (20, 22, 24):   # each +2 qubits: 4x the amplitudes, (n+2)/n the gates
-            t_by_n[n] = t_by_n[n - 2] * 4.0 * (n + 2) / n
+        for n in present:   # each +2 qubits: 4x the amplitudes, (n+2)/n the gates
+            if n not in t_by_n:
+                m = max(k for k in t_by_n if k < n)
+                t = t_by_n[m]
+                for k in range(m, n, 2):
+                    t *= 4.0 * (k + 2) / k
+                t_by_n[n] = t
         total = sum(t_by_n[x["n"]] for x in inst)
         res["cpu_baseline"] = {"value": len(inst) / total, "unit": "QAOA evals/s", "cores": 1, "kind": "port",
                                "sample": "one evaluate_qaoa_cost (reference f64 engine, energy only, no shots) "
-                                         "per n in {12,14,16,18} timed; n = 20, 22, 24 scaled by 4(n+2)/n per +2 "
-                                         "qubits; summed over the 2048 instances"}
+                                         "per n in {%s} timed; larger n scaled by 4(n+2)/n per +2 qubits; summed "
+                                         "over the %d instances" % (",".join(map(str, timed)), len(inst))}
     return res
 
 
