@@ -761,6 +761,23 @@ def run_ours(a):
                "h2d_bytes_per_step": len(gates) * C.sizeof(rq._capi.RqGate),
                "d2h_bytes_per_step": 8 * a.qubits, "ms_per_step": dt * 1e3,
                "path": "QuantumState.reset + apply_gates(host list) + expectation_values(<Z_i>) -> host"}
+        # the same path with a new angle set every step (what an optimizer's evaluations do):
+        # the structure repeats, so each step rebuilds only the matrix tables and operand images
+        vsteps = max(2, min(a.steps, 4))
+        varr = [gates_to_array(workloads.random_layer_circuit(a.qubits, a.layers, 1000 + a.seed + k))
+                for k in range(vsteps + 1)]
+        state.reset()
+        state.apply_gates(varr[0], mode)
+        state.expectation_values(zs)
+        t0 = time.perf_counter()
+        for k in range(1, vsteps + 1):
+            state.reset()
+            state.apply_gates(varr[k], mode)
+            state.expectation_values(zs)
+        dtv = (time.perf_counter() - t0) / vsteps
+        e2e["varying_angles"] = {"value": ws * layer_bytes / dtv / 1e9, "unit": UNIT, "ms_per_step": dtv * 1e3,
+                                 "steps": vsteps, "ratio_to_e2e": dt / dtv,
+                                 "path": "as e2e, with a new angle set (same gate structure) every step"}
 
     readout = None
     if not a.no_sampling:

@@ -259,6 +259,17 @@ RQ_API int rq_state_apply_2q_matrix(rq_state* s, uint32_t q1, uint32_t q2,
 RQ_API int rq_plan_create(const rq_state* s, const rq_gate* gates, uint64_t n,
                           int32_t mode, rq_plan** out);
 RQ_API int rq_plan_execute(rq_state* s, const rq_plan* p);
+
+/* New gate values for a prepared plan: `gates` must have the plan's gate kinds and
+ * qubits (barriers aside) and may change any angle or matrix.  No counterpart in the
+ * reference (whose drivers rebuild the circuit for every evaluation, qaoa.rs:232 and
+ * vqe.rs:129); this is what makes those evaluations cheap here: the plan's sweeps and
+ * phases are kept, the fused matrices are re-derived on the host and the tensor-core
+ * operand images rebuilt on the GPU, in stream order on s's stream (after every earlier
+ * launch of the plan, on any stream).  RQ_ERR_CIRCUIT when the structure differs (the
+ * plan is then unchanged).  rq_state_apply does the same by itself for gate lists that
+ * repeat the structure of a recently applied list. */
+RQ_API int rq_plan_update(rq_state* s, rq_plan* p, const rq_gate* gates, uint64_t n);
 RQ_API int rq_plan_get_stats(const rq_plan* p, rq_plan_stats* out);
 RQ_API int rq_plan_destroy(rq_plan* p);
 

@@ -368,6 +368,19 @@ int rq_plan_create(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t 
     return rq::plan_build(s, gates, n, use_sweep ? RQ_EXEC_SWEEP : RQ_EXEC_PER_GATE, out, passes, 2, m);
 }
 
+int rq_plan_update(rq_state* s, rq_plan* p, const rq_gate* gates, uint64_t n) {
+    if (!s || !p || (!gates && n)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (!rq::plan_fits(p, s))
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "plan was built for another qubit count, precision or device");
+    for (uint64_t k = 0; k < n; ++k) {
+        RQ_TRY(validate_gate(s, gates[k]));
+        if (gates[k].kind == RQ_GATE_MEASURE || gates[k].kind == RQ_GATE_RESET)
+            return rq::fail(RQ_ERR_CIRCUIT, "circuit error: a plan holds unitary gates only");
+    }
+    RQ_TRY(set_device(s));
+    return rq::plan_rebind(s, p, gates, n);
+}
+
 int rq_plan_execute(rq_state* s, const rq_plan* p) {
     if (!s || !p) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
     if (!rq::plan_fits(p, s))

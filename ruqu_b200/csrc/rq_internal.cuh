@@ -120,6 +120,10 @@ inline int tc_passes_of(int32_t mode) {
     return mode == RQ_EXEC_SWEEP_TC ? 3 : mode == RQ_EXEC_SWEEP_TC_FAST ? 1 : mode == RQ_EXEC_SWEEP_TC16 ? TC_F16 : 0;
 }
 int plan_launch(rq_state* s, const rq_plan* p);
+// the same gate kinds and qubits as the plan was built for (barriers ignored)
+bool plan_same_shape(const rq_plan* p, const rq_gate* gates, uint64_t n);
+// new gate values for a plan of the same structure (RQ_ERR_CIRCUIT, plan unchanged, otherwise)
+int plan_rebind(rq_state* s, rq_plan* p, const rq_gate* gates, uint64_t n);
 void plan_free(rq_plan* p);
 rq_plan_stats plan_stats(const rq_plan* p);
 bool plan_fits(const rq_plan* p, const rq_state* s);

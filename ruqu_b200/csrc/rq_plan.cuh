@@ -672,9 +672,15 @@ inline void retable_f16(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& p
 
 // Flatten sweeps into kernel tables: one SweepDesc per sweep, PhaseDescs,
 // op records and the f64 matrix entries (narrowed later for f32 states).
+// given_phases (optional): the phase plans to use per sweep instead of planning them (a program
+// rebuilt for new gate values with an unchanged structure); used_phases (optional) receives the
+// phase plans of every sweep.
 inline void build_program(std::vector<Sweep>& sweeps, uint32_t nq, uint32_t m, uint32_t c, uint32_t rb,
                           uint32_t epv, std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& phases,
-                          std::vector<SwOp>& ops, std::vector<double>& mats, bool all_slots = false) {
+                          std::vector<SwOp>& ops, std::vector<double>& mats, bool all_slots = false,
+                          const std::vector<std::vector<PhasePlan>>* given_phases = nullptr,
+                          std::vector<std::vector<PhasePlan>>* used_phases = nullptr) {
+    size_t sweep_index = 0;
     for (auto& sw : sweeps) {
         uint64_t L = sw.L;
         for (uint32_t q = 0; q < nq && (uint32_t)__builtin_popcountll(L) < m; ++q) L |= 1ull << q;
@@ -701,7 +707,9 @@ inline void build_program(std::vector<Sweep>& sweeps, uint32_t nq, uint32_t m, u
             d.sgj[j] = swz_host((uint32_t)x, cb);
         }
         d.phase_begin = (uint32_t)phases.size();
-        auto pplan = plan_phases(sw, rb, all_slots);
+        auto pplan = given_phases ? (*given_phases)[sweep_index] : plan_phases(sw, rb, all_slots);
+        if (used_phases) used_phases->push_back(pplan);
+        ++sweep_index;
         for (auto& pp : pplan) {
             PhaseDesc Ph{};
             Ph.op_begin = (uint32_t)ops.size();
@@ -780,134 +788,159 @@ constexpr int DENSE_F16_WORDS = 64 * 64;       // 32-bit words per image (two 8 
 enum DenseFormat : int { DENSE_TF32 = 0, DENSE_F16 = 1 };
 inline size_t dense_image_words(int fmt) { return fmt == DENSE_F16 ? DENSE_F16_WORDS : DENSE_IMAGE_FLOATS; }
 
+// Exactly rounded double arithmetic, the same on the host and the device (no fused
+// multiply-add on either side), so that operand images built on the GPU are bit-identical to
+// the host's restatement of the same products.
+__host__ __device__ inline double dmul(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return __dmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+__host__ __device__ inline double dadd(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return __dadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+__host__ __device__ inline double dsub(double a, double b) {
+#ifdef __CUDA_ARCH__
+    return __dsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+
 // v <- op(v) on a 32-vector of register amplitudes (the kernel's op semantics); u0 / u1
 // are the values of q0 / q1 when they are not register slots (uniform over a tile)
-inline void apply_op32(const SwOp& o, const double* mt, double* v /* 64: re, im interleaved */, int u0 = 0,
-                       int u1 = 0) {
-    auto re = [&](int i) -> double& { return v[2 * i]; };
-    auto im = [&](int i) -> double& { return v[2 * i + 1]; };
+__host__ __device__ inline void apply_op32(const SwOp& o, const double* mt, double* v /* 64: re, im */,
+                                           int u0 = 0, int u1 = 0) {
     if (o.type == OP_U1) {
         const int b = 1 << o.k0;
         for (int i = 0; i < 32; ++i) {
             if (i & b) continue;
             const int j = i | b;
-            const double xr = re(i), xi = im(i), yr = re(j), yi = im(j);
-            re(i) = mt[0] * xr - mt[1] * xi + mt[2] * yr - mt[3] * yi;
-            im(i) = mt[0] * xi + mt[1] * xr + mt[2] * yi + mt[3] * yr;
-            re(j) = mt[4] * xr - mt[5] * xi + mt[6] * yr - mt[7] * yi;
-            im(j) = mt[4] * xi + mt[5] * xr + mt[6] * yi + mt[7] * yr;
+            const double xr = v[2 * i], xi = v[2 * i + 1], yr = v[2 * j], yi = v[2 * j + 1];
+            v[2 * i] = dsub(dadd(dsub(dmul(mt[0], xr), dmul(mt[1], xi)), dmul(mt[2], yr)), dmul(mt[3], yi));
+            v[2 * i + 1] = dadd(dadd(dadd(dmul(mt[0], xi), dmul(mt[1], xr)), dmul(mt[2], yi)), dmul(mt[3], yr));
+            v[2 * j] = dsub(dadd(dsub(dmul(mt[4], xr), dmul(mt[5], xi)), dmul(mt[6], yr)), dmul(mt[7], yi));
+            v[2 * j + 1] = dadd(dadd(dadd(dmul(mt[4], xi), dmul(mt[5], xr)), dmul(mt[6], yi)), dmul(mt[7], yr));
         }
-    } else if (o.type == OP_D1) {
+    } else if (o.type == OP_D1 || o.type == OP_ZZ) {
         for (int i = 0; i < 32; ++i) {
-            const int bit = o.k0 >= 0 ? (i >> o.k0) & 1 : u0;
-            const double dr = bit ? mt[2] : mt[0], di = bit ? mt[3] : mt[1];
-            const double xr = re(i), xi = im(i);
-            re(i) = xr * dr - xi * di;
-            im(i) = xr * di + xi * dr;
+            bool second;
+            if (o.type == OP_D1) {
+                second = (o.k0 >= 0 ? (i >> o.k0) & 1 : u0) != 0;
+            } else {   // diag(en, ep, ep, en): the second entry for differing bits
+                const int b0 = o.k0 >= 0 ? (i >> o.k0) & 1 : u0, b1 = o.k1 >= 0 ? (i >> o.k1) & 1 : u1;
+                second = (b0 ^ b1) != 0;
+            }
+            const double dr = second ? mt[2] : mt[0], di = second ? mt[3] : mt[1];
+            const double xr = v[2 * i], xi = v[2 * i + 1];
+            v[2 * i] = dsub(dmul(xr, dr), dmul(xi, di));
+            v[2 * i + 1] = dadd(dmul(xr, di), dmul(xi, dr));
         }
     } else if (o.type == OP_CX) {
         const int t = 1 << o.k1;
         for (int i = 0; i < 32; ++i)
             if (!(i & t) && (o.k0 >= 0 ? (i >> o.k0) & 1 : u0)) {
-                std::swap(re(i), re(i | t));
-                std::swap(im(i), im(i | t));
+                const double ar = v[2 * i], ai = v[2 * i + 1];
+                v[2 * i] = v[2 * (i | t)];
+                v[2 * i + 1] = v[2 * (i | t) + 1];
+                v[2 * (i | t)] = ar;
+                v[2 * (i | t) + 1] = ai;
             }
     } else if (o.type == OP_CZ) {
         for (int i = 0; i < 32; ++i) {
             const int b0 = o.k0 >= 0 ? (i >> o.k0) & 1 : u0, b1 = o.k1 >= 0 ? (i >> o.k1) & 1 : u1;
-            if (b0 && b1) { re(i) = -re(i); im(i) = -im(i); }
-        }
-    } else if (o.type == OP_ZZ) {
-        for (int i = 0; i < 32; ++i) {
-            const int b0 = o.k0 >= 0 ? (i >> o.k0) & 1 : u0, b1 = o.k1 >= 0 ? (i >> o.k1) & 1 : u1;
-            const bool diff = (b0 ^ b1) != 0;
-            const double dr = diff ? mt[2] : mt[0], di = diff ? mt[3] : mt[1];
-            const double xr = re(i), xi = im(i);
-            re(i) = xr * dr - xi * di;
-            im(i) = xr * di + xi * dr;
+            if (b0 && b1) {
+                v[2 * i] = -v[2 * i];
+                v[2 * i + 1] = -v[2 * i + 1];
+            }
         }
     }
 }
 
-inline float tf32_round(float x) {
+__host__ __device__ inline float tf32_round(float x) {
+#ifdef __CUDA_ARCH__
+    uint32_t b = __float_as_uint(x);
+#else
     uint32_t b;
     std::memcpy(&b, &x, 4);
+#endif
     if ((b & 0x7F800000u) != 0x7F800000u) {   // finite: round to nearest, ties away, at 10 mantissa bits
         b += 0x1000u;
         b &= 0xFFFFE000u;
     }
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(b);
+#else
     float r;
     std::memcpy(&r, &b, 4);
     return r;
+#endif
 }
 
-inline size_t dense_offset(int c, int k) {   // in floats
+__host__ __device__ inline size_t dense_offset(int c, int k) {   // in floats
     return (size_t)(c / 8) * 512 + (size_t)(k / 4) * 32 + (size_t)(c % 8) * 4 + (size_t)(k % 4);
 }
 
-// U (column-major over inputs: U[i][col] = amplitude i of the image of basis col) -> operand image
-inline void dense_image(const std::vector<double>& U /* 32 x 32 complex, [col][i] re/im */, float* out) {
-    for (int col = 0; col < 32; ++col)
-        for (int i = 0; i < 32; ++i) {
-            const double ur = U[(size_t)col * 64 + 2 * i], ui = U[(size_t)col * 64 + 2 * i + 1];
-            // output i, input col
-            const double vals[2][2] = {{ur, -ui}, {ui, ur}};
-            for (int rp = 0; rp < 2; ++rp)
-                for (int r = 0; r < 2; ++r) {
-                    const double x = vals[rp][r];
-                    const float f = (float)x;
-                    const float hi = tf32_round(f);
-                    const float lo = (float)(x - (double)hi);
-                    const size_t off = dense_offset(2 * i + rp, 2 * col + r);
-                    out[off] = hi;
-                    out[DENSE_FLOATS + off] = lo;
-                }
-        }
-}
-
 // IEEE binary16 bits of x, rounded to nearest even (subnormals kept; |x| < 65520 here)
-inline uint16_t f16_bits(double x) {
-    const uint16_t sign = std::signbit(x) ? 0x8000u : 0u;
-    const double a = std::fabs(x);
+__host__ __device__ inline uint16_t f16_bits(double x) {
+    const uint16_t sign = signbit(x) ? 0x8000u : 0u;
+    const double a = fabs(x);
     if (a == 0.0) return sign;
     if (a >= 65520.0) return (uint16_t)(sign | 0x7C00u);
     int e = 0;
-    const double m = std::frexp(a, &e);   // a = m * 2^e, m in [0.5, 1)
-    int E = e - 1;                        // a = (2m) * 2^E
-    if (E < -14) return (uint16_t)(sign | (uint16_t)std::nearbyint(a * 16777216.0));   // units of 2^-24
-    double q = std::nearbyint(m * 2048.0);   // 11 significant bits, in [1024, 2048]
+    const double m = frexp(a, &e);   // a = m * 2^e, m in [0.5, 1)
+    int E = e - 1;                   // a = (2m) * 2^E
+    if (E < -14) return (uint16_t)(sign | (uint16_t)nearbyint(a * 16777216.0));   // units of 2^-24
+    double q = nearbyint(m * 2048.0);   // 11 significant bits, in [1024, 2048]
     if (q == 2048.0) { q = 1024.0; E += 1; }
     if (E > 15) return (uint16_t)(sign | 0x7C00u);
     return (uint16_t)(sign | (uint16_t)(((E + 15) << 10) | ((int)q - 1024)));
 }
 
-inline double f16_value(uint16_t h) {
+__host__ __device__ inline double f16_value(uint16_t h) {
     const int e = (h >> 10) & 0x1F, f = h & 0x3FF;
-    double v = e == 0 ? std::ldexp((double)f, -24) : std::ldexp((double)(1024 + f), e - 25);
+    double v = e == 0 ? ldexp((double)f, -24) : ldexp((double)(1024 + f), e - 25);
     return (h & 0x8000u) ? -v : v;
 }
 
-inline size_t dense_offset16(int c, int k) {   // in 16-bit elements
+__host__ __device__ inline size_t dense_offset16(int c, int k) {   // in 16-bit elements
     return (size_t)(c / 8) * 512 + (size_t)(k / 8) * 64 + (size_t)(c % 8) * 8 + (size_t)(k % 8);
 }
 
-inline void dense_image_f16(const std::vector<double>& U /* as dense_image */, uint32_t* out_words) {
-    uint16_t* out = reinterpret_cast<uint16_t*>(out_words);
-    const double sc = std::ldexp(1.0, DENSE_F16_SCALE_LOG2);
-    for (int col = 0; col < 32; ++col)
-        for (int i = 0; i < 32; ++i) {
-            const double ur = U[(size_t)col * 64 + 2 * i], ui = U[(size_t)col * 64 + 2 * i + 1];
-            const double vals[2][2] = {{ur, -ui}, {ui, ur}};
-            for (int rp = 0; rp < 2; ++rp)
-                for (int r = 0; r < 2; ++r) {
-                    const double x = vals[rp][r] * sc;
+// Column col of an operand image from u = U e_col (32 complex, re/im interleaved): the entries
+// B[2i'+r'][2col+r] of the real form of U, split into the format's high and low parts.
+__host__ __device__ inline void dense_image_column(const double* u, int col, uint32_t* out_words, int fmt) {
+    const double sc = fmt == DENSE_F16 ? (double)(1u << DENSE_F16_SCALE_LOG2) : 1.0;
+    for (int i = 0; i < 32; ++i) {
+        const double ur = u[2 * i], ui = u[2 * i + 1];
+        const double vals[2][2] = {{ur, -ui}, {ui, ur}};
+        for (int rp = 0; rp < 2; ++rp)
+            for (int r = 0; r < 2; ++r) {
+                if (fmt == DENSE_F16) {
+                    uint16_t* out = reinterpret_cast<uint16_t*>(out_words);
+                    const double x = dmul(vals[rp][r], sc);
                     const uint16_t hi = f16_bits(x);
-                    const uint16_t lo = f16_bits(x - f16_value(hi));
+                    const uint16_t lo = f16_bits(dsub(x, f16_value(hi)));
                     const size_t off = dense_offset16(2 * i + rp, 2 * col + r);
                     out[off] = hi;
                     out[DENSE_F16_WORDS + off] = lo;
+                } else {
+                    float* out = reinterpret_cast<float*>(out_words);
+                    const double x = vals[rp][r];
+                    const float hi = tf32_round((float)x);
+                    const float lo = (float)dsub(x, (double)hi);
+                    const size_t off = dense_offset(2 * i + rp, 2 * col + r);
+                    out[off] = hi;
+                    out[DENSE_FLOATS + off] = lo;
                 }
-        }
+            }
+    }
 }
 
 // Tensor-core plans: every phase becomes one OP_DENSE.  Gate qubits that are register
@@ -929,9 +962,38 @@ __host__ __device__ inline uint32_t dense_vq(const SwOp& o, int j) {
     }
 }
 
+// One operand image to build: a (phase, variant) pair -- the image slot, the phase's range in
+// the op list before fusion, and the values of its qubits outside the tile.
+struct DenseJob {
+    uint32_t slot, op_begin, op_end, var, nvq;
+    uint32_t vq[DENSE_MAX_VQ];
+};
+
+// Column col of the job's 32x32 unitary: the phase's ops applied in order to e_col.
+__host__ __device__ inline void dense_job_column(const DenseJob& jb, const SwOp* ops, const double* mats, int col,
+                                                 double* v /* 64 */) {
+    for (int k = 0; k < 64; ++k) v[k] = 0.0;
+    v[2 * col] = 1.0;
+    for (uint32_t o = jb.op_begin; o < jb.op_end; ++o) {
+        const SwOp& op = ops[o];
+        int u0 = 0, u1 = 0;
+        for (uint32_t k = 0; k < jb.nvq; ++k) {
+            if (jb.vq[k] == op.q0) u0 = (int)((jb.var >> k) & 1u);
+            if (jb.vq[k] == op.q1) u1 = (int)((jb.var >> k) & 1u);
+        }
+        apply_op32(op, mats + 2 * (size_t)op.mat, v, u0, u1);
+    }
+}
+
+// Rewrites every phase into one OP_DENSE (its image slots and outside qubits), leaving in
+// *jobs the images to build and in *pre_ops the op list they read (the ops before fusion);
+// with build_images the images are built here, on the host's cores, else the caller builds
+// them (the library does so on the GPU, bit-identically).  Returns false when a phase cannot
+// be one dense op.
 inline bool fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& phases, std::vector<SwOp>& ops,
                        const std::vector<double>& mats, std::vector<uint32_t>& images, uint64_t* ndense,
-                       int fmt = DENSE_TF32) {
+                       int fmt = DENSE_TF32, std::vector<DenseJob>* jobs_out = nullptr,
+                       std::vector<SwOp>* pre_ops = nullptr, bool build_images = true) {
     const size_t words = dense_image_words(fmt);
     std::vector<SwOp> out;
     std::vector<uint32_t> sweep_of(phases.size(), 0);
@@ -940,14 +1002,7 @@ inline bool fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& ph
         descs[d].img_begin = 0;
         descs[d].img_count = 0;
     }
-    // one job per (phase, variant): the image slot, the phase's op range and its outside qubits
-    struct Job {
-        size_t slot;
-        uint32_t op_begin, op_end, var;
-        uint32_t vq[DENSE_MAX_VQ];
-        uint32_t nvq;
-    };
-    std::vector<Job> jobs;
+    std::vector<DenseJob> jobs;
     size_t nimg = 0;
     for (size_t pi = 0; pi < phases.size(); ++pi) {
         auto& ph = phases[pi];
@@ -971,8 +1026,8 @@ inline bool fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& ph
         const size_t first = nimg;
         const uint32_t nvar = 1u << vq.size();
         for (uint32_t var = 0; var < nvar; ++var) {
-            Job jb{};
-            jb.slot = nimg++;
+            DenseJob jb{};
+            jb.slot = (uint32_t)nimg++;
             jb.op_begin = ph.op_begin;
             jb.op_end = ph.op_end;
             jb.var = var;
@@ -999,43 +1054,33 @@ inline bool fuse_dense(std::vector<SweepDesc>& descs, std::vector<PhaseDesc>& ph
         ph.op_end = (uint32_t)out.size();
         ++*ndense;
     }
-    // build the images (the products in f64 and their TF32 split) on the host's cores
     images.assign(nimg * words, 0u);
-    auto work = [&](size_t j0, size_t j1) {
-        std::vector<double> U(32 * 64);
-        for (size_t jj = j0; jj < j1; ++jj) {
-            const Job& jb = jobs[jj];
-            auto val = [&](uint32_t q) {
-                for (uint32_t k = 0; k < jb.nvq; ++k)
-                    if (jb.vq[k] == q) return (int)((jb.var >> k) & 1u);
-                return 0;
-            };
-            std::fill(U.begin(), U.end(), 0.0);
-            for (int col = 0; col < 32; ++col) {
-                double* v = &U[(size_t)col * 64];
-                v[2 * col] = 1.0;
-                for (uint32_t o = jb.op_begin; o < jb.op_end; ++o) {
-                    const SwOp& op = ops[o];
-                    apply_op32(op, mats.data() + 2 * (size_t)op.mat, v, val(op.q0), val(op.q1));
+    if (build_images) {
+        auto work = [&](size_t j0, size_t j1) {
+            double v[64];
+            for (size_t jj = j0; jj < j1; ++jj)
+                for (int col = 0; col < 32; ++col) {
+                    dense_job_column(jobs[jj], ops.data(), mats.data(), col, v);
+                    dense_image_column(v, col, images.data() + (size_t)jobs[jj].slot * words, fmt);
                 }
+        };
+        const size_t nt =
+            std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), (jobs.size() + 15) / 16));
+        if (nt <= 1) {
+            work(0, jobs.size());
+        } else {
+            std::vector<std::thread> pool;
+            const size_t per = (jobs.size() + nt - 1) / nt;
+            for (size_t t = 0; t < nt; ++t) {
+                const size_t j0 = t * per, j1 = std::min(jobs.size(), j0 + per);
+                if (j0 < j1) pool.emplace_back(work, j0, j1);
             }
-            if (fmt == DENSE_F16) dense_image_f16(U, images.data() + jb.slot * words);
-            else dense_image(U, reinterpret_cast<float*>(images.data() + jb.slot * words));
+            for (auto& th : pool) th.join();
         }
-    };
-    const size_t nt = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), (jobs.size() + 15) / 16));
-    if (nt <= 1) {
-        work(0, jobs.size());
-    } else {
-        std::vector<std::thread> pool;
-        const size_t per = (jobs.size() + nt - 1) / nt;
-        for (size_t t = 0; t < nt; ++t) {
-            const size_t j0 = t * per, j1 = std::min(jobs.size(), j0 + per);
-            if (j0 < j1) pool.emplace_back(work, j0, j1);
-        }
-        for (auto& th : pool) th.join();
     }
+    if (jobs_out) jobs_out->swap(jobs);
     if (out.empty()) out.push_back(SwOp{});
+    if (pre_ops) *pre_ops = ops;
     ops.swap(out);
     return true;
 }

@@ -1253,6 +1253,20 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
     }
 }
 
+// Operand images of a tensor-core plan, built on the GPU: one CTA of 32 threads per image, one
+// thread per column (the phase's ops applied to e_col in exactly rounded f64, the same
+// arithmetic as the host restatement in rq_plan.cuh, so the images are bit-identical).
+__global__ void __launch_bounds__(32) k_dense_images(const SwOp* __restrict__ ops, const double* __restrict__ mats,
+                                                     const DenseJob* __restrict__ jobs, uint32_t njobs,
+                                                     uint32_t* __restrict__ images, int fmt, uint32_t words) {
+    double v[64];
+    for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
+        const DenseJob jb = jobs[j];
+        dense_job_column(jb, ops, mats, (int)threadIdx.x, v);
+        dense_image_column(v, (int)threadIdx.x, images + (size_t)jb.slot * words, fmt);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // host planner
 // ---------------------------------------------------------------------------
@@ -1327,6 +1341,25 @@ struct rq_plan {
     size_t smem = 0;
     uint32_t rb = 0;
     rq_plan_stats stats{};
+    // Rebinding to new gate values with the same structure (kinds and qubits): the planner's
+    // decisions depend on the structure only, so the sweeps' local sets and the phase plans
+    // are kept; new values re-derive the fused matrices (take_sweep over the same local sets)
+    // and, for tensor-core plans, the operand images on the GPU.
+    bool rebindable = false;
+    uint32_t m = 0, c = 0;
+    std::vector<uint64_t> sweep_L;                       // planner's local sets (unpadded)
+    std::vector<std::vector<PhasePlan>> phase_plans;     // per sweep
+    std::vector<std::vector<uint32_t>> sig;              // per sweep: type | q0 << 8 | q1 << 16 per op
+    std::vector<uint32_t> shape;                         // kind | q0 << 8 | q1 << 16 per gate
+    int dense_fmt = DENSE_TF32;
+    size_t off_pre = 0, off_m64 = 0, off_jobs = 0;       // tensor-core plans: image-building inputs
+    uint32_t njobs = 0;
+    size_t nmats = 0;                                    // doubles in the matrix table
+    mutable cudaEvent_t done = nullptr;                  // after the last launch sequence
+    mutable cudaStream_t done_stream = nullptr;
+    unsigned char* pin = nullptr;                        // pinned staging of new matrix tables
+    size_t pin_cap = 0;
+    cudaEvent_t pin_free = nullptr;                      // the last copy out of `pin` has finished
 };
 
 namespace rq {
@@ -1343,6 +1376,43 @@ static uint32_t sweep_local_qubits(uint32_t nq, int32_t prec) {
 
 // tc_passes > 0 turns every phase into one dense 32x32 op applied on the tensor cores
 // (complex f32 states, m in {12, 13} only); tc_min_ops is kept for the ABI of this helper.
+namespace {
+
+uint32_t shape_of(const rq_gate& g) { return (uint32_t)g.kind | ((g.q0 & 0xFFu) << 8) | ((g.q1 & 0xFFu) << 16); }
+
+std::vector<uint32_t> sweep_signature(const Sweep& sw) {
+    std::vector<uint32_t> sig;
+    sig.reserve(sw.ops.size());
+    for (const auto& g : sw.ops) sig.push_back((uint32_t)g.type | ((g.q0 & 0xFFu) << 8) | ((g.q1 & 0xFFu) << 16));
+    return sig;
+}
+
+// the fused matrix table in the kernels' precision
+void narrow_mats(const std::vector<double>& mats, int32_t prec, unsigned char* dst) {
+    if (prec == RQ_F32) {
+        float* f = reinterpret_cast<float*>(dst);
+        for (size_t k = 0; k < mats.size(); ++k) f[k] = (float)mats[k];
+    } else {
+        std::memcpy(dst, mats.data(), mats.size() * sizeof(double));
+    }
+}
+
+// the operand images of a tensor-core plan from its ops and f64 matrices (already on the device)
+int build_images(const rq_plan* P, cudaStream_t st) {
+    if (!P->njobs) return RQ_OK;
+    const size_t words = dense_image_words(P->dense_fmt);
+    const unsigned grid = (unsigned)std::min<uint32_t>(P->njobs, 65535u);
+    k_dense_images<<<grid, 32, 0, st>>>(reinterpret_cast<const SwOp*>(P->dev + P->off_pre),
+                                        reinterpret_cast<const double*>(P->dev + P->off_m64),
+                                        reinterpret_cast<const DenseJob*>(P->dev + P->off_jobs), P->njobs,
+                                        reinterpret_cast<uint32_t*>(P->dev + P->off_img), P->dense_fmt,
+                                        (uint32_t)words);
+    RQ_CUDA(cudaGetLastError());
+    return RQ_OK;
+}
+
+}  // namespace
+
 int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out, int tc_passes,
                uint32_t tc_min_ops, uint32_t m_override) {
     rq_plan* P = new rq_plan();
@@ -1352,6 +1422,8 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
     const uint32_t nq = s->nq;
     const uint32_t rb = s->prec == RQ_F32 ? 5 : 4;
     const uint64_t S = s->bytes();
+    for (uint64_t k = 0; k < n; ++k)
+        if (gates[k].kind != RQ_GATE_BARRIER) P->shape.push_back(shape_of(gates[k]));
     if (mode == RQ_EXEC_PER_GATE || nq < rb + 2) {
         P->mode = RQ_EXEC_PER_GATE;
         for (uint64_t k = 0; k < n; ++k)
@@ -1367,6 +1439,7 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
                      g.kind == RQ_GATE_TDG || g.kind == RQ_GATE_PHASE) b = S;
             P->stats.hbm_bytes += b;
         }
+        P->rebindable = true;
         *out = P;
         return RQ_OK;
     }
@@ -1384,16 +1457,26 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
     }
     const bool tcp = tc_passes > 0;
     auto sweeps = plan_sweeps(pg, nq, m, c, tcp);
+    for (const auto& sw : sweeps) {   // the structure, before build_program pads the local sets
+        P->sweep_L.push_back(sw.L);
+        P->sig.push_back(sweep_signature(sw));
+    }
+    P->m = m;
+    P->c = c;
 
     std::vector<PhaseDesc> phases;
     std::vector<SwOp> ops;
     std::vector<double> mats;
-    build_program(sweeps, nq, m, c, rb, s->prec == RQ_F32 ? 2 : 1, P->descs, phases, ops, mats, tcp);
+    build_program(sweeps, nq, m, c, rb, s->prec == RQ_F32 ? 2 : 1, P->descs, phases, ops, mats, tcp, nullptr,
+                  &P->phase_plans);
     std::vector<uint32_t> images;
+    std::vector<DenseJob> jobs;
+    std::vector<SwOp> pre_ops;
     uint64_t ndense = 0;
     if (tcp) {
-        // images resident in shared memory next to one tile
-        if (!fuse_dense(P->descs, phases, ops, mats, images, &ndense, tc_passes == TC_F16 ? DENSE_F16 : DENSE_TF32)) {
+        P->dense_fmt = tc_passes == TC_F16 ? DENSE_F16 : DENSE_TF32;
+        // the images are built on the GPU below, from the ops before fusion and their f64 matrices
+        if (!fuse_dense(P->descs, phases, ops, mats, images, &ndense, P->dense_fmt, &jobs, &pre_ops, false)) {
             delete P;
             return fail(RQ_ERR_CIRCUIT, "tensor-core plan: a phase touches more than 5 qubits outside the tile");
         }
@@ -1407,22 +1490,27 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
         P->mode = RQ_EXEC_SWEEP_TC;
     }
 
-    size_t mat_elem = s->prec == RQ_F32 ? sizeof(float) : sizeof(double);
+    const size_t mat_elem = s->prec == RQ_F32 ? sizeof(float) : sizeof(double);
+    auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
     P->off_ph = 0;
-    P->off_ops = (P->off_ph + phases.size() * sizeof(PhaseDesc) + 255) & ~size_t(255);
-    P->off_mat = (P->off_ops + ops.size() * sizeof(SwOp) + 255) & ~size_t(255);
-    P->off_img = (P->off_mat + mats.size() * mat_elem + 255) & ~size_t(255);
-    size_t total = P->off_img + images.size() * sizeof(uint32_t);
-    std::vector<unsigned char> host(total);
-    if (!images.empty()) std::memcpy(host.data() + P->off_img, images.data(), images.size() * sizeof(uint32_t));
+    P->off_ops = align(P->off_ph + phases.size() * sizeof(PhaseDesc));
+    P->off_mat = align(P->off_ops + ops.size() * sizeof(SwOp));
+    P->off_img = align(P->off_mat + mats.size() * mat_elem);
+    P->off_pre = align(P->off_img + images.size() * sizeof(uint32_t));
+    P->off_m64 = align(P->off_pre + pre_ops.size() * sizeof(SwOp));
+    P->off_jobs = align(P->off_m64 + (tcp ? mats.size() * sizeof(double) : 0));
+    const size_t total = P->off_jobs + jobs.size() * sizeof(DenseJob);
+    std::vector<unsigned char> host(total, 0);
     std::memcpy(host.data() + P->off_ph, phases.data(), phases.size() * sizeof(PhaseDesc));
     std::memcpy(host.data() + P->off_ops, ops.data(), ops.size() * sizeof(SwOp));
-    if (s->prec == RQ_F32) {
-        float* f = reinterpret_cast<float*>(host.data() + P->off_mat);
-        for (size_t k = 0; k < mats.size(); ++k) f[k] = (float)mats[k];
-    } else {
-        std::memcpy(host.data() + P->off_mat, mats.data(), mats.size() * sizeof(double));
+    narrow_mats(mats, s->prec, host.data() + P->off_mat);
+    if (tcp) {
+        std::memcpy(host.data() + P->off_pre, pre_ops.data(), pre_ops.size() * sizeof(SwOp));
+        std::memcpy(host.data() + P->off_m64, mats.data(), mats.size() * sizeof(double));
+        std::memcpy(host.data() + P->off_jobs, jobs.data(), jobs.size() * sizeof(DenseJob));
     }
+    P->njobs = (uint32_t)jobs.size();
+    P->nmats = mats.size();
     cudaError_t e = cudaMalloc((void**)&P->dev, total);
     if (e == cudaSuccess) e = cudaMemcpy(P->dev, host.data(), total, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
@@ -1430,10 +1518,21 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
         delete P;
         return cuda_fail(e, "plan upload");
     }
+    int rc = build_images(P, s->stream);
+    if (rc == RQ_OK) {
+        e = cudaStreamSynchronize(s->stream);   // a plan is complete when it is handed out
+        if (e != cudaSuccess) rc = cuda_fail(e, "operand images");
+    }
+    if (rc != RQ_OK) {
+        cudaFree(P->dev);
+        delete P;
+        return rc;
+    }
     P->smem = ((size_t)1 << m) * s->elem_bytes();
     if (tcp) P->host_phases = phases;
     P->ntiles = 1ull << (nq - m);
     P->rb = rb;
+    P->rebindable = true;
     P->stats.gates = filtered.size();
     P->stats.sweeps = P->descs.size();
     P->stats.launches = P->descs.size();
@@ -1445,6 +1544,88 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
                                                : tc_passes == 1 ? RQ_EXEC_SWEEP_TC_FAST : RQ_EXEC_SWEEP_TC;
     P->stats.local_qubits = m;
     *out = P;
+    return RQ_OK;
+}
+
+bool plan_same_shape(const rq_plan* P, const rq_gate* gates, uint64_t n) {
+    uint64_t k = 0;
+    for (uint64_t j = 0; j < n; ++j) {
+        if (gates[j].kind == RQ_GATE_BARRIER) continue;
+        if (k >= P->shape.size() || P->shape[k] != shape_of(gates[j])) return false;
+        ++k;
+    }
+    return k == P->shape.size();
+}
+
+// New gate values for a plan of the same gate structure: re-derive each sweep's fused
+// matrices from the planner's recorded local sets, check that every sweep takes the same ops,
+// and replace the matrix table (and, for tensor-core plans, rebuild the operand images on the
+// GPU) in stream order on s's stream.  RQ_ERR_CIRCUIT when the structure does not match (the
+// plan is then unchanged).
+int plan_rebind(rq_state* s, rq_plan* P, const rq_gate* gates, uint64_t n) {
+    if (!P->rebindable || !plan_same_shape(P, gates, n))
+        return fail(RQ_ERR_CIRCUIT, "circuit error: the gate list's kinds and qubits differ from the plan's");
+    if (P->mode == RQ_EXEC_PER_GATE) {
+        uint64_t k = 0;
+        for (uint64_t j = 0; j < n; ++j)
+            if (gates[j].kind != RQ_GATE_BARRIER) P->gates[k++] = gates[j];
+        return RQ_OK;
+    }
+    std::vector<rq_gate> filtered;
+    filtered.reserve(P->shape.size());
+    for (uint64_t j = 0; j < n; ++j)
+        if (gates[j].kind != RQ_GATE_BARRIER) filtered.push_back(gates[j]);
+    std::vector<PGate> pg;
+    if (!to_pgates(filtered.data(), filtered.size(), pg)) return fail(RQ_ERR_CIRCUIT, "circuit error: unplannable gate");
+    std::vector<Sweep> sweeps;
+    std::vector<char> taken(pg.size(), 0);
+    size_t first = 0;
+    for (size_t k = 0; k < P->sweep_L.size(); ++k) {
+        Sweep sw = take_sweep(pg, taken, first, P->sweep_L[k], P->nq, P->m);
+        sw.L = P->sweep_L[k];
+        while (first < pg.size() && taken[first]) ++first;
+        if (sweep_signature(sw) != P->sig[k]) {
+            P->rebindable = false;
+            return fail(RQ_ERR_CIRCUIT, "circuit error: the plan's sweeps cannot be re-derived for these gates");
+        }
+        sweeps.push_back(std::move(sw));
+    }
+    if (first != pg.size()) {
+        P->rebindable = false;
+        return fail(RQ_ERR_CIRCUIT, "circuit error: the plan's sweeps cannot be re-derived for these gates");
+    }
+    std::vector<SweepDesc> descs;
+    std::vector<PhaseDesc> phases;
+    std::vector<SwOp> ops;
+    std::vector<double> mats;
+    build_program(sweeps, P->nq, P->m, P->c, P->rb, P->prec == RQ_F32 ? 2 : 1, descs, phases, ops, mats,
+                  P->tc_passes > 0, &P->phase_plans, nullptr);
+    if (mats.size() != P->nmats) {
+        P->rebindable = false;
+        return fail(RQ_ERR_CIRCUIT, "circuit error: the plan's matrix table changed shape");
+    }
+    // stage the new table in pinned memory (once the previous copy out of it has finished), then
+    // copy it in stream order after every earlier launch of this plan, on any stream
+    const bool tc = P->tc_passes > 0;
+    const size_t bytes = mats.size() * (tc || P->prec == RQ_F64 ? sizeof(double) : sizeof(float));
+    if (P->pin_free) RQ_CUDA(cudaEventSynchronize(P->pin_free));
+    else RQ_CUDA(cudaEventCreateWithFlags(&P->pin_free, cudaEventDisableTiming));
+    if (P->pin_cap < bytes) {
+        if (P->pin) cudaFreeHost(P->pin);
+        P->pin = nullptr;
+        P->pin_cap = 0;
+        RQ_CUDA(cudaMallocHost((void**)&P->pin, bytes));
+        P->pin_cap = bytes;
+    }
+    if (tc) std::memcpy(P->pin, mats.data(), bytes);
+    else narrow_mats(mats, P->prec, P->pin);
+    if (P->done && P->done_stream != s->stream) RQ_CUDA(cudaStreamWaitEvent(s->stream, P->done, 0));
+    RQ_CUDA(cudaMemcpyAsync(P->dev + (tc ? P->off_m64 : P->off_mat), P->pin, bytes, cudaMemcpyHostToDevice, s->stream));
+    RQ_CUDA(cudaEventRecord(P->pin_free, s->stream));
+    if (tc) RQ_TRY(build_images(P, s->stream));
+    if (!P->done) RQ_CUDA(cudaEventCreateWithFlags(&P->done, cudaEventDisableTiming));
+    RQ_CUDA(cudaEventRecord(P->done, s->stream));
+    P->done_stream = s->stream;
     return RQ_OK;
 }
 
@@ -1594,7 +1775,23 @@ static int launch_tc16(rq_state* s, const rq_plan* P, const PhaseDesc* ph, const
     return RQ_OK;
 }
 
+static int plan_launch_kernels(rq_state* s, const rq_plan* P);
+
+// Launch a prepared plan on s's stream; the plan remembers the stream and an event after the
+// launches, so that new matrix tables (plan_rebind) are written only once they have run.
 int plan_launch(rq_state* s, const rq_plan* P) {
+    // the plan's last use (launches or new tables) on another stream comes first
+    if (P->done && P->done_stream != s->stream) RQ_CUDA(cudaStreamWaitEvent(s->stream, P->done, 0));
+    RQ_TRY(plan_launch_kernels(s, P));
+    if (P->mode != RQ_EXEC_PER_GATE) {
+        if (!P->done) RQ_CUDA(cudaEventCreateWithFlags(&P->done, cudaEventDisableTiming));
+        RQ_CUDA(cudaEventRecord(P->done, s->stream));
+        P->done_stream = s->stream;
+    }
+    return RQ_OK;
+}
+
+static int plan_launch_kernels(rq_state* s, const rq_plan* P) {
     if (P->mode == RQ_EXEC_PER_GATE) {
         for (const auto& g : P->gates) RQ_TRY(apply_one_gate(s, g));
         return RQ_OK;
@@ -1642,10 +1839,11 @@ int plan_launch(rq_state* s, const rq_plan* P) {
 
 void plan_free(rq_plan* P) {
     if (!P) return;
-    if (P->dev) {
-        cudaSetDevice(P->device);
-        cudaFree(P->dev);
-    }
+    cudaSetDevice(P->device);
+    if (P->dev) cudaFree(P->dev);
+    if (P->pin) cudaFreeHost(P->pin);
+    if (P->pin_free) cudaEventDestroy(P->pin_free);
+    if (P->done) cudaEventDestroy(P->done);
     delete P;
 }
 
@@ -1717,6 +1915,19 @@ int apply_sweeps(rq_state* s, const rq_gate* gates, uint64_t n, int tc_passes, u
             c.hash == h &&
             c.gates.size() == n && std::memcmp(c.gates.data(), gates, n * sizeof(rq_gate)) == 0) {
             std::rotate(g_plans.begin() + k, g_plans.begin() + k + 1, g_plans.end());   // most recent last
+            return plan_launch(s, g_plans.back().plan);
+        }
+    }
+    // the same gate structure with other angles (a driver's next evaluation): new matrix tables
+    // and operand images for the cached plan, no planning
+    for (size_t k = g_plans.size(); k-- > 0;) {
+        CachedPlan& c = g_plans[k];
+        if (c.device == s->device && c.nq == s->nq && c.prec == s->prec && c.passes == tc_passes && c.m == m &&
+            c.gates.size() == n && c.plan->rebindable && plan_same_shape(c.plan, gates, n)) {
+            if (plan_rebind(s, c.plan, gates, n) != RQ_OK) break;   // not re-derivable: plan afresh below
+            c.gates.assign(gates, gates + n);
+            c.hash = h;
+            std::rotate(g_plans.begin() + k, g_plans.begin() + k + 1, g_plans.end());
             return plan_launch(s, g_plans.back().plan);
         }
     }

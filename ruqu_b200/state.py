@@ -289,6 +289,13 @@ class Plan:
     def execute(self, state: QuantumState) -> None:
         check(lib.rq_plan_execute(state.handle, self._h))
 
+    def update(self, state: QuantumState, gates) -> None:
+        """New angles (or matrices) for the same gate kinds and qubits (rq_plan_update): the
+        planning is kept, the matrix tables and operand images are rebuilt in stream order on
+        the state's stream.  Raises CircuitError if the structure differs."""
+        arr = gates if isinstance(gates, C.Array) else gates_to_array(gates)
+        check(lib.rq_plan_update(state.handle, self._h, arr, len(gates)))
+
     def stats(self) -> dict:
         st = RqPlanStats()
         check(lib.rq_plan_get_stats(self._h, C.byref(st)))

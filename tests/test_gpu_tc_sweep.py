@@ -159,3 +159,59 @@ def test_repeated_gate_lists_reuse_their_program_and_changes_are_seen():
     g.apply_gates(changed, rq.RQ_EXEC_SWEEP_TC)
     ref = _oracle_f64(n, changed)
     assert float(np.max(np.abs(g.state_vector() - ref))) < 1e-5
+
+
+@pytest.mark.parametrize("prec,mode", [("f64", rq.RQ_EXEC_SWEEP), ("f32", rq.RQ_EXEC_SWEEP), ("f32", rq.RQ_EXEC_SWEEP_TC),
+                                       ("f32", rq.RQ_EXEC_SWEEP_TC16), ("f64", rq.RQ_EXEC_PER_GATE)])
+def test_plan_update_equals_a_fresh_plan(prec, mode):
+    """rq_plan_update: a plan built for one angle set and given another (same kinds and qubits)
+    computes exactly what a plan built for the new angles computes (bit for bit: the fused
+    matrices are re-derived the same way and the operand images are built by the same GPU
+    kernel), and matches the oracle (1e-12 f64, 1e-5 f32)."""
+    n = 16
+    a = workloads.random_layer_circuit(n, 6, 21)
+    b = workloads.random_layer_circuit(n, 6, 22)   # same structure, new angles
+    sa = QuantumState(n, 0, prec)
+    plan = rq.Plan(sa, a, mode)
+    plan.execute(sa)
+    plan.update(sa, b)
+    sa.reset()
+    plan.execute(sa)
+    got = sa.state_vector()
+    sb = QuantumState(n, 0, prec)
+    fresh = rq.Plan(sb, b, mode)
+    fresh.execute(sb)
+    assert np.array_equal(got, sb.state_vector())
+    tol = 1e-12 if prec == "f64" else 1e-5
+    assert float(np.max(np.abs(got - _oracle_f64(n, b)))) < tol
+
+
+def test_plan_update_rejects_another_structure_and_keeps_the_plan():
+    n = 14
+    a = workloads.random_layer_circuit(n, 4, 5)
+    other = list(a)
+    k = next(i for i, g in enumerate(other) if g[0] == 12)   # move one CNOT
+    other[k] = (12, other[k][1], (other[k][2] + 1) % n if (other[k][2] + 1) % n != other[k][1] else (other[k][2] + 2) % n, 0.0)
+    s = QuantumState(n, 0, "f32")
+    plan = rq.Plan(s, a, rq.RQ_EXEC_SWEEP_TC16)
+    with pytest.raises(rq.CircuitError):
+        plan.update(s, other)
+    with pytest.raises(rq.CircuitError):
+        plan.update(s, a[:-1])
+    plan.execute(s)
+    assert float(np.max(np.abs(s.state_vector() - _oracle_f64(n, a)))) < 1e-5
+
+
+def test_apply_with_new_angles_reuses_the_structure_across_states_and_streams():
+    """apply_gates keeps recent plans by structure: new angles rebuild only the tables, in
+    stream order; two states (two streams) alternating between angle sets both stay exact."""
+    n = 15
+    sets = [workloads.random_layer_circuit(n, 5, 40 + k) for k in range(4)]
+    refs = [_oracle_f64(n, g) for g in sets]
+    s1, s2 = QuantumState(n, 0, "f32"), QuantumState(n, 0, "f32")
+    for rounds in range(2):
+        for k, g in enumerate(sets):
+            st = s1 if k % 2 == 0 else s2
+            st.reset()
+            st.apply_gates(g, rq.RQ_EXEC_SWEEP_TC16)
+            assert float(np.max(np.abs(st.state_vector() - refs[k]))) < 1e-5, (rounds, k)
