@@ -1840,6 +1840,10 @@ static int plan_launch_kernels(rq_state* s, const rq_plan* P) {
 void plan_free(rq_plan* P) {
     if (!P) return;
     cudaSetDevice(P->device);
+    // the plan's last launches and table copies may still be running on another state's
+    // stream: let them finish before the device tables and the pinned staging are released
+    if (P->done) cudaEventSynchronize(P->done);
+    if (P->pin_free) cudaEventSynchronize(P->pin_free);
     if (P->dev) cudaFree(P->dev);
     if (P->pin) cudaFreeHost(P->pin);
     if (P->pin_free) cudaEventDestroy(P->pin_free);
