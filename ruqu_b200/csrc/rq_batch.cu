@@ -1514,6 +1514,9 @@ int rq_qaoa_batch_create(uint32_t ninst, const uint32_t* num_nodes, const uint32
     RQ_CUDA(cudaMemcpy(b->d_eoff, eoff.data(), (ninst + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice));
     RQ_CUDA(cudaMalloc((void**)&b->d_ne, std::max<uint32_t>(1, ninst) * sizeof(uint32_t)));
     if (ninst) RQ_CUDA(cudaMemcpy(b->d_ne, b->ne_of.data(), ninst * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    // the copies above (from pageable memory) may return before their DMA lands, and the
+    // batch's stream is not ordered after them: wait here, once, before any run
+    RQ_CUDA(cudaDeviceSynchronize());
     *out = b.release();
     return RQ_OK;
 }
@@ -2452,6 +2455,9 @@ int rq_vqe_batch_create(uint32_t num_qubits, uint32_t depth, const double* coeff
     RQ_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     RQ_CUDA(cudaEventCreate(&b->ev0));
     RQ_CUDA(cudaEventCreate(&b->ev1));
+    // the table copies above may return before their DMA lands (pageable sources), and the
+    // batch's stream is not ordered after them: wait here, once, before any run
+    RQ_CUDA(cudaDeviceSynchronize());
     *out = b.release();
     return RQ_OK;
 }

@@ -263,7 +263,10 @@ int gemm_bf16(cudaStream_t stream, const __nv_bfloat16* A, int lda, const __nv_b
 int mma_timeout_flag(int* out) {
     int v = 0, zero = 0;
     RQ_CUDA(cudaMemcpyFromSymbol(&v, g_mma_timeout, sizeof(int)));
-    if (v) RQ_CUDA(cudaMemcpyToSymbol(g_mma_timeout, &zero, sizeof(int)));
+    if (v) {
+        RQ_CUDA(cudaMemcpyToSymbol(g_mma_timeout, &zero, sizeof(int)));
+        RQ_CUDA(cudaDeviceSynchronize());
+    }
     *out = v;
     return RQ_OK;
 }
@@ -271,6 +274,7 @@ int mma_timeout_flag(int* out) {
 int mma_set_wait_polls(uint32_t polls) {
     const uint32_t v = polls == RQ_WAIT_LIMIT_DEFAULT ? WAIT_POLLS : polls;
     RQ_CUDA(cudaMemcpyToSymbol(g_mma_wait_polls, &v, sizeof(v)));
+    RQ_CUDA(cudaDeviceSynchronize());   // landed before any later launch, on any stream
     return RQ_OK;
 }
 
@@ -624,7 +628,8 @@ int rq_mlp_create(int32_t in, int32_t h1, int32_t h2, int32_t out, uint64_t seed
     fill(m->off_w1, h1, in);
     fill(m->off_w2, h2, h1);
     fill(m->off_w3, out, h2);
-    RQ_CUDA(cudaMemcpy(m->P, P.data(), m->nparam * sizeof(float), cudaMemcpyHostToDevice));
+    // stream-ordered: the refresh below runs on the network's (non-blocking) stream
+    RQ_CUDA(cudaMemcpyAsync(m->P, P.data(), m->nparam * sizeof(float), cudaMemcpyHostToDevice, m->stream));
     RQ_TRY(mlp_refresh_bf16(m.get()));
     RQ_CUDA(cudaStreamSynchronize(m->stream));
     *res = m.release();

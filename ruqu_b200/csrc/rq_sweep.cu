@@ -1511,10 +1511,16 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
     }
     P->njobs = (uint32_t)jobs.size();
     P->nmats = mats.size();
+    // Upload in stream order on the state's stream: a synchronous copy from pageable memory may
+    // return before its DMA lands, and the state's stream (non-blocking) is not ordered after
+    // the legacy stream, so the kernels below could otherwise read the tables half-written.
     cudaError_t e = cudaMalloc((void**)&P->dev, total);
-    if (e == cudaSuccess) e = cudaMemcpy(P->dev, host.data(), total, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(P->dev, host.data(), total, cudaMemcpyHostToDevice, s->stream);
     if (e != cudaSuccess) {
-        if (P->dev) cudaFree(P->dev);
+        if (P->dev) {
+            cudaStreamSynchronize(s->stream);
+            cudaFree(P->dev);
+        }
         delete P;
         return cuda_fail(e, "plan upload");
     }
@@ -1856,7 +1862,10 @@ rq_plan_stats plan_stats(const rq_plan* p) { return p->stats; }
 int tc_timeout_flag(int* out) {
     int v = 0, zero = 0;
     RQ_CUDA(cudaMemcpyFromSymbol(&v, tc::g_tc_timeout, sizeof(int)));
-    if (v) RQ_CUDA(cudaMemcpyToSymbol(tc::g_tc_timeout, &zero, sizeof(int)));
+    if (v) {
+        RQ_CUDA(cudaMemcpyToSymbol(tc::g_tc_timeout, &zero, sizeof(int)));
+        RQ_CUDA(cudaDeviceSynchronize());
+    }
     *out = v;
     return RQ_OK;
 }
@@ -1872,6 +1881,7 @@ int sync_checked(rq_state* s) {
 int tc_set_wait_polls(uint32_t polls) {
     const uint32_t v = polls == RQ_WAIT_LIMIT_DEFAULT ? tc::WAIT_POLLS : polls;
     RQ_CUDA(cudaMemcpyToSymbol(tc::g_tc_wait_polls, &v, sizeof(v)));
+    RQ_CUDA(cudaDeviceSynchronize());   // landed before any later launch, on any stream
     return RQ_OK;
 }
 
