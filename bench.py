@@ -68,7 +68,13 @@ def _args():
     ap.add_argument("--no-sampling", action="store_true", help="skip the <Z_i> + shots leg on the final state")
     ap.add_argument("--no-small", action="store_true", help="skip the 20-qubit f64 circuit leg")
     ap.add_argument("--warm-train", type=int, default=2048, help="training graphs for the warm start")
-    ap.add_argument("--warm-eval", type=int, default=256, help="held-out graphs for the warm start")
+    ap.add_argument("--warm-train-sizes", default="12,14,16,18,20,22,24",
+                    help="graph sizes of the warm start's training graphs")
+    ap.add_argument("--warm-eval", type=int, default=192, help="held-out graphs for the warm start")
+    ap.add_argument("--warm-eval-sizes", default="16,18,20,22,24,26",
+                    help="graph sizes of the held-out graphs (the config's n in {16..26})")
+    ap.add_argument("--warm-extra", action="store_true",
+                    help="also run the 50-step-budget and run_qaoa-convergence-rule arms")
     return ap.parse_args()
 
 
@@ -349,29 +355,39 @@ def vqe_batch_leg(a, ws, rank, with_cpu):
     return res
 
 
-def warmstart_leg(a, ws, rank):
-    """Learned warm start vs linear ramp for QAOA p = 4 (scaled down from 200k training
-    pairs / 4096 held-out graphs to keep the default bench within minutes).
-    Training: a.warm_train random 3-regular graphs, n in {12, ..., 20}, angles from the
-    plain batched optimizer (linear ramp + 100 Adam steps, lr 0.05, exact adjoint
-    gradients); the MLP (325 -> 256 -> 256 -> 8, BF16 tensor cores) learns them.
-    Evaluation on a.warm_eval held-out graphs, n in {16, 18, 20}: the target of each graph
-    is the energy of 200 plain Adam steps from the ramp; each arm then runs until every graph
-    is within 1e-5 relative of its target (at most 200 steps; finished graphs leave the
-    launches): plain = linear ramp + Adam (lr 0.05); warm + Adam = the MLP's angles + Adam
-    (lr 0.005); learned pipeline = the MLP's angles + ascent steps preconditioned by the
-    learned curvature (-H^-1 of the graph size's average Hessian at the training optima,
-    damping 0.8, halved on a fall); ramp + preconditioned steps for comparison; the learned
-    pipeline with a 50-step budget; plain and learned pipelines with run_qaoa's convergence
-    rule as well (|dE| < 1e-6 in a step stops an instance).  solves/s = graphs that reached
-    the target / device time of the arm (plus the MLP inference for the MLP arms).  The
-    headline speedup is the learned pipeline against plain, both without the rule."""
+def warmstart_leg(a, ws, rank, with_cpu=False):
+    """Learned warm start vs linear ramp for QAOA p = 4.  The config asks for 200k training
+    pairs and 4096 held-out graphs with n in {16..26}; that many optimizer runs take tens of
+    GPU-minutes (about 3 ms per Adam step of one 26-node graph), so the default leg keeps the
+    sizes and scales the counts down (--warm-train / --warm-eval set them).
+    Training: a.warm_train random 3-regular graphs with n in --warm-train-sizes, angles from
+    the plain batched optimizer (linear ramp + 100 Adam steps, lr 0.05, exact adjoint
+    gradients); the MLP (325 -> 256 -> 256 -> 8, BF16 tensor cores) learns the per-graph
+    correction to the size trend of the optimal angles.
+    Evaluation on a.warm_eval held-out graphs, n uniform over --warm-eval-sizes: the target of
+    each graph is the energy of 200 plain Adam steps from the ramp; each arm then runs until
+    every graph is within 1e-5 relative of its target (at most 200 steps; finished graphs
+    leave the launches):
+      plain            linear ramp + Adam (lr 0.05)
+      warm + Adam      the MLP's angles + Adam (lr 0.005)
+      learned pipeline the MLP's angles + ascent steps preconditioned by the learned curvature
+                       (-H^-1 of the graph size's average Hessian at the training optima,
+                       damping 0.8, halved on a fall)
+      mean + curvature the size trend alone (no network) + the same preconditioned steps:
+                       what the network itself adds is learned pipeline vs this arm
+      ramp + curvature the linear ramp + the same preconditioned steps
+    (--warm-extra adds the learned pipeline with a 50-step budget and both pipelines with
+    run_qaoa's convergence rule).  solves/s = graphs that reached the target / device time of
+    the arm (plus the MLP inference for the MLP arms).  The headline speedup is the learned
+    pipeline against plain."""
     import numpy as np
 
     from ruqu_b200 import rng, workloads
     from ruqu_b200.batch import QaoaBatch
     from ruqu_b200.warmstart import WarmStart, linear_ramp
     p, lr, lr_warm = 4, 0.05, 0.005
+    train_sizes = tuple(int(x) for x in a.warm_train_sizes.split(","))
+    eval_sizes = tuple(int(x) for x in a.warm_eval_sizes.split(","))
 
     def graphs(count, sizes, seed):
         st = rng.Stream(seed, 2)
@@ -379,9 +395,12 @@ def warmstart_leg(a, ws, rank):
         return [(n, workloads.random_3regular_graph(n, st)) for n in
                 (sizes[sel.randint(len(sizes))] for _ in range(count))]
 
+    def reached(e, target):
+        return e >= target * (1 - 1e-5)
+
     g0, b0 = linear_ramp(p)
     t0 = time.perf_counter()
-    train = graphs(a.warm_train, (12, 14, 16, 18, 20), 21)
+    train = graphs(a.warm_train, train_sizes, 21)
     qb = QaoaBatch(train, p, "f32")
     g, b, _, _ = qb.optimize(np.tile(g0, (len(train), 1)), np.tile(b0, (len(train), 1)), 100, lr)
     gen_ms = qb.last_ms()
@@ -389,68 +408,91 @@ def warmstart_leg(a, ws, rank):
     hist = warm.fit(train, g, b)
     warm.fit_curvature(train, g, b)
     from ruqu_b200.dist import shard
-    held = shard(graphs(a.warm_eval, (16, 18, 20), 22), rank, ws)
+    held = shard(graphs(a.warm_eval, eval_sizes, 22), rank, ws)
     hb = QaoaBatch(held, p, "f32")
     G0, B0 = np.tile(g0, (len(held), 1)), np.tile(b0, (len(held), 1))
-    _, _, target, _ = hb.optimize(G0, B0, 200, lr)
-    _, _, e_ramp, st_ramp = hb.optimize(G0, B0, 200, lr, target=target, rtol=1e-5)
-    ramp_ms = hb.last_ms()
+    opt_g, opt_b, target, _ = hb.optimize(G0, B0, 200, lr)
+    setup_s = time.perf_counter() - t0
+    arms = {}
+
+    def arm(name, ms, e, steps):
+        ok = reached(e, target)
+        arms[name] = {"ms": ms, "reached": float(ok.mean()), "solves_per_s": float(ok.sum()) * ws / (ms / 1e3),
+                      "median_steps": float(np.median(steps)), "max_steps": int(np.max(steps))}
+
+    _, _, e, st = hb.optimize(G0, B0, 200, lr, target=target, rtol=1e-5)
+    arm("plain", hb.last_ms(), e, st)
     warm.predict(held)                       # warm-up (host threads, device buffers)
     t1 = time.perf_counter()
     pg, pb = warm.predict(held)
     infer_ms = (time.perf_counter() - t1) * 1e3
-    _, _, e_warm, st_warm = hb.optimize(pg, pb, 200, lr_warm, target=target, rtol=1e-5)
-    warm_ms = hb.last_ms() + infer_ms
-    ok_ramp = e_ramp >= target * (1 - 1e-5)
-    ok_warm = e_warm >= target * (1 - 1e-5)
-    # the learned pipeline: MLP start + steps preconditioned by the learned curvature
+    _, _, e, st = hb.optimize(pg, pb, 200, lr_warm, target=target, rtol=1e-5)
+    arm("warm_adam", hb.last_ms() + infer_ms, e, st)
     P = warm.preconditioners(held)
-    _, _, e_wp, st_wp = hb.optimize_precond(pg, pb, P, 200, 0.8, target=target, rtol=1e-5)
-    wp_ms = hb.last_ms() + infer_ms
-    ok_wp = e_wp >= target * (1 - 1e-5)
-    _, _, e_rp, st_rp = hb.optimize_precond(G0, B0, P, 200, 0.8, target=target, rtol=1e-5)
-    rp_ms = hb.last_ms()
-    ok_rp = e_rp >= target * (1 - 1e-5)
-    # the learned pipeline with a 50-step budget (the few graphs it has not solved by then stop)
-    _, _, e_w50, _ = hb.optimize_precond(pg, pb, P, 50, 0.8, target=target, rtol=1e-5)
-    w50_ms = hb.last_ms() + infer_ms
-    ok_w50 = e_w50 >= target * (1 - 1e-5)
-    # both pipelines with run_qaoa's convergence rule (an instance stops once a step changes
-    # its energy by less than 1e-6, qaoa.rs:266-269) besides the target
-    hb.set_convergence(1e-6)
-    _, _, e_rc, _ = hb.optimize(G0, B0, 200, lr, target=target, rtol=1e-5)
-    rc_ms = hb.last_ms()
-    _, _, e_wc, st_wc = hb.optimize_precond(pg, pb, P, 200, 0.8, target=target, rtol=1e-5)
-    wc_ms = hb.last_ms() + infer_ms
-    hb.set_convergence(0.0)
-    ok_rc = e_rc >= target * (1 - 1e-5)
-    ok_wc = e_wc >= target * (1 - 1e-5)
-    return {"workload": "QAOA p=4 warm start vs linear ramp: train %d graphs n in {12..20}, evaluate %d held-out "
-                        "graphs n in {16,18,20}; Adam with exact adjoint gradients until within 1e-5 of the "
-                        "200-step plain energy; f32 states" % (a.warm_train, a.warm_eval),
-            "train_data_device_ms": gen_ms, "mlp_val_mse_normalised": min(hist) if hist else None,
-            "setup_s": time.perf_counter() - t0,
-            "ramp_ms": ramp_ms, "warm_ms": warm_ms, "warm_inference_ms": infer_ms,
-            "solves_per_s_ramp": float(ok_ramp.sum()) * ws / (ramp_ms / 1e3),
-            "solves_per_s_warm": float(ok_warm.sum()) * ws / (warm_ms / 1e3),
-            "speedup_warm_adam": (float(ok_warm.sum()) / warm_ms) / max(1e-9, float(ok_ramp.sum()) / ramp_ms),
-            "reached_ramp": float(ok_ramp.mean()), "reached_warm": float(ok_warm.mean()),
-            "median_steps_ramp": float(np.median(st_ramp)), "median_steps_warm": float(np.median(st_warm)),
-            "warm_precond_ms": wp_ms, "solves_per_s_warm_precond": float(ok_wp.sum()) * ws / (wp_ms / 1e3),
-            "reached_warm_precond": float(ok_wp.mean()), "median_steps_warm_precond": float(np.median(st_wp)),
-            "ramp_precond_ms": rp_ms, "solves_per_s_ramp_precond": float(ok_rp.sum()) * ws / (rp_ms / 1e3),
-            "reached_ramp_precond": float(ok_rp.mean()), "median_steps_ramp_precond": float(np.median(st_rp)),
-            "warm_precond_50_ms": w50_ms, "solves_per_s_warm_precond_50": float(ok_w50.sum()) * ws / (w50_ms / 1e3),
-            "reached_warm_precond_50": float(ok_w50.mean()),
-            "speedup_50_step_budget": (float(ok_w50.sum()) / w50_ms) / max(1e-9, float(ok_ramp.sum()) / ramp_ms),
-            "ramp_conv_ms": rc_ms, "solves_per_s_ramp_conv": float(ok_rc.sum()) * ws / (rc_ms / 1e3),
-            "reached_ramp_conv": float(ok_rc.mean()),
-            "warm_precond_conv_ms": wc_ms, "solves_per_s_warm_precond_conv": float(ok_wc.sum()) * ws / (wc_ms / 1e3),
-            "reached_warm_precond_conv": float(ok_wc.mean()), "max_steps_warm_precond_conv": int(np.max(st_wc)),
-            "speedup_with_convergence_rule": (float(ok_wc.sum()) / wc_ms) / max(1e-9, float(ok_rc.sum()) / rc_ms),
-            "speedup": (float(ok_wp.sum()) / wp_ms) / max(1e-9, float(ok_ramp.sum()) / ramp_ms),
-            "speedup_definition": "learned pipeline (MLP start + learned-curvature steps) vs plain (linear ramp + "
-                                  "Adam), solves/s"}
+    _, _, e, st = hb.optimize_precond(pg, pb, P, 200, 0.8, target=target, rtol=1e-5)
+    arm("learned_pipeline", hb.last_ms() + infer_ms, e, st)
+    mg, mb = warm.mean_angles(held)
+    _, _, e, st = hb.optimize_precond(mg, mb, P, 200, 0.8, target=target, rtol=1e-5)
+    arm("mean_curvature", hb.last_ms(), e, st)
+    _, _, e, st = hb.optimize_precond(G0, B0, P, 200, 0.8, target=target, rtol=1e-5)
+    arm("ramp_curvature", hb.last_ms(), e, st)
+    if a.warm_extra:
+        _, _, e, st = hb.optimize_precond(pg, pb, P, 50, 0.8, target=target, rtol=1e-5)
+        arm("learned_pipeline_50_steps", hb.last_ms() + infer_ms, e, st)
+        hb.set_convergence(1e-6)   # run_qaoa's rule (qaoa.rs:266-269): |dE| < 1e-6 stops an instance
+        _, _, e, st = hb.optimize(G0, B0, 200, lr, target=target, rtol=1e-5)
+        arm("plain_convergence_rule", hb.last_ms(), e, st)
+        _, _, e, st = hb.optimize_precond(pg, pb, P, 200, 0.8, target=target, rtol=1e-5)
+        arm("learned_pipeline_convergence_rule", hb.last_ms() + infer_ms, e, st)
+        hb.set_convergence(0.0)
+    # start-point quality: distance of each start from the graph's own optimum (the plain run's)
+    ng = np.array([n for n, _ in held])
+    opt = np.concatenate([opt_g, opt_b], axis=1)
+    dist = {"mlp": np.linalg.norm(np.concatenate([pg, pb], axis=1) - opt, axis=1),
+            "mean": np.linalg.norm(np.concatenate([mg, mb], axis=1) - opt, axis=1)}
+    by_size = {int(n): {"held_out": int((ng == n).sum()),
+                        "median_start_distance_mlp": float(np.median(dist["mlp"][ng == n])),
+                        "median_start_distance_mean": float(np.median(dist["mean"][ng == n]))}
+               for n in sorted(set(ng.tolist()))}
+    res = {"workload": "QAOA p=4 warm start vs linear ramp: train %d graphs n in {%s}, evaluate %d held-out graphs "
+                       "n in {%s}; each arm runs until every graph is within 1e-5 of its 200-step plain Adam energy; "
+                       "f32 states" % (a.warm_train, a.warm_train_sizes, a.warm_eval, a.warm_eval_sizes),
+           "counts_note": "the config's 200k training pairs / 4096 held-out graphs are scaled down to keep the "
+                          "default bench within minutes; sizes are the config's",
+           "train_data_device_ms": gen_ms, "setup_s": setup_s, "warm_inference_ms": infer_ms,
+           "mlp_val_error_vs_trend": min(hist) if hist else None,
+           "mlp_val_error_definition": "held-out mean squared error of the network's correction, as a fraction "
+                                       "of the residual variance around the size trend (below 1: the network "
+                                       "predicts part of the per-graph correction)",
+           "arms": arms, "by_size": by_size,
+           "speedup": arms["learned_pipeline"]["solves_per_s"] / max(1e-9, arms["plain"]["solves_per_s"]),
+           "speedup_network_vs_mean": arms["learned_pipeline"]["solves_per_s"] /
+                                      max(1e-9, arms["mean_curvature"]["solves_per_s"]),
+           "speedup_definition": "learned pipeline (MLP start + learned-curvature steps) vs plain (linear ramp + "
+                                 "Adam), solves/s; speedup_network_vs_mean = learned pipeline vs the size trend "
+                                 "with the same steps"}
+    if with_cpu:
+        # the plain method on the CPU restatement: Adam steps with central-difference gradients
+        # of the oracle's evaluate_qaoa_cost (16 evaluations per step) on one 16-node graph,
+        # 2 steps timed, scaled by the plain GPU arm's median step count
+        import oracle
+        n16 = next(x for x in held if x[0] == min(eval_sizes))
+        edges = [(u, v, 1.0) for u, v in n16[1]]
+        th = np.concatenate([g0, b0])
+        t2 = time.perf_counter()
+        for _ in range(2):
+            for j in range(2 * p):
+                for d in (1e-5, -1e-5):
+                    tt = th.copy()
+                    tt[j] += d
+                    oracle.qaoa_cost(n16[0], edges, tt[:p], tt[p:])
+        step_s = (time.perf_counter() - t2) / 2
+        res["cpu_baseline"] = {"value": 1.0 / (step_s * arms["plain"]["median_steps"]), "unit": "solves/s",
+                               "cores": 1, "kind": "port",
+                               "sample": "2 Adam steps (16 oracle evaluate_qaoa_cost calls each, f64, n=%d) timed, "
+                                         "scaled by the plain GPU arm's median steps (%g)"
+                                         % (n16[0], arms["plain"]["median_steps"])}
+    return res
 
 
 # DRAM bytes (read + write) of one sweep launch measured by ncu on the 26-qubit
@@ -807,7 +849,7 @@ def run_ours(a):
 
     warm = None
     if not a.no_warm:
-        warm = warmstart_leg(a, ws, rank)
+        warm = warmstart_leg(a, ws, rank, with_cpu=(rank == 0 and ws == 1 and not a.no_cpu_baseline))
 
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:

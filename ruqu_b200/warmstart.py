@@ -133,44 +133,70 @@ def features(graphs, copies: int = 1, seed=None) -> np.ndarray:
 class WarmStart:
     """Learned QAOA warm start: an Mlp from padded adjacency features to the 2p angles.
 
-    Targets are normalised per angle (mean / standard deviation of the training set),
-    so an untrained network predicts the mean angles -- optimal QAOA angles of graphs
-    from one family concentrate, and the network learns the per-graph correction.
-    Training rows place each graph's nodes at random rows of the padded matrix
-    (`copies` placements per graph); a held-out slice of the graphs picks the
-    parameters with the lowest validation error; predictions average `tta` random
-    placements."""
+    Optimal QAOA angles of one graph family concentrate around a size-dependent value, so
+    the prediction is trend(n) + sd * MLP(adjacency): trend(n) is the training set's mean
+    angle vector for graphs of n nodes (a straight line in n, fitted to the per-size means,
+    for sizes not seen in training) and the network learns the per-graph correction, in
+    units of the residual spread sd.  An untrained network (or one that never beats zero on
+    the held-out slice) predicts the trend alone -- the "mean predictor", which
+    mean_angles() returns for comparison.  Training rows place each graph's nodes at random
+    rows of the padded matrix (`copies` placements per graph); a held-out slice of the
+    graphs picks the parameters with the lowest validation error; predictions average `tta`
+    random placements."""
 
     def __init__(self, p: int, hidden: int = 256, seed: int = 5):
         self.p = p
         self.net = Mlp(h1=hidden, h2=hidden, n_out=2 * p, seed=seed)
-        self.mu = np.zeros(2 * p)
         self.sd = np.ones(2 * p)
+        self.size_mean = {}                 # n -> mean angle vector of the training graphs of size n
+        self.line = np.zeros((2, 2 * p))    # trend(n) = line[0] + line[1] * n for unseen sizes
         self.precond = {}
+
+    def trend(self, ns) -> np.ndarray:
+        """Mean angle vector for graphs of each size in ns (seen sizes: their training mean;
+        others: the least-squares line through the per-size means)."""
+        return np.stack([self.size_mean[int(n)] if int(n) in self.size_mean else self.line[0] + self.line[1] * n
+                         for n in ns])
+
+    def mean_angles(self, graphs):
+        """The mean predictor: trend(n) for each graph (gammas, betas)."""
+        y = self.trend([n for n, _ in graphs])
+        return y[:, :self.p], y[:, self.p:]
 
     def fit(self, graphs, gammas, betas, copies: int = 4, val_fraction: float = 0.125, chunks: int = 12,
             chunk_steps: int = 500, lr: float = 1e-3, batch: int = 256, seed: int = 3) -> list:
+        """Returns the validation error after each training chunk, as a fraction of the
+        residual variance (below 1: the network predicts part of the per-graph correction)."""
         y = np.concatenate([np.asarray(gammas, dtype=np.float64), np.asarray(betas, dtype=np.float64)], axis=1)
         nval = max(1, int(len(graphs) * val_fraction))
         ntr = len(graphs) - nval
-        self.mu = y[:ntr].mean(axis=0)
-        # angles that hardly vary (a family with few distinct graphs) are not blown up to
-        # unit variance: their spread below 1e-3 rad carries no information for the optimizer
-        self.sd = np.maximum(y[:ntr].std(axis=0), 1e-3)
-        z = (y - self.mu) / self.sd
+        ns = np.array([n for n, _ in graphs])
+        sizes = sorted(set(ns[:ntr].tolist()))
+        self.size_mean = {n: y[:ntr][ns[:ntr] == n].mean(axis=0) for n in sizes}
+        if len(sizes) > 1:
+            A = np.stack([np.ones(len(sizes)), np.array(sizes, dtype=np.float64)], axis=1)
+            self.line = np.linalg.lstsq(A, np.stack([self.size_mean[n] for n in sizes]), rcond=None)[0]
+        else:
+            self.line = np.stack([self.size_mean[sizes[0]], np.zeros(2 * self.p)])
+        r = y - self.trend(ns)
+        # residual spreads below 1e-3 rad carry no information for the optimizer and are not
+        # blown up to unit variance
+        self.sd = np.maximum(r[:ntr].std(axis=0), 1e-3)
+        z = r / self.sd
         x = features(graphs[:ntr], copies, seed=seed)
         t = np.repeat(z[:ntr], copies, axis=0).astype(np.float32)
         xv = features(graphs[ntr:], copies, seed=seed + 1)
         tv = np.repeat(z[ntr:], copies, axis=0).astype(np.float32)
-        best, best_p, hist = float(np.mean(tv.astype(np.float64) ** 2)), None, []
+        var = float(np.mean(tv.astype(np.float64) ** 2))
+        best, best_p, hist = var, None, []
         for c in range(chunks):
             self.net.train(x, t, batch=batch, steps=chunk_steps, lr=lr if c < (2 * chunks) // 3 else lr / 3)
-            vl = float(np.mean((self.net.forward(xv) - tv) ** 2))
+            vl = float(np.mean((self.net.forward(xv) - tv) ** 2)) / max(var, 1e-30)
             hist.append(vl)
             if not np.isfinite(vl):     # diverged: keep the best parameters seen so far
                 break
-            if vl < best:
-                best, best_p = vl, self.net.get_params()
+            if vl * var < best:
+                best, best_p = vl * var, self.net.get_params()
         if best_p is None:     # never better than the mean: predict the mean
             self.net.set_params(np.zeros(self.net.nparam, dtype=np.float32))
         else:
@@ -216,6 +242,6 @@ class WarmStart:
     def predict(self, graphs, tta: int = 8, seed: int = 9):
         x = features(graphs, tta, seed=seed)
         z = self.net.forward(x).reshape(len(graphs), tta, -1).mean(axis=1).astype(np.float64)
-        y = self.mu + self.sd * z
+        y = self.trend([n for n, _ in graphs]) + self.sd * z
         return y[:, :self.p], y[:, self.p:]
 
