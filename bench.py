@@ -68,9 +68,9 @@ def _args():
     ap.add_argument("--no-sampling", action="store_true", help="skip the <Z_i> + shots leg on the final state")
     ap.add_argument("--no-small", action="store_true", help="skip the 20-qubit f64 circuit leg")
     ap.add_argument("--warm-train", type=int, default=2048, help="training graphs for the warm start")
-    ap.add_argument("--warm-train-sizes", default="12,14,16,18,20,22,24",
+    ap.add_argument("--warm-train-sizes", default="12,14,16,18,20,22",
                     help="graph sizes of the warm start's training graphs")
-    ap.add_argument("--warm-eval", type=int, default=192, help="held-out graphs for the warm start")
+    ap.add_argument("--warm-eval", type=int, default=96, help="held-out graphs for the warm start")
     ap.add_argument("--warm-eval-sizes", default="16,18,20,22,24,26",
                     help="graph sizes of the held-out graphs (the config's n in {16..26})")
     ap.add_argument("--warm-extra", action="store_true",

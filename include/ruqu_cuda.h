@@ -274,8 +274,24 @@ RQ_API int rq_plan_get_stats(const rq_plan* p, rq_plan_stats* out);
 RQ_API int rq_plan_destroy(rq_plan* p);
 
 /* ------------------------------------------------------------------------ */
-/* measurement (state.rs:288-352)                                            */
+/* noise channels (noise.rs:151-280)                                         */
+/* One quantum-trajectory step of a single-qubit noise channel given by its Kraus
+ * operators (kraus: nk row-major 2x2 matrices, 8 doubles each as (re, im) pairs, the
+ * sets of depolarizing_kraus / amplitude_damping_kraus / phase_damping_kraus /
+ * thermal_relaxation_kraus, noise.rs:166-280).  The reference builds these sets but no
+ * caller applies them to a state; here, with rho the qubit's reduced density matrix,
+ * operator k is chosen with probability p_k = tr(K_k rho K_k^dagger) / sum_j p_j using
+ * the next uniform of the state's measurement stream (the draw a measurement would
+ * take), and the state becomes K_k |psi> / sqrt(p_k) (its norm kept).  Averaged over
+ * trajectories this is the channel.  *chosen = k, *probability = its p_k (either may be
+ * NULL).  Two device passes: the reduction of <I>, <Z_q>, <X_q>, <Y_q> and the 2x2
+ * update.  RQ_ERR_INVALID_STATE_VECTOR if every p_k is 0. */
+#define RQ_KRAUS_MAX 16u
+RQ_API int rq_state_apply_kraus(rq_state* s, uint32_t q, const double* kraus, uint32_t nk,
+                                int32_t* chosen, double* probability);
+
 /* ------------------------------------------------------------------------ */
+/* measurement (state.rs:288-352)                                            */
 
 RQ_API int rq_state_measure(rq_state* s, uint32_t qubit, rq_measurement* out);
 RQ_API int rq_state_measure_all(rq_state* s, rq_measurement* out /* num_qubits */);

@@ -66,6 +66,7 @@ def _load() -> C.CDLL:
         "orc_apply_noisy": (i32, [vp, P(Gate), u64, P(C.c_double), P(Measurement), u64, P(u64)]),
         "orc_apply_1q_matrix": (i32, [vp, u32, P(dbl)]),
         "orc_apply_2q_matrix": (i32, [vp, u32, u32, P(dbl)]),
+        "orc_apply_kraus": (i32, [vp, u32, P(dbl), u32, P(i32), P(dbl)]),
         "orc_measure": (i32, [vp, u32, P(Measurement)]),
         "orc_reset_qubit": (i32, [vp, u32]),
         "orc_probabilities": (None, [vp, P(dbl)]),
@@ -207,6 +208,14 @@ class OracleState:
     def apply_1q_matrix(self, q, m8):
         m = np.ascontiguousarray(m8, dtype=np.float64)
         _check(lib().orc_apply_1q_matrix(self._h, q, _dp(m)))
+
+    def apply_kraus(self, q, ops):
+        """One trajectory step of a single-qubit channel (ops: k x 2 x 2 complex); (k, p)."""
+        k = np.ascontiguousarray(np.asarray(ops, dtype=np.complex128).reshape(-1, 2, 2)).view(np.float64)
+        k = np.ascontiguousarray(k.reshape(-1))
+        chosen, prob = C.c_int32(), C.c_double()
+        _check(lib().orc_apply_kraus(self._h, q, _dp(k), len(k) // 8, C.byref(chosen), C.byref(prob)))
+        return chosen.value, prob.value
 
     def apply_2q_matrix(self, q1, q2, m32):
         m = np.ascontiguousarray(m32, dtype=np.float64)

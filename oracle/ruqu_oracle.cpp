@@ -579,6 +579,60 @@ int orc_apply_1q_matrix(void* h, uint32_t q, const double* m8) {
     return RQ_OK;
 }
 
+// One quantum-trajectory step of a single-qubit channel (Kraus operators K_k, row-major 2x2,
+// (re, im) pairs).  The reference constructs these sets (noise.rs:166-280) but never applies
+// them to a state; this is the standard unravelling the library implements: with
+// rho_ij = sum over the pairs differing in bit q of a_i conj(a_j), p_k = tr(K_k rho K_k^+),
+// k drawn with the state's next uniform against the normalised cumulative p, and the state
+// replaced by K_k psi / sqrt(p_k / sum p).
+int orc_apply_kraus(void* h, uint32_t q, const double* kraus, uint32_t nk, int32_t* chosen, double* probability) {
+    StateBase* s = (StateBase*)h;
+    if (q >= s->nq) return RQ_ERR_INVALID_QUBIT_INDEX;
+    if (nk == 0) return RQ_ERR_INVALID_ARGUMENT;
+    double r00 = 0, r11 = 0, r01r = 0, r01i = 0;
+    auto sums = [&](auto* st) {
+        const size_t bit = (size_t)1 << q, n = st->a.size();
+        for (size_t i = 0; i < n; ++i) {
+            if (i & bit) continue;
+            const double a0r = st->a[i].re, a0i = st->a[i].im, a1r = st->a[i | bit].re, a1i = st->a[i | bit].im;
+            r00 += a0r * a0r + a0i * a0i;
+            r11 += a1r * a1r + a1i * a1i;
+            r01r += a0r * a1r + a0i * a1i;   // a0 conj(a1)
+            r01i += a0i * a1r - a0r * a1i;
+        }
+    };
+    if (auto d = as<double>(s)) sums(d); else sums(as<float>(s));
+    std::vector<double> pk(nk);
+    double total = 0;
+    for (uint32_t k = 0; k < nk; ++k) {
+        const double* K = kraus + 8 * (size_t)k;
+        double acc = 0;
+        for (int i = 0; i < 2; ++i) {
+            const double ar = K[4 * i], ai = K[4 * i + 1], br = K[4 * i + 2], bi = K[4 * i + 3];
+            const double cr = ar * r01r - ai * r01i, ci = ar * r01i + ai * r01r;
+            acc += (ar * ar + ai * ai) * r00 + (br * br + bi * bi) * r11 + 2.0 * (cr * br + ci * bi);
+        }
+        pk[k] = acc > 0 ? acc : 0;
+        total += pk[k];
+    }
+    if (!(total > 0)) return RQ_ERR_INVALID_STATE_VECTOR;
+    const double u = s->next_uniform();
+    uint32_t pick = nk - 1;
+    double cum = 0;
+    for (uint32_t k = 0; k < nk; ++k) {
+        cum += pk[k] / total;
+        if (u < cum && pk[k] > 0) { pick = k; break; }
+    }
+    while (pk[pick] == 0 && pick > 0) --pick;
+    const double f = 1.0 / std::sqrt(pk[pick] / total);
+    double m8[8];
+    for (int j = 0; j < 8; ++j) m8[j] = kraus[8 * (size_t)pick + j] * f;
+    orc_apply_1q_matrix(h, q, m8);
+    if (chosen) *chosen = (int32_t)pick;
+    if (probability) *probability = pk[pick] / total;
+    return RQ_OK;
+}
+
 int orc_apply_2q_matrix(void* h, uint32_t q1, uint32_t q2, const double* m32) {
     StateBase* s = (StateBase*)h;
     if (q1 >= s->nq || q2 >= s->nq) return RQ_ERR_INVALID_QUBIT_INDEX;

@@ -76,6 +76,7 @@ SIGNATURES = {
     "rq_state_apply_1q_matrix": (C.c_int, [_vp, _u32, _P(_dbl)]),
     "rq_state_apply_2q_matrix": (C.c_int, [_vp, _u32, _u32, _P(_dbl)]),
     "rq_state_measure": (C.c_int, [_vp, _u32, _P(RqMeasurement)]),
+    "rq_state_apply_kraus": (C.c_int, [_vp, _u32, _P(_dbl), _u32, _P(_i32), _P(_dbl)]),
     "rq_state_measure_all": (C.c_int, [_vp, _P(RqMeasurement)]),
     "rq_state_reset_qubit": (C.c_int, [_vp, _u32]),
     "rq_state_sample": (C.c_int, [_vp, _P(_u32), _u32, _u64, _u64, _P(_u64)]),

@@ -368,6 +368,59 @@ int rq_plan_create(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t 
     return rq::plan_build(s, gates, n, use_sweep ? RQ_EXEC_SWEEP : RQ_EXEC_PER_GATE, out, passes, 2, m);
 }
 
+int rq_state_apply_kraus(rq_state* s, uint32_t q, const double* kraus, uint32_t nk, int32_t* chosen,
+                         double* probability) {
+    if (!s || (!kraus && nk)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (nk == 0 || nk > RQ_KRAUS_MAX)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "a channel has 1.." + std::to_string(RQ_KRAUS_MAX) + " Kraus operators");
+    if (q >= s->nq)
+        return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "invalid qubit index " + std::to_string(q) + " for " +
+                                                        std::to_string(s->nq) + "-qubit system");
+    RQ_TRY(set_device(s));
+    // the qubit's reduced density matrix rho_ij = sum a_i conj(a_j) over the pairs of amplitudes
+    // that differ in bit q, from <I>, <Z_q>, <X_q>, <Y_q> (FP64 reductions on the device)
+    const uint64_t b = 1ull << q;
+    const rq::PauliMask t[4] = {{0, 0, 0}, {0, b, 0}, {b, 0, 0}, {b, b, 1}};
+    double ev[4];
+    RQ_TRY(rq::pauli_expect(s, t, 4, ev));
+    const double r00 = 0.5 * (ev[0] + ev[1]), r11 = 0.5 * (ev[0] - ev[1]);
+    const double r01r = 0.5 * ev[2], r01i = -0.5 * ev[3];   // rho_10 = conj(rho_01)
+    // p_k = tr(K_k rho K_k^dagger)
+    std::vector<double> pk(nk);
+    double total = 0.0;
+    for (uint32_t k = 0; k < nk; ++k) {
+        const double* K = kraus + 8 * (size_t)k;   // row-major 2x2, (re, im) pairs
+        double acc = 0.0;
+        for (int i = 0; i < 2; ++i) {
+            const double ar = K[4 * i], ai = K[4 * i + 1], br = K[4 * i + 2], bi = K[4 * i + 3];
+            // (K rho K^dagger)_ii = |a|^2 r00 + |b|^2 r11 + 2 Re(a rho01 conj(b))
+            const double cr = ar * r01r - ai * r01i, ci = ar * r01i + ai * r01r;   // a rho01
+            acc += (ar * ar + ai * ai) * r00 + (br * br + bi * bi) * r11 + 2.0 * (cr * br + ci * bi);
+        }
+        pk[k] = acc > 0.0 ? acc : 0.0;
+        total += pk[k];
+    }
+    if (!(total > 0.0)) return rq::fail(RQ_ERR_INVALID_STATE_VECTOR, "the channel annihilates the state");
+    const double u = rqd::uniform(s->seed, 0, s->draws++);
+    uint32_t pick = nk - 1;
+    double cum = 0.0;
+    for (uint32_t k = 0; k < nk; ++k) {
+        cum += pk[k] / total;
+        if (u < cum && pk[k] > 0.0) {
+            pick = k;
+            break;
+        }
+    }
+    while (pk[pick] == 0.0 && pick > 0) --pick;
+    const double f = 1.0 / std::sqrt(pk[pick] / total);   // the state keeps its norm
+    double m8[8];
+    for (int j = 0; j < 8; ++j) m8[j] = kraus[8 * (size_t)pick + j] * f;
+    RQ_TRY(rq::gate1q(s, q, m8));
+    if (chosen) *chosen = (int32_t)pick;
+    if (probability) *probability = pk[pick] / total;
+    return RQ_OK;
+}
+
 int rq_plan_update(rq_state* s, rq_plan* p, const rq_gate* gates, uint64_t n) {
     if (!s || !p || (!gates && n)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
     if (!rq::plan_fits(p, s))

@@ -207,6 +207,16 @@ class QuantumState:
         m = np.ascontiguousarray(np.asarray(matrix, dtype=np.complex128).reshape(4, 4)).view(np.float64)
         check(lib.rq_state_apply_2q_matrix(self._h, int(q1), int(q2), _dp(m)))
 
+    def apply_kraus(self, qubit: int, ops) -> tuple[int, float]:
+        """One quantum-trajectory step of the single-qubit channel with Kraus operators
+        ``ops`` (k x 2 x 2 complex, e.g. from ``ruqu_b200.noise``): operator k is picked
+        with probability tr(K_k rho K_k^dagger) by the next draw of this state's stream
+        and applied renormalised.  Returns (k, its probability)."""
+        k = np.ascontiguousarray(np.asarray(ops, dtype=np.complex128).reshape(-1, 2, 2)).view(np.float64)
+        chosen, prob = C.c_int32(), C.c_double()
+        check(lib.rq_state_apply_kraus(self._h, int(qubit), _dp(k), k.size // 8, C.byref(chosen), C.byref(prob)))
+        return chosen.value, prob.value
+
     # ---- measurement (state.rs:288-352) ----
     def measure(self, qubit: int) -> MeasurementOutcome:
         m = RqMeasurement()
