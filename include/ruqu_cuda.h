@@ -120,7 +120,9 @@ typedef enum rq_exec_mode {
                                   FP16 MMA passes (hi*hi + hi*lo + lo*hi of
                                   per-tile-scaled amplitudes and 2^14-scaled
                                   unitaries, FP32 accumulation): FP32-level
-                                  accuracy at twice the TF32 tensor rate        */
+                                  accuracy at twice the TF32 tensor rate; a list
+                                  with a non-unitary UNITARY1Q matrix runs as
+                                  RQ_EXEC_SWEEP_TC                               */
 } rq_exec_mode;
 
 typedef struct rq_state rq_state;   /* opaque: device-resident amplitudes */
@@ -304,6 +306,21 @@ RQ_API int rq_state_reset_qubit(rq_state* s, uint32_t qubit);
  * was measured as 1.  The state is not modified. */
 RQ_API int rq_state_sample(rq_state* s, const uint32_t* qubits, uint32_t nqubits,
                     uint64_t base_seed, uint64_t shots, uint64_t* out_bits);
+
+/* The prefix tree rq_state_sample walks, kept with the state for lookups: the qubits
+ * ordered as `qubits` lists them (first appearance; the qubits not listed after them),
+ * level L (0 <= L <= num_qubits) holds 2^L FP64 sums of |a_i|^2, entry j over the
+ * amplitudes whose first L ordered qubits take the bits of j (bit k of j = qubit k of
+ * that order); level 0 is the squared norm, level num_qubits the |a_i|^2 themselves.
+ * A snapshot of the amplitudes at build time (level num_qubits reads them live): build
+ * again after the state changes.  rq_state_sample replaces it with its own tree.
+ * A rank of a state split over several GPUs samples or measures through these sums: its
+ * share of every conditional probability of the shot walk (simulator.rs:107-147) is one
+ * lookup, and the ranks add their shares (ruqu_b200/distributed.py). */
+RQ_API int rq_state_tree_build(rq_state* s, const uint32_t* qubits, uint32_t nqubits);
+/* out[i] = entry index[i] of level `level` (host arrays; index[i] < 2^level). */
+RQ_API int rq_state_tree_lookup(rq_state* s, uint32_t level, const uint64_t* index, uint64_t count,
+                                double* out);
 
 /* ------------------------------------------------------------------------ */
 /* reductions (state.rs:123-137, 362-435)                                    */

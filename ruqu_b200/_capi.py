@@ -80,6 +80,8 @@ SIGNATURES = {
     "rq_state_measure_all": (C.c_int, [_vp, _P(RqMeasurement)]),
     "rq_state_reset_qubit": (C.c_int, [_vp, _u32]),
     "rq_state_sample": (C.c_int, [_vp, _P(_u32), _u32, _u64, _u64, _P(_u64)]),
+    "rq_state_tree_build": (C.c_int, [_vp, _P(_u32), _u32]),
+    "rq_state_tree_lookup": (C.c_int, [_vp, _u32, _P(_u64), _u64, _P(_dbl)]),
     "rq_state_probabilities": (C.c_int, [_vp, _P(_dbl)]),
     "rq_state_probability_of_qubit": (C.c_int, [_vp, _u32, _P(_dbl)]),
     "rq_state_expectation_value": (C.c_int, [_vp, _P(RqPauliOp), _u32, _P(_dbl)]),

@@ -677,6 +677,23 @@ int rq_state_sample(rq_state* s, const uint32_t* qubits, uint32_t nqubits, uint6
     return rq::sample(s, qubits, nqubits, base_seed, shots, out_bits);
 }
 
+int rq_state_tree_build(rq_state* s, const uint32_t* qubits, uint32_t nqubits) {
+    if (!s || (!qubits && nqubits)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    if (nqubits > 64) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "a prefix tree orders at most 64 qubits");
+    for (uint32_t k = 0; k < nqubits; ++k)
+        if (qubits[k] >= s->nq)
+            return rq::fail(RQ_ERR_INVALID_QUBIT_INDEX, "invalid qubit index " + std::to_string(qubits[k]) + " for " +
+                                                            std::to_string(s->nq) + "-qubit system");
+    RQ_TRY(set_device(s));
+    return rq::tree_build(s, qubits, nqubits);
+}
+
+int rq_state_tree_lookup(rq_state* s, uint32_t level, const uint64_t* index, uint64_t count, double* out) {
+    if (!s || ((!index || !out) && count)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    RQ_TRY(set_device(s));
+    return rq::tree_lookup(s, level, index, count, out);
+}
+
 int rq_state_probabilities(rq_state* s, double* out) {
     if (!s || !out) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
     RQ_TRY(set_device(s));

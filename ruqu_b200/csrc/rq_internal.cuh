@@ -25,6 +25,8 @@ struct rq_state {
     size_t partials_cap = 0;      // in doubles
     double* tree = nullptr;       // sampling prefix tree (levels 0..n-1)
     size_t tree_cap = 0;          // in doubles
+    uint8_t tree_order[64] = {};  // the tree's bit k -> qubit (measured qubits first)
+    bool tree_ready = false;      // tree holds the levels of tree_order (rq_state_tree_build / sample)
     double* hbuf = nullptr;       // pinned host staging for small results
     size_t hbuf_cap = 0;          // in doubles
     int32_t exec_mode = RQ_EXEC_AUTO;
@@ -101,6 +103,8 @@ int probabilities_dev(rq_state* s, double* dev_out);
 // ---- sampling (rq_sample.cu) -------------------------------------------------
 int sample(rq_state* s, const uint32_t* qubits, uint32_t nq, uint64_t base_seed,
            uint64_t shots, uint64_t* host_out);
+int tree_build(rq_state* s, const uint32_t* qubits, uint32_t nq);
+int tree_lookup(rq_state* s, uint32_t level, const uint64_t* index, uint64_t count, double* host_out);
 
 // ---- fused sweeps and prepared plans (rq_sweep.cu) ---------------------------
 // tc_passes > 0: fuse each phase's slot-local gate runs into dense 32x32 unitaries

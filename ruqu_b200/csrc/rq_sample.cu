@@ -112,15 +112,26 @@ __global__ void k_sample(const typename C2<T>::t* __restrict__ a, const double* 
     }
 }
 
+// out[i] = entry index[i] of tree level `level` (level n: |a|^2 at that permuted index)
+template <typename T>
+__global__ void k_tree_lookup(const typename C2<T>::t* __restrict__ a, const double* __restrict__ tree, Perm P,
+                              uint32_t level, const uint64_t* __restrict__ index, uint64_t count,
+                              double* __restrict__ out) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t j = index[i];
+        out[i] = level == P.n ? prob_at<T>(a, unpermute(j, P)) : tree[((1ull << level) - 1) + j];
+    }
+}
+
 }  // namespace
 
 namespace rq {
 
-int sample(rq_state* s, const uint32_t* qubits, uint32_t nqm, uint64_t base_seed, uint64_t shots,
-           uint64_t* host_out) {
-    if (shots == 0) return RQ_OK;
-    const uint32_t n = s->nq;
-    if (n > 63 || nqm > MAXQ) return fail(RQ_ERR_INVALID_ARGUMENT, "sampling supports at most 63 qubits and 64 measurements");
+namespace {
+
+// The permutation of a tree over `qubits` (first appearance order; the other qubits after them).
+Perm make_perm(uint32_t n, const uint32_t* qubits, uint32_t nqm) {
     Perm P{};
     P.n = n;
     std::vector<int> pos(n, -1);
@@ -134,11 +145,25 @@ int sample(rq_state* s, const uint32_t* qubits, uint32_t nqm, uint64_t base_seed
         P.pos[q] = (uint8_t)pos[q];
         if (pos[q] != (int)q) P.identity = 0;
     }
-    Plan plan{};
-    plan.m = nqm;
-    for (uint32_t k = 0; k < nqm; ++k) plan.qubits[k] = (uint8_t)qubits[k];
+    return P;
+}
 
-    // tree levels 0..n-1 at offsets 2^k - 1 (level n is the probability vector itself)
+Perm stored_perm(const rq_state* s) {
+    Perm P{};
+    P.n = s->nq;
+    P.identity = 1;
+    for (uint32_t b = 0; b < s->nq; ++b) {
+        P.order[b] = s->tree_order[b];
+        P.pos[s->tree_order[b]] = (uint8_t)b;
+        if (s->tree_order[b] != b) P.identity = 0;
+    }
+    return P;
+}
+
+// tree levels 0..n-1 at offsets 2^k - 1 (level n is the probability vector itself)
+int build_tree(rq_state* s, const Perm& P) {
+    const uint32_t n = s->nq;
+    s->tree_ready = false;
     RQ_TRY(ensure_tree(s, (size_t)1 << n));
     int sms = num_sms(s->device);
     double* top = s->tree + ((1ull << (n - 1)) - 1);
@@ -159,6 +184,24 @@ int sample(rq_state* s, const uint32_t* qubits, uint32_t nqm, uint64_t base_seed
         k_fold_tail<<<1, 1024, 0, s->stream>>>(s->tree, k + 1);
         RQ_CUDA(cudaGetLastError());
     }
+    for (uint32_t b = 0; b < n; ++b) s->tree_order[b] = P.order[b];
+    s->tree_ready = true;
+    return RQ_OK;
+}
+
+}  // namespace
+
+int sample(rq_state* s, const uint32_t* qubits, uint32_t nqm, uint64_t base_seed, uint64_t shots,
+           uint64_t* host_out) {
+    if (shots == 0) return RQ_OK;
+    const uint32_t n = s->nq;
+    if (n > 63 || nqm > MAXQ) return fail(RQ_ERR_INVALID_ARGUMENT, "sampling supports at most 63 qubits and 64 measurements");
+    const Perm P = make_perm(n, qubits, nqm);
+    Plan plan{};
+    plan.m = nqm;
+    for (uint32_t k = 0; k < nqm; ++k) plan.qubits[k] = (uint8_t)qubits[k];
+    RQ_TRY(build_tree(s, P));
+    const int sms = num_sms(s->device);
     uint64_t* dout = nullptr;
     RQ_CUDA(cudaMallocAsync((void**)&dout, shots * sizeof(uint64_t), s->stream));
     unsigned gs = grid_for(shots, 128, sms);
@@ -171,6 +214,44 @@ int sample(rq_state* s, const uint32_t* qubits, uint32_t nqm, uint64_t base_seed
     cudaFreeAsync(dout, s->stream);
     RQ_CUDA(le);
     RQ_CUDA(ce);
+    return rq::sync_checked(s);
+}
+
+int tree_build(rq_state* s, const uint32_t* qubits, uint32_t nqm) {
+    if (s->nq > 63) return fail(RQ_ERR_INVALID_ARGUMENT, "prefix trees support at most 63 qubits");
+    RQ_TRY(build_tree(s, make_perm(s->nq, qubits, nqm)));
+    return rq::sync_checked(s);
+}
+
+int tree_lookup(rq_state* s, uint32_t level, const uint64_t* index, uint64_t count, double* host_out) {
+    if (!s->tree_ready) return fail(RQ_ERR_INVALID_ARGUMENT, "no prefix tree: build one first");
+    if (level > s->nq) return fail(RQ_ERR_INVALID_ARGUMENT, "tree level above the qubit count");
+    const uint64_t lim = 1ull << level;
+    for (uint64_t i = 0; i < count; ++i)
+        if (index[i] >= lim) return fail(RQ_ERR_INVALID_ARGUMENT, "tree index out of range for its level");
+    if (count == 0) return RQ_OK;
+    const Perm P = stored_perm(s);
+    uint64_t* didx = nullptr;
+    double* dout = nullptr;
+    RQ_CUDA(cudaMallocAsync((void**)&didx, count * sizeof(uint64_t), s->stream));
+    cudaError_t e = cudaMallocAsync((void**)&dout, count * sizeof(double), s->stream);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(didx, s->stream);
+        return cuda_fail(e, "tree lookup buffers");
+    }
+    e = cudaMemcpyAsync(didx, index, count * sizeof(uint64_t), cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) {
+        const unsigned g = grid_for(count, TPB, num_sms(s->device));
+        if (s->prec == RQ_F32)
+            k_tree_lookup<float><<<g, TPB, 0, s->stream>>>((const float2*)s->amps, s->tree, P, level, didx, count, dout);
+        else
+            k_tree_lookup<double><<<g, TPB, 0, s->stream>>>((const double2*)s->amps, s->tree, P, level, didx, count, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(host_out, dout, count * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    cudaFreeAsync(didx, s->stream);
+    cudaFreeAsync(dout, s->stream);
+    RQ_CUDA(e);
     return rq::sync_checked(s);
 }
 

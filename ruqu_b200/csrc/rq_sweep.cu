@@ -1411,6 +1411,25 @@ int build_images(const rq_plan* P, cudaStream_t st) {
     return RQ_OK;
 }
 
+// Every Unitary1Q matrix of the list unitary to 1e-6 (|U^dagger U - I| entrywise; NaN fails).
+// The FP16-split tensor-core sweep bounds a tile's components by its norm when it picks the
+// tile's scale and restores that norm at the store, which holds for unitary phases only;
+// other lists take the 3xTF32 sweep, whose FP32-range operands need no such bound.
+bool all_unitary(const rq_gate* gates, uint64_t n) {
+    for (uint64_t k = 0; k < n; ++k) {
+        if (gates[k].kind != RQ_GATE_UNITARY1Q) continue;
+        const double* m = gates[k].m;   // m00 m01 m10 m11 as (re, im)
+        const double c00 = m[0] * m[0] + m[1] * m[1] + m[4] * m[4] + m[5] * m[5];
+        const double c11 = m[2] * m[2] + m[3] * m[3] + m[6] * m[6] + m[7] * m[7];
+        const double c01r = m[0] * m[2] + m[1] * m[3] + m[4] * m[6] + m[5] * m[7];   // conj(m00) m01 + conj(m10) m11
+        const double c01i = m[0] * m[3] - m[1] * m[2] + m[4] * m[7] - m[5] * m[6];
+        if (!(std::fabs(c00 - 1.0) <= 1e-6 && std::fabs(c11 - 1.0) <= 1e-6 && std::fabs(c01r) <= 1e-6 &&
+              std::fabs(c01i) <= 1e-6))
+            return false;
+    }
+    return true;
+}
+
 }  // namespace
 
 int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, rq_plan** out, int tc_passes,
@@ -1446,6 +1465,7 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
     P->mode = RQ_EXEC_SWEEP;
     const uint32_t m = m_override ? std::min(nq, m_override) : sweep_local_qubits(nq, s->prec);
     if (s->prec != RQ_F32 || (m != 12 && m != 13)) tc_passes = 0;   // the tensor-core sweep's tile shapes
+    if (tc_passes == TC_F16 && !all_unitary(gates, n)) tc_passes = 3;
     const uint32_t c = std::min<uint32_t>(m, 5);
     std::vector<PGate> pg;
     std::vector<rq_gate> filtered;
@@ -1571,6 +1591,8 @@ bool plan_same_shape(const rq_plan* P, const rq_gate* gates, uint64_t n) {
 int plan_rebind(rq_state* s, rq_plan* P, const rq_gate* gates, uint64_t n) {
     if (!P->rebindable || !plan_same_shape(P, gates, n))
         return fail(RQ_ERR_CIRCUIT, "circuit error: the gate list's kinds and qubits differ from the plan's");
+    if (P->tc_passes == TC_F16 && !all_unitary(gates, n))
+        return fail(RQ_ERR_CIRCUIT, "circuit error: an FP16-split tensor-core plan holds unitary matrices only");
     if (P->mode == RQ_EXEC_PER_GATE) {
         uint64_t k = 0;
         for (uint64_t j = 0; j < n; ++j)

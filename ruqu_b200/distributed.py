@@ -14,6 +14,13 @@ the partner's half in its place (`rq_state_half_copy` packs and unpacks on the
 device).  The local qubit given up is the one whose next use lies furthest ahead.
 A SWAP gate only relabels the layout.
 
+Measurement, reset and shots follow state.rs:288-352 and simulator.rs:107-147 on the
+whole state: each rank reduces its own amplitudes, the ranks add their shares, and every
+rank takes the same draw of one measurement stream (Philox key = the state's seed), so
+all ranks reach the same outcome and collapse their own amplitudes.  Shots walk the
+sampler's prefix tree: each rank keeps the tree of its local qubits, and every step of
+the walk adds the ranks' shares of the conditional probabilities of all shots at once.
+
 The schedule (local runs and swaps) depends on the gate list and the layout alone,
 so every rank computes the same one; the per-rank translation of a local run depends
 on the rank's bits.  Executors: `DistributedState` runs one rank per process (SPMD,
@@ -30,7 +37,10 @@ import math
 
 import numpy as np
 
+from .error import InvalidQubitIndex
 from .gate import Gate
+from .rng import uniforms, uniforms_keys
+from .types import MeasurementOutcome
 
 H, X, Y, Z, S, SDG, T, TDG, RX, RY, RZ, PHASE, CNOT, CZ, SWAP, RZZ, MEASURE, RESET, BARRIER, U1 = range(20)
 _DIAG_1Q = (Z, S, SDG, T, TDG, RZ, PHASE)
@@ -107,7 +117,7 @@ def schedule(gates, layout: Layout):
     gl = [_as_tuple(g) for g in gates]
     for g in gl:
         if g[0] in (MEASURE, RESET):
-            raise ValueError("measurement and reset are not supported on a distributed state")
+            raise ValueError("a schedule holds unitary gates only (apply_gates runs Measure / Reset)")
         if g[0] > U1:
             raise ValueError(f"unsupported gate kind {g[0]}")
     steps = []
@@ -243,6 +253,12 @@ class DeviceRank:
     def expectation(self, strings) -> np.ndarray:
         return self.state.expectation_values(strings)
 
+    def tree_build(self, bits) -> None:
+        self.state.tree_build(bits)
+
+    def tree_lookup(self, level: int, index) -> np.ndarray:
+        return self.state.tree_lookup(level, index)
+
     def amplitudes(self) -> np.ndarray:
         return self.state.state_vector()
 
@@ -250,9 +266,12 @@ class DeviceRank:
 class _Distributed:
     """Layout bookkeeping and gate / expectation logic shared by the executors."""
 
-    def _init_layout(self, num_qubits: int, global_qubits: int):
+    def _init_layout(self, num_qubits: int, global_qubits: int, seed: int = 0):
         self.layout = Layout(num_qubits, global_qubits)
         self.n, self.nl = self.layout.n, self.layout.nl
+        self.seed = int(seed) & (2**64 - 1)   # the measurement stream (stream 0 of this key)
+        self.draws = 0
+        self.measurement_record = []
 
     def _localize(self, qubits) -> None:
         """Make the given logical qubits local (swapping out local qubits not among them)."""
@@ -265,7 +284,28 @@ class _Distributed:
             self._swap(victim, j)
             self.layout.exchange(victim, self.layout.phys[q])
 
-    def apply_gates(self, gates) -> None:
+    def apply_gates(self, gates) -> list:
+        """The gates in order (QuantumState::apply_gate, state.rs:158-204): unitary runs
+        through the schedule, Measure / Reset through measure / reset_qubit; returns the
+        measurement outcomes."""
+        outcomes, run = [], []
+        for g in gates:
+            t = _as_tuple(g)
+            if t[0] in (MEASURE, RESET):
+                self._apply_unitary(run)
+                run = []
+                if t[0] == MEASURE:
+                    outcomes.append(self.measure(t[1]))
+                else:
+                    self.reset_qubit(t[1])
+            else:
+                run.append(g)
+        self._apply_unitary(run)
+        return outcomes
+
+    def _apply_unitary(self, gates) -> None:
+        if not gates:
+            return
         for step in schedule(gates, self.layout):
             if step[0] == "swap":
                 self._swap(step[1], step[2])
@@ -315,6 +355,123 @@ class _Distributed:
             self._localize(sorted(flips))
             yield idx, [strings[k] for k in idx]
 
+    # ---- measurement (state.rs:288-352) and shots (simulator.rs:107-147) ----
+    def _check_qubit(self, q: int) -> int:
+        q = int(q)
+        if not 0 <= q < self.n:
+            raise InvalidQubitIndex(f"invalid qubit index {q} for {self.n}-qubit system")
+        return q
+
+    def measure(self, qubit: int) -> MeasurementOutcome:
+        """QuantumState::measure (state.rs:288-326) on the whole distributed state:
+        p0 = sum over every rank of |a|^2 with the qubit 0 (FP64), the next draw u of
+        the measurement stream, outcome = u >= p0, probability = 1 - p0 or p0, and
+        the collapse scaled by 1/sqrt(probability) (0 for a zero probability).  A local
+        qubit is one reduction per rank and a projector on it; a global qubit is each
+        rank's norm, and the ranks on the other side of the outcome are zeroed."""
+        q = self._check_qubit(qubit)
+        p = self.layout.phys[q]
+        if p < self.nl:
+            def part(r, eng):
+                i, z = eng.expectation([[], [(p, 3)]])
+                return np.array([0.5 * (float(i) + float(z))])
+        else:
+            j = p - self.nl
+
+            def part(r, eng):
+                return np.array([0.0 if (r >> j) & 1 else float(eng.expectation([[]])[0])])
+        p0 = float(self._rank_sum(part)[0])
+        u = float(uniforms(self.seed, 0, self.draws, 1)[0])
+        self.draws += 1
+        result = u >= p0
+        prob = 1.0 - p0 if result else p0
+        f = 1.0 / math.sqrt(prob) if prob > 0.0 else 0.0
+        for r, eng in self._local_ranks():
+            if p < self.nl:
+                m = [0.0, 0.0, 0.0, 0.0, 0.0, 0.0, f, 0.0] if result else [f, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0]
+                eng.apply([(U1, p, 0, 0.0, m)])
+            elif ((r >> j) & 1) == int(result):
+                eng.apply([_phase_gate(complex(f))])
+            else:
+                eng.zero()
+        out = MeasurementOutcome(q, bool(result), prob)
+        self.measurement_record.append(out)
+        return out
+
+    def measure_all(self) -> list:
+        """Qubit 0 first (state.rs:329-335)."""
+        return [self.measure(q) for q in range(self.n)]
+
+    def reset_qubit(self, qubit: int) -> None:
+        """Measure, then X if the outcome was 1 (state.rs:340-350)."""
+        if self.measure(qubit).result:
+            self.apply_gates([(X, int(qubit), 0, 0.0)])
+
+    def sample(self, shots: int, base_seed: int = 42, qubits=None) -> np.ndarray:
+        """Shot bitstrings without collapse, as QuantumState.sample / rq_state_sample: shot s
+        measures ``qubits`` in order with draws 0, 1, ... of key base_seed + s, outcome 1
+        iff u >= P(qubit = 0 | earlier outcomes) (simulator.rs:107-147, state.rs:288-304).
+        Each rank builds the prefix tree of its local qubits in measurement order; at step
+        k every rank looks up its share of P(prefix, 0) and P(prefix, 1) for every shot (a
+        global qubit: its rank bit splits the ranks' shares; ranks whose bits contradict a
+        shot's global outcomes add nothing) and the shares are summed over ranks (one
+        all-reduce of 2 x shots doubles per measured qubit).  Every rank walks the same
+        shots to the same bitstrings.  Sums over ranks round differently from one tree over
+        the whole state, so a shot can differ from the one-GPU sampler only where its draw
+        falls within rounding of its conditional probability."""
+        qs = list(range(self.n)) if qubits is None else [self._check_qubit(q) for q in qubits]
+        if len(qs) > 64:
+            raise ValueError("at most 64 measurements per shot")
+        shots = int(shots)
+        out = np.zeros(shots, dtype=np.uint64)
+        if shots == 0 or not qs:
+            return out
+        pos = {}
+        for q in qs:
+            p = self.layout.phys[q]
+            if p < self.nl and p not in pos:
+                pos[p] = len(pos)
+        order = sorted(pos, key=pos.get)
+        for _, eng in self._local_ranks():
+            eng.tree_build(order)
+        keys = np.uint64(int(base_seed) & (2**64 - 1)) + np.arange(shots, dtype=np.uint64)
+        prefix = np.zeros(shots, dtype=np.uint64)
+        ok = {r: np.ones(shots, dtype=bool) for r, _ in self._local_ranks()}
+        zeros = np.zeros(shots)
+        lvl = 0
+        val = {}
+        for k, q in enumerate(qs):
+            if q not in val:
+                p = self.layout.phys[q]
+                if p < self.nl:
+                    b = np.uint64(1) << np.uint64(pos[p])
+
+                    def part(r, eng):
+                        v0 = eng.tree_lookup(lvl + 1, prefix)
+                        v1 = eng.tree_lookup(lvl + 1, prefix | b)
+                        return np.concatenate([np.where(ok[r], v0, 0.0), np.where(ok[r], v1, 0.0)])
+                else:
+                    j = p - self.nl
+
+                    def part(r, eng):
+                        v = np.where(ok[r], eng.tree_lookup(lvl, prefix), 0.0)
+                        return np.concatenate([zeros, v] if (r >> j) & 1 else [v, zeros])
+                m = self._rank_sum(part)
+                m0, m1 = m[:shots], m[shots:]
+                with np.errstate(invalid="ignore", divide="ignore"):
+                    p0 = m0 / (m0 + m1)
+                res = uniforms_keys(keys, 0, k) >= p0
+                if p < self.nl:
+                    prefix |= res.astype(np.uint64) << np.uint64(pos[p])
+                    lvl += 1
+                else:
+                    for r in ok:
+                        ok[r] &= res == bool((r >> j) & 1)
+                val[q] = res
+            bit = np.uint64(1) << np.uint64(q)
+            out = np.where(val[q], out | bit, out & ~bit)
+        return out
+
     def _logical_order(self, phys_amps: np.ndarray) -> np.ndarray:
         """Amplitudes in physical index order -> logical index order."""
         n = self.n
@@ -331,7 +488,7 @@ class StateGroup(_Distributed):
 
     def __init__(self, num_qubits: int, global_qubits: int, precision: str = "f64", seed: int = 0,
                  engines=None):
-        self._init_layout(num_qubits, global_qubits)
+        self._init_layout(num_qubits, global_qubits, seed)
         w = 1 << global_qubits
         self.ranks = list(engines) if engines is not None else [DeviceRank(self.nl, seed, precision)
                                                                  for _ in range(w)]
@@ -339,6 +496,17 @@ class StateGroup(_Distributed):
             raise ValueError(f"{w} ranks needed")
         for r in range(1, w):
             self.ranks[r].zero()
+
+    def _local_ranks(self):
+        return list(enumerate(self.ranks))
+
+    def _rank_sum(self, fn) -> np.ndarray:
+        """The sum over ranks (in rank order) of fn(rank, engine)."""
+        total = None
+        for r, eng in enumerate(self.ranks):
+            v = np.asarray(fn(r, eng), dtype=np.float64)
+            total = v.copy() if total is None else total + v
+        return total
 
     def _run_local(self, run) -> None:
         for r, eng in enumerate(self.ranks):
@@ -382,10 +550,23 @@ class DistributedState(_Distributed):
         g = world.bit_length() - 1
         if 1 << g != world:
             raise ValueError("the number of ranks must be a power of two")
-        self._init_layout(num_qubits, g)
+        self._init_layout(num_qubits, g, seed)
         self.engine = engine if engine is not None else DeviceRank(self.nl, seed, precision)
         if self.rank != 0:
             self.engine.zero()
+
+    def _local_ranks(self):
+        return [(self.rank, self.engine)]
+
+    def _rank_sum(self, fn) -> np.ndarray:
+        """fn(rank, engine) summed over the process group (all-reduce; the same on every rank)."""
+        import torch
+
+        from .dist import _device
+        t = torch.tensor(np.asarray(fn(self.rank, self.engine), dtype=np.float64), dtype=torch.float64,
+                         device=_device())
+        self._dist.all_reduce(t)
+        return t.cpu().numpy()
 
     def _run_local(self, run) -> None:
         gl, ph = translate(run, self.nl, self.rank)

@@ -53,6 +53,23 @@ def uniforms(seed: int, stream: int, start: int, count: int) -> np.ndarray:
     return (w >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
 
 
+def uniforms_keys(seeds, stream: int, index: int) -> np.ndarray:
+    """Draw ``index`` of (seed, stream) for every seed of an array (one shot per key, the
+    way shot s of a run draws from key base_seed + s)."""
+    seeds = np.asarray(seeds, dtype=np.uint64)
+    blk = int(index) >> 1
+    x0, x1, x2, x3 = philox4x32_10(np.full(seeds.shape, blk & 0xFFFFFFFF, dtype=np.uint64),
+                                   np.full(seeds.shape, blk >> 32, dtype=np.uint64),
+                                   np.full(seeds.shape, stream, dtype=np.uint64), np.zeros(seeds.shape, dtype=np.uint64),
+                                   seeds & _MASK32, seeds >> np.uint64(32))
+    if int(index) & 1:
+        hi, lo = x2.astype(np.uint64), x3.astype(np.uint64)
+    else:
+        hi, lo = x0.astype(np.uint64), x1.astype(np.uint64)
+    w = (hi << np.uint64(32)) | lo
+    return (w >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
 class Stream:
     """Sequential reader of one (seed, stream) pair."""
 

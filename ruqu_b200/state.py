@@ -244,6 +244,21 @@ class QuantumState:
                                   out.ctypes.data_as(C.POINTER(C.c_uint64))))
         return out
 
+    def tree_build(self, qubits) -> None:
+        """Build the FP64 prefix tree of the sampler over ``qubits`` (in that order, the
+        rest after them) from the current amplitudes."""
+        qs = np.ascontiguousarray(qubits, dtype=np.uint32)
+        check(lib.rq_state_tree_build(self._h, qs.ctypes.data_as(C.POINTER(C.c_uint32)), len(qs)))
+
+    def tree_lookup(self, level: int, index) -> np.ndarray:
+        """Entries ``index`` of tree level ``level``: sums of |a|^2 over the amplitudes whose
+        first ``level`` tree qubits take the bits of the index."""
+        idx = np.ascontiguousarray(index, dtype=np.uint64)
+        out = np.empty(len(idx), dtype=np.float64)
+        check(lib.rq_state_tree_lookup(self._h, int(level), idx.ctypes.data_as(C.POINTER(C.c_uint64)), len(idx),
+                                       _dp(out)))
+        return out
+
     # ---- expectations (state.rs:362-408) ----
     def expectation_value(self, pauli) -> float:
         arr, off = pauli_array([pauli])

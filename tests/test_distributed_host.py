@@ -55,6 +55,20 @@ class OracleRank:
     def expectation(self, strings):
         return [self.s.expectation(st) if st else float(np.sum(np.abs(self.s.amplitudes()) ** 2)) for st in strings]
 
+    def tree_build(self, bits):
+        """The sampler's prefix tree over the local bits in that order (the rest after them):
+        entry j of level L sums |a|^2 over the amplitudes whose first L ordered bits are j."""
+        p = np.abs(self.s.amplitudes()) ** 2
+        order = list(bits) + [b for b in range(self.nl) if b not in bits]
+        j = np.arange(1 << self.nl)
+        src = np.zeros_like(j)
+        for k, b in enumerate(order):
+            src |= ((j >> k) & 1) << b
+        self._pj = p[src]
+
+    def tree_lookup(self, level, index):
+        return self._pj.reshape(-1, 1 << level).sum(axis=0)[np.asarray(index, dtype=np.int64)]
+
     def amplitudes(self):
         return self.s.amplitudes()
 
@@ -163,10 +177,13 @@ def _spmd_worker(rank, world, port, n, seed, q):
         strings = random_strings(n, 8, rng)
         ev = st.expectation_values(strings)
         sv = st.state_vector()
+        outs = [st.measure(x) for x in (n - 1, 0)]
+        shots = st.sample(300, 5)
+        sv2 = st.state_vector()
         tdist.barrier()
         tdist.destroy_process_group()
         if rank == 0:
-            q.put(("ok", gates, strings, ev, sv))
+            q.put(("ok", gates, strings, ev, sv, [(o.qubit, o.result, o.probability) for o in outs], shots, sv2))
     except Exception as e:     # report to the parent instead of hanging it
         q.put(("error", repr(e)))
 
@@ -184,8 +201,83 @@ def test_spmd_over_gloo_matches_one_state(world, n):
     for p in procs:
         p.join(timeout=120)
     assert res[0] == "ok", res
-    _, gates, strings, ev, sv = res
+    _, gates, strings, ev, sv, outs, shots, sv2 = res
     full = _full(n, gates)
     assert np.max(np.abs(sv - full.amplitudes())) < 1e-12
     want = [full.expectation(st) if st else 1.0 for st in strings]
     assert np.max(np.abs(ev - np.asarray(want))) < 1e-12
+    for (qb, r, pr), x in zip(outs, (n - 1, 0)):
+        w = full.measure(x)
+        assert (qb, r) == (w[0], w[1]) and abs(pr - w[2]) < 1e-12
+    assert np.max(np.abs(sv2 - full.amplitudes())) < 1e-12
+    want = oracle.tree_sample(np.abs(full.amplitudes()) ** 2, n, list(range(n)), 5, 300)
+    assert np.array_equal(shots, want)
+
+
+def _group(n, g, seed, gates):
+    grp = StateGroup(n, g, seed=seed, engines=[OracleRank(n - g) for _ in range(1 << g)])
+    full = oracle.OracleState(n, seed=seed)
+    ops = [x for x in gates if x[0] != BARRIER]
+    grp.apply_gates(ops)
+    full.apply(ops)
+    return grp, full
+
+
+def _split(grp):
+    """(a qubit held on a rank bit, a qubit held on a local bit) under the current layout."""
+    glob = next(q for q in range(grp.n) if not grp.layout.is_local(q))
+    loc = next(q for q in range(grp.n) if grp.layout.is_local(q))
+    return glob, loc
+
+
+@pytest.mark.parametrize("n,g,seed", [(7, 1, 1), (8, 2, 2), (9, 3, 3), (6, 2, 4)])
+def test_group_measure_and_reset_match_one_state(n, g, seed):
+    """measure / reset_qubit / measure_all / Measure and Reset gates of a distributed state
+    equal QuantumState's (state.rs:288-352) on one oracle state with the same stream:
+    outcomes exact, probabilities and amplitudes to 1e-12, on global and local qubits."""
+    rng = np.random.default_rng(seed)
+    grp, full = _group(n, g, seed, random_circuit(n, 80, rng))
+    for _ in range(3):
+        for q in _split(grp):
+            out, want = grp.measure(q), full.measure(q)
+            assert (out.qubit, out.result) == (want[0], want[1])
+            assert abs(out.probability - want[2]) < 1e-12
+            assert np.max(np.abs(grp.state_vector() - full.amplitudes())) < 1e-12
+        more = [x for x in random_circuit(n, 30, rng) if x[0] != BARRIER]
+        grp.apply_gates(more)
+        full.apply(more)
+    for q in _split(grp):
+        grp.reset_qubit(q)
+        full.reset_qubit(q)
+        assert np.max(np.abs(grp.state_vector() - full.amplitudes())) < 1e-12
+    tail = [(H, k, 0, 0.0) for k in range(n)] + [(MEASURE, n - 1, 0, 0.0), (RESET, 0, 0, 0.0), (CNOT, 0, n - 1, 0.0),
+                                                  (MEASURE, 1, 0, 0.0)]
+    got = grp.apply_gates(tail)
+    want = full.apply(tail)
+    assert [(o.qubit, o.result) for o in got] == [(w[0], w[1]) for w in want]
+    assert np.max(np.abs(grp.state_vector() - full.amplitudes())) < 1e-12
+    grp.apply_gates([(H, k, 0, 0.0) for k in range(n)])
+    full.apply([(H, k, 0, 0.0) for k in range(n)])
+    outs = grp.measure_all()
+    want = [full.measure(q) for q in range(n)]
+    assert [(o.qubit, o.result) for o in outs] == [(w[0], w[1]) for w in want]
+    assert np.max(np.abs(grp.state_vector() - full.amplitudes())) < 1e-12
+    assert len(grp.measurement_record) == 3 * 2 + 2 + 3 + n     # reset_qubit measures too
+
+
+@pytest.mark.parametrize("n,g,seed", [(7, 1, 1), (8, 2, 2), (9, 3, 3)])
+def test_group_sample_matches_the_tree_sampler(n, g, seed):
+    """Shots of a distributed state equal the one-state sampler's (simulator.rs:107-147
+    semantics) on the same probabilities: all qubits, a subset in a shuffled order with a
+    repeat, and a single global qubit."""
+    rng = np.random.default_rng(seed)
+    grp, full = _group(n, g, seed, random_circuit(n, 100, rng))
+    probs = np.abs(full.amplitudes()) ** 2
+    glob, loc = _split(grp)
+    for qubits in (None, [glob, loc, (loc + 2) % n, glob, 1], [glob]):
+        got = grp.sample(400, base_seed=9, qubits=qubits)
+        qs = list(range(n)) if qubits is None else qubits
+        assert np.array_equal(got, oracle.tree_sample(probs, n, qs, 9, 400)), qubits
+    assert grp.sample(0).size == 0
+    with pytest.raises(Exception):
+        grp.measure(n)

@@ -89,3 +89,66 @@ def test_half_copy_round_trip():
     assert np.array_equal(s.state_vector(), want)
     with pytest.raises(rq.InvalidArgument):
         s.half_copy(3, 2, buf.data_ptr())
+
+
+def test_prefix_tree_lookups_match_numpy():
+    """rq_state_tree_build / rq_state_tree_lookup: level L, entry j = sum of |a|^2 over the
+    amplitudes whose first L tree qubits (the listed order, then the rest) take the bits of
+    j; level 0 is the squared norm, level n the probabilities."""
+    n = 11
+    r = np.random.default_rng(3)
+    a = r.normal(size=1 << n) + 1j * r.normal(size=1 << n)
+    for prec, tol in (("f64", 1e-12), ("f32", 1e-6)):
+        s = rq.QuantumState.from_amplitudes(a, n, prec)
+        with pytest.raises(rq.InvalidArgument):
+            s.tree_lookup(0, [0])                      # no tree yet
+        amps = s.state_vector()
+        p = np.abs(amps) ** 2
+        for listed in ([3, 0, 7], [10, 2, 2, 5, 1], []):
+            s.tree_build(listed)
+            order = list(dict.fromkeys(listed)) + [q for q in range(n) if q not in listed]
+            j = np.arange(1 << n)
+            src = np.zeros_like(j)
+            for k, q in enumerate(order):
+                src |= ((j >> k) & 1) << q
+            pj = p[src]
+            for level in range(n + 1):
+                want = pj.reshape(-1, 1 << level).sum(axis=0)
+                idx = np.arange(1 << level, dtype=np.uint64)
+                got = s.tree_lookup(level, idx)
+                assert np.max(np.abs(got - want)) < tol * max(1.0, float(np.sum(p))), (prec, listed, level)
+        with pytest.raises(rq.InvalidArgument):
+            s.tree_lookup(3, [8])
+        with pytest.raises(rq.InvalidArgument):
+            s.tree_lookup(n + 1, [0])
+        with pytest.raises(rq.InvalidQubitIndex):
+            s.tree_build([n])
+
+
+@pytest.mark.parametrize("n,g,prec,seed", [(12, 1, "f64", 5), (13, 2, "f64", 6), (14, 2, "f32", 7)])
+def test_group_measure_reset_sample_on_device_match_one_state(n, g, prec, seed):
+    """measure / reset_qubit / Measure gates / sample of a distributed state (all ranks on
+    this GPU) equal one QuantumState's with the same measurement seed: outcomes and shots
+    exact, probabilities and amplitudes 1e-12 (f64) / 1e-5 (f32)."""
+    tol = 1e-12 if prec == "f64" else 1e-5
+    gates = _random_circuit(n, 150, seed)
+    grp = StateGroup(n, g, prec, seed=seed, engines=[DeviceRank(n - g, 0, prec) for _ in range(1 << g)])
+    one = rq.QuantumState(n, seed, prec)
+    grp.apply_gates(gates)
+    one.apply_gates(gates)
+    glob = next(q for q in range(n) if not grp.layout.is_local(q))
+    loc = next(q for q in range(n) if grp.layout.is_local(q))
+    for q in (glob, loc, glob):
+        a, b = grp.measure(q), one.measure(q)
+        assert (a.qubit, a.result) == (b.qubit, b.result)
+        assert abs(a.probability - b.probability) < tol
+        assert np.max(np.abs(grp.state_vector() - one.state_vector())) < tol
+    more = _random_circuit(n, 60, seed + 1) + [(16, loc, 0, 0.0), (17, glob, 0, 0.0)]
+    got = grp.apply_gates(more)
+    want = one.apply_gates(more)
+    assert [(o.qubit, o.result) for o in got] == [(o.qubit, o.result) for o in want]
+    assert np.max(np.abs(grp.state_vector() - one.state_vector())) < tol
+    grp.apply_gates([(H, k, 0, 0.0) for k in range(0, n, 2)])
+    one.apply_gates([(H, k, 0, 0.0) for k in range(0, n, 2)])
+    for qubits in (None, [glob, loc, 3, glob]):
+        assert np.array_equal(grp.sample(1024, 42, qubits), one.sample(1024, 42, qubits)), qubits

@@ -215,3 +215,39 @@ def test_apply_with_new_angles_reuses_the_structure_across_states_and_streams():
             st.reset()
             st.apply_gates(g, rq.RQ_EXEC_SWEEP_TC16)
             assert float(np.max(np.abs(st.state_vector() - refs[k]))) < 1e-5, (rounds, k)
+
+
+def test_tc16_non_unitary_matrices_run_on_the_tf32_split():
+    """A Unitary1Q matrix that is not unitary (a scaled projector, a general 2x2) breaks the
+    FP16-split sweep's tile bound and norm restoration, so such lists plan as 3xTF32 sweeps
+    (also under RQ_EXEC_SWEEP_TC16), a TC16 plan refuses such values in rq_plan_update, and
+    apply_gates re-plans them; every result matches the oracle (1e-5 of the largest
+    amplitude)."""
+    n = 14
+    base = workloads.random_layer_circuit(n, 4, 7)
+    had = [2 ** -0.5, 0.0, 2 ** -0.5, 0.0, 2 ** -0.5, 0.0, -(2 ** -0.5), 0.0]
+    proj = [3.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0]
+    gen = [0.3, 0.1, 1.2, -0.4, 0.0, 0.7, 0.9, 0.2]
+    unit = base[:40] + [(19, 3, 0, 0.0, had), (19, 9, 0, 0.0, had)] + base[40:]
+    nonu = base[:40] + [(19, 3, 0, 0.0, proj), (19, 9, 0, 0.0, gen)] + base[40:]
+
+    def err(g, gates):
+        ref = _oracle_f64(n, gates)
+        return float(np.max(np.abs(g.state_vector() - ref))) / max(1.0, float(np.max(np.abs(ref))))
+
+    g = QuantumState(n, 0, "f32")
+    plan = rq.Plan(g, nonu, rq.RQ_EXEC_SWEEP_TC16)
+    assert plan.stats()["exec_mode"] == rq.RQ_EXEC_SWEEP_TC
+    plan.execute(g)
+    assert err(g, nonu) < 1e-5
+    g.reset()
+    p16 = rq.Plan(g, unit, rq.RQ_EXEC_SWEEP_TC16)
+    assert p16.stats()["exec_mode"] == rq.RQ_EXEC_SWEEP_TC16
+    with pytest.raises(rq.CircuitError):
+        p16.update(g, nonu)
+    p16.execute(g)
+    assert err(g, unit) < 1e-5
+    for gates in (unit, nonu, unit):   # the apply path: structure match, then a fresh plan
+        g.reset()
+        g.apply_gates(gates, rq.RQ_EXEC_SWEEP_TC16)
+        assert err(g, gates) < 1e-5
