@@ -493,6 +493,17 @@ RQ_API int rq_qaoa_batch_last_ms(const rq_qaoa_batch* b, float* ms);
  * prefix tree; times are CUDA events around each class's launches. */
 RQ_API int rq_qaoa_batch_last_profile(const rq_qaoa_batch* b, double* out6);
 
+/* CUDA graphs of the batched runs (rq_qaoa_batch_run / _gradient, rq_vqe_batch_run): the
+ * first run of a shape (sizes, gradient mode, shots and seed, buffers) launches its kernels
+ * one by one and is the one the profile describes; the next run of the same shape captures
+ * the same kernels into a graph and launches it, later runs replay it (one launch per run;
+ * the angles and parameters are uploaded before it, the results read after it).  Results
+ * are those of the plain launches.  On by default (off with RUQU_NO_GRAPHS=1 in the
+ * environment).  *replayed = 1 if the last run launched the graph, *kernels = the kernels
+ * in the captured graph. */
+RQ_API int rq_qaoa_batch_set_graphs(rq_qaoa_batch* b, int32_t enable);
+RQ_API int rq_qaoa_batch_last_graph(const rq_qaoa_batch* b, int32_t* replayed, uint64_t* kernels);
+
 /* Upper bound of state memory per wave (default 24 GiB). */
 RQ_API int rq_qaoa_batch_set_state_budget(rq_qaoa_batch* b, uint64_t bytes);
 
@@ -537,6 +548,9 @@ RQ_API int rq_vqe_batch_last_ms(const rq_vqe_batch* b, float* ms);
  * adjoint ms}.  The waves are sized to stay in L2, so the sweep bytes are mostly L2
  * traffic.  No counterpart in the reference. */
 RQ_API int rq_vqe_batch_last_profile(const rq_vqe_batch* b, double* out6);
+/* As rq_qaoa_batch_set_graphs / _last_graph for rq_vqe_batch_run. */
+RQ_API int rq_vqe_batch_set_graphs(rq_vqe_batch* b, int32_t enable);
+RQ_API int rq_vqe_batch_last_graph(const rq_vqe_batch* b, int32_t* replayed, uint64_t* kernels);
 RQ_API int rq_vqe_batch_destroy(rq_vqe_batch* b);
 
 /* ------------------------------------------------------------------------ */

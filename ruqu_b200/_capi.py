@@ -99,6 +99,10 @@ SIGNATURES = {
     "rq_qaoa_batch_set_convergence": (C.c_int, [_vp, _dbl]),
     "rq_qaoa_batch_last_ms": (C.c_int, [_vp, _P(C.c_float)]),
     "rq_qaoa_batch_last_profile": (C.c_int, [_vp, _P(_dbl)]),
+    "rq_qaoa_batch_set_graphs": (C.c_int, [_vp, _i32]),
+    "rq_qaoa_batch_last_graph": (C.c_int, [_vp, _P(_i32), _P(_u64)]),
+    "rq_vqe_batch_set_graphs": (C.c_int, [_vp, _i32]),
+    "rq_vqe_batch_last_graph": (C.c_int, [_vp, _P(_i32), _P(_u64)]),
     "rq_qaoa_batch_set_state_budget": (C.c_int, [_vp, _u64]),
     "rq_qaoa_batch_destroy": (C.c_int, [_vp]),
     "rq_vqe_batch_create": (C.c_int, [_u32, _u32, _P(_dbl), _P(RqPauliOp), _P(_u32), _u32, _i32, _P(_vp)]),

@@ -147,6 +147,16 @@ class QaoaBatch:
     def set_state_budget(self, nbytes: int) -> None:
         check(lib.rq_qaoa_batch_set_state_budget(self._h, int(nbytes)))
 
+    def set_graphs(self, enable: bool) -> None:
+        """Capture repeated runs of one shape as a CUDA graph (default on)."""
+        check(lib.rq_qaoa_batch_set_graphs(self._h, 1 if enable else 0))
+
+    def last_graph(self) -> dict:
+        """Whether the last run / gradient launched its captured graph, and its kernel count."""
+        r, k = C.c_int32(), C.c_uint64()
+        check(lib.rq_qaoa_batch_last_graph(self._h, C.byref(r), C.byref(k)))
+        return {"replayed": bool(r.value), "kernels": int(k.value)}
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None:
@@ -198,6 +208,16 @@ class VqeBatch:
         ms = C.c_float()
         check(lib.rq_vqe_batch_last_ms(self._h, C.byref(ms)))
         return ms.value
+
+    def set_graphs(self, enable: bool) -> None:
+        """Capture repeated runs of one shape as a CUDA graph (default on)."""
+        check(lib.rq_vqe_batch_set_graphs(self._h, 1 if enable else 0))
+
+    def last_graph(self) -> dict:
+        """Whether the last run launched its captured graph, and its kernel count."""
+        r, k = C.c_int32(), C.c_uint64()
+        check(lib.rq_vqe_batch_last_graph(self._h, C.byref(r), C.byref(k)))
+        return {"replayed": bool(r.value), "kernels": int(k.value)}
 
     def __del__(self):
         h = getattr(self, "_h", None)

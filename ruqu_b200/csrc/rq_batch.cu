@@ -1156,6 +1156,71 @@ inline double sweep_bytes(const std::vector<SweepDesc>& descs, double state_byte
     return b;
 }
 
+// A run's kernels as one CUDA graph.  The first run of a shape (sizes, modes, seeds and
+// every buffer address the kernels see) launches plainly and is the profiled one; the next
+// run of the same shape captures the same launch sequence and launches the graph, and later
+// runs replay it.  A replay issues exactly the captured kernels with the captured
+// arguments, so its results are those of a plain run.  RUQU_NO_GRAPHS=1 or
+// rq_*_batch_set_graphs(0) keeps every run plain.
+struct RunGraph {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint64_t> key;      // shape of the last plain run (after it ran)
+    bool enabled = std::getenv("RUQU_NO_GRAPHS") == nullptr;
+    bool replayed = false;          // the last run launched the graph
+    uint64_t nodes = 0;             // kernels (graph nodes) of the captured run
+    void drop() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+    }
+    // enqueue() issues the run's work on st; key_now() gives the shape; ev0 is recorded right
+    // before the work (plain or graph)
+    template <class F, class K>
+    int run(cudaStream_t st, cudaEvent_t ev0, RunProfile& prof, F enqueue, K key_now) {
+        replayed = false;
+        const std::vector<uint64_t> k0 = key_now();
+        const bool same = enabled && !key.empty() && k0 == key;
+        if (!same) drop();
+        if (same && !exec) {
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed);
+            const int crc = e == cudaSuccess ? enqueue() : RQ_ERR_CUDA;
+            const cudaError_t e2 = e == cudaSuccess ? cudaStreamEndCapture(st, &g) : e;
+            bool ok = crc == RQ_OK && e2 == cudaSuccess && g && key_now() == key;
+            if (ok) {
+                size_t nn = 0;
+                cudaGraphGetNodes(g, nullptr, &nn);
+                nodes = nn;
+                ok = cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+            }
+            if (g) cudaGraphDestroy(g);
+            if (!ok) {   // capture did not work here: plain runs from now on
+                exec = nullptr;
+                enabled = false;
+                cudaGetLastError();
+            }
+        }
+        if (same && exec) {
+            RQ_CUDA(cudaEventRecord(ev0, st));
+            RQ_CUDA(cudaGraphLaunch(exec, st));
+            replayed = true;
+            return RQ_OK;
+        }
+        prof.start();
+        RQ_CUDA(cudaEventRecord(ev0, st));
+        const int rc = enqueue();
+        if (rc != RQ_OK) {
+            prof.on = false;
+            key.clear();
+            return rc;
+        }
+        key = key_now();
+        return RQ_OK;
+    }
+    void collect(RunProfile& prof) {   // after the stream has been synchronised
+        if (!replayed) prof.collect();
+    }
+};
+
 struct QClass {
     uint32_t n = 0, m = 0, c = 0;
     std::vector<uint32_t> insts;            // instances of this size
@@ -1213,6 +1278,7 @@ struct rq_qaoa_batch {
     uint32_t last_wave_n = 0;
     float last_ms = 0.f;
     RunProfile prof;
+    RunGraph graph;                        // rq_qaoa_batch_run / _gradient
     size_t state_budget = (size_t)24 << 30;
     double conv_tol = 0.0;                 // optimizers: stop an instance when |E - E_prev| < conv_tol (0: off)
 };
@@ -1533,6 +1599,7 @@ int rq_qaoa_batch_destroy(rq_qaoa_batch* b) {
                     b->d_best_bits, b->d_best_cut, b->d_states, b->d_epart, b->d_tree, b->d_lam, b->d_gpart,
                     b->d_grad};
     for (void* q : ptrs) if (q) cudaFree(q);
+    b->graph.drop();
     b->prof.release();
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
@@ -1592,6 +1659,15 @@ int qaoa_prepare(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, const d
     // the pageable sources must outlive the copies
     RQ_CUDA(cudaStreamSynchronize(b->stream));
     return RQ_OK;
+}
+
+// What a captured run depends on besides the uploaded angles: the run kind, sizes, seed and
+// every buffer its kernels read or write.
+std::vector<uint64_t> qaoa_shape(const rq_qaoa_batch* b, uint64_t kind, uint64_t nsets, uint64_t shots, uint64_t seed) {
+    auto a = [](const void* p) { return (uint64_t)(uintptr_t)p; };
+    return {kind, nsets, shots, seed, b->ninst, a(b->d_circ_inst), a(b->d_ang), a(b->d_rx), a(b->d_ph),
+            a(b->d_energy), a(b->d_best_bits), a(b->d_best_cut), a(b->d_states), a(b->d_epart), a(b->d_tree),
+            a(b->d_lam), a(b->d_gpart), a(b->d_grad), (uint64_t)b->state_budget};
 }
 
 // tables + every class's sweeps (+ shots) for the angles in d_ang; energies land in d_energy (run order).
@@ -1782,13 +1858,9 @@ int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, co
     RQ_CUDA(cudaSetDevice(b->device));
     const uint64_t ncirc = (uint64_t)b->ninst * nsets;
     RQ_TRY(qaoa_prepare(b, nsets, gammas, betas));
-    b->prof.start();
-    RQ_CUDA(cudaEventRecord(b->ev0, b->stream));
-    const int lrc = qaoa_launch(b, nsets, shots, base_seed);
-    if (lrc != RQ_OK) {
-        b->prof.on = false;
-        return lrc;
-    }
+    RQ_TRY(b->graph.run(
+        b->stream, b->ev0, b->prof, [&]() { return qaoa_launch(b, nsets, shots, base_seed); },
+        [&]() { return qaoa_shape(b, 0, nsets, shots, base_seed); }));
     RQ_CUDA(cudaEventRecord(b->ev1, b->stream));
     std::vector<double> e(ncirc);
     RQ_CUDA(cudaMemcpyAsync(e.data(), b->d_energy, ncirc * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
@@ -1802,7 +1874,7 @@ int rq_qaoa_batch_run(rq_qaoa_batch* b, uint32_t nsets, const double* gammas, co
     }
     RQ_CUDA(cudaStreamSynchronize(b->stream));
     RQ_CUDA(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
-    b->prof.collect();
+    b->graph.collect(b->prof);
     for (uint64_t k = 0; k < ncirc; ++k) {
         const uint64_t user = b->order[k];
         energies[user] = e[k];
@@ -1821,20 +1893,16 @@ int rq_qaoa_batch_gradient(rq_qaoa_batch* b, const double* gammas, const double*
     RQ_CUDA(cudaSetDevice(b->device));
     const uint32_t p = b->p, P2 = 2 * p, ninst = b->ninst;
     RQ_TRY(qaoa_prepare(b, 1, gammas, betas));
-    b->prof.start();
-    RQ_CUDA(cudaEventRecord(b->ev0, b->stream));
-    const int lrc = qaoa_launch(b, 1, 0, 0, nullptr, true);
-    if (lrc != RQ_OK) {
-        b->prof.on = false;
-        return lrc;
-    }
+    RQ_TRY(b->graph.run(
+        b->stream, b->ev0, b->prof, [&]() { return qaoa_launch(b, 1, 0, 0, nullptr, true); },
+        [&]() { return qaoa_shape(b, 1, 1, 0, 0); }));
     RQ_CUDA(cudaEventRecord(b->ev1, b->stream));
     std::vector<double> e(ninst), g((size_t)ninst * P2);
     RQ_CUDA(cudaMemcpyAsync(e.data(), b->d_energy, ninst * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
     RQ_CUDA(cudaMemcpyAsync(g.data(), b->d_grad, g.size() * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
     RQ_CUDA(cudaStreamSynchronize(b->stream));
     RQ_CUDA(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
-    b->prof.collect();
+    b->graph.collect(b->prof);
     for (uint32_t k = 0; k < ninst; ++k) {
         const uint64_t user = b->order[k];
         energies[user] = e[k];
@@ -2109,6 +2177,23 @@ int rq_qaoa_batch_last_profile(const rq_qaoa_batch* b, double* out6) {
     return RQ_OK;
 }
 
+int rq_qaoa_batch_set_graphs(rq_qaoa_batch* b, int32_t enable) {
+    if (!b) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    RQ_CUDA(cudaSetDevice(b->device));
+    RQ_CUDA(cudaStreamSynchronize(b->stream));
+    b->graph.drop();
+    b->graph.key.clear();
+    b->graph.enabled = enable != 0;
+    return RQ_OK;
+}
+
+int rq_qaoa_batch_last_graph(const rq_qaoa_batch* b, int32_t* replayed, uint64_t* kernels) {
+    if (!b || !replayed || !kernels) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    *replayed = b->graph.replayed ? 1 : 0;
+    *kernels = b->graph.nodes;
+    return RQ_OK;
+}
+
 int rq_qaoa_batch_last_ms(const rq_qaoa_batch* b, float* ms) {
     if (!b || !ms) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
     *ms = b->last_ms;
@@ -2157,6 +2242,7 @@ struct rq_vqe_batch {
     size_t energy_cap = 0;
     float last_ms = 0.f;
     RunProfile prof;
+    RunGraph graph;                         // rq_vqe_batch_run
     size_t wave_bytes = (size_t)96 << 20;   // states per wave kept around the L2 size
     // exact gradients: the reversed ansatz as an adjoint program, H as operator strings
     uint32_t am = 0;
@@ -2280,6 +2366,39 @@ int vqe_adjoint(rq_vqe_batch* b, uint64_t ncirc, uint64_t circ0) {
         k_grad_finalize<<<rq::grid_for(ncirc * b->P, TPB, sms), TPB, 0, b->stream>>>(b->d_gpart, ncirc, b->antiles,
                                                                                    b->P, circ0, b->d_grad);
         RQ_CUDA(cudaGetLastError());
+    }
+    return RQ_OK;
+}
+
+// every kernel of one VQE run: the rotation table, then per wave the ansatz sweeps, the
+// energies and (adjoint) the backward pass
+int vqe_enqueue(rq_vqe_batch* b, uint64_t ncirc, uint32_t V, uint64_t wave, bool adj) {
+    const uint32_t P = b->P;
+    const int sms = rq::num_sms(b->device);
+    if (b->prec == RQ_F32)
+        k_vqe_rot<float><<<rq::grid_for(ncirc * P, TPB, sms), TPB, 0, b->stream>>>(b->d_params, ncirc, P, V, (float*)b->d_rot);
+    else
+        k_vqe_rot<double><<<rq::grid_for(ncirc * P, TPB, sms), TPB, 0, b->stream>>>(b->d_params, ncirc, P, V, (double*)b->d_rot);
+    RQ_CUDA(cudaGetLastError());
+    for (uint64_t w0 = 0; w0 < ncirc; w0 += wave) {
+        const uint64_t wn = std::min<uint64_t>(wave, ncirc - w0);
+        if (b->prec == RQ_F32) {
+            RQ_TRY(vqe_wave<float>(b, wn, w0));
+            if (adj) {
+                const int ev = b->prof.begin(b->stream);
+                RQ_TRY(vqe_adjoint<float>(b, wn, w0));
+                b->prof.end(ev, b->stream, 2, (double)wn * (2.0 * (double)((size_t)8 << b->n) +
+                                                            sweep_bytes(b->adescs, (double)((size_t)8 << b->n), 2.0)));
+            }
+        } else {
+            RQ_TRY(vqe_wave<double>(b, wn, w0));
+            if (adj) {
+                const int ev = b->prof.begin(b->stream);
+                RQ_TRY(vqe_adjoint<double>(b, wn, w0));
+                b->prof.end(ev, b->stream, 2, (double)wn * (2.0 * (double)((size_t)16 << b->n) +
+                                                            sweep_bytes(b->adescs, (double)((size_t)16 << b->n), 2.0)));
+            }
+        }
     }
     return RQ_OK;
 }
@@ -2488,34 +2607,13 @@ int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* params, int3
         RQ_CUDA(cudaMemsetAsync(b->d_grad, 0, (size_t)nsets * P * sizeof(double), b->stream));
     }
     RQ_CUDA(cudaMemcpyAsync(b->d_params, params, (size_t)nsets * P * sizeof(double), cudaMemcpyHostToDevice, b->stream));
-    const int sms = rq::num_sms(b->device);
-    b->prof.start();
-    RQ_CUDA(cudaEventRecord(b->ev0, b->stream));
-    if (b->prec == RQ_F32)
-        k_vqe_rot<float><<<rq::grid_for(ncirc * P, TPB, sms), TPB, 0, b->stream>>>(b->d_params, ncirc, P, V, (float*)b->d_rot);
-    else
-        k_vqe_rot<double><<<rq::grid_for(ncirc * P, TPB, sms), TPB, 0, b->stream>>>(b->d_params, ncirc, P, V, (double*)b->d_rot);
-    RQ_CUDA(cudaGetLastError());
-    for (uint64_t w0 = 0; w0 < ncirc; w0 += wave) {
-        const uint64_t wn = std::min<uint64_t>(wave, ncirc - w0);
-        if (b->prec == RQ_F32) {
-            RQ_TRY(vqe_wave<float>(b, wn, w0));
-            if (adj) {
-                const int ev = b->prof.begin(b->stream);
-                RQ_TRY(vqe_adjoint<float>(b, wn, w0));
-                b->prof.end(ev, b->stream, 2, (double)wn * (2.0 * (double)((size_t)8 << b->n) +
-                                                            sweep_bytes(b->adescs, (double)((size_t)8 << b->n), 2.0)));
-            }
-        } else {
-            RQ_TRY(vqe_wave<double>(b, wn, w0));
-            if (adj) {
-                const int ev = b->prof.begin(b->stream);
-                RQ_TRY(vqe_adjoint<double>(b, wn, w0));
-                b->prof.end(ev, b->stream, 2, (double)wn * (2.0 * (double)((size_t)16 << b->n) +
-                                                            sweep_bytes(b->adescs, (double)((size_t)16 << b->n), 2.0)));
-            }
-        }
-    }
+    RQ_TRY(b->graph.run(
+        b->stream, b->ev0, b->prof, [&]() { return vqe_enqueue(b, ncirc, V, wave, adj); },
+        [&]() {
+            auto a = [](const void* p) { return (uint64_t)(uintptr_t)p; };
+            return std::vector<uint64_t>{ncirc, V, wave, (uint64_t)adj, a(b->d_params), a(b->d_rot), a(b->d_energy),
+                                         a(b->d_states), a(b->d_part), a(b->d_lam), a(b->d_gpart), a(b->d_grad)};
+        }));
     RQ_CUDA(cudaEventRecord(b->ev1, b->stream));
     std::vector<double> e(ncirc);
     RQ_CUDA(cudaMemcpyAsync(e.data(), b->d_energy, ncirc * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
@@ -2524,7 +2622,7 @@ int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* params, int3
                                 b->stream));
     RQ_CUDA(cudaStreamSynchronize(b->stream));
     RQ_CUDA(cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
-    b->prof.collect();
+    b->graph.collect(b->prof);
     for (uint32_t s = 0; s < nsets; ++s) {
         energies[s] = e[(uint64_t)s * V];
         if (with_gradient == RQ_VQE_GRAD_SHIFT)
@@ -2534,12 +2632,30 @@ int rq_vqe_batch_run(rq_vqe_batch* b, uint32_t nsets, const double* params, int3
     return RQ_OK;
 }
 
+
 int rq_vqe_batch_last_profile(const rq_vqe_batch* b, double* out6) {
     if (!b || !out6) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
     for (int k = 0; k < 3; ++k) {
         out6[2 * k] = b->prof.work[k];
         out6[2 * k + 1] = b->prof.ms[k];
     }
+    return RQ_OK;
+}
+
+int rq_vqe_batch_set_graphs(rq_vqe_batch* b, int32_t enable) {
+    if (!b) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    RQ_CUDA(cudaSetDevice(b->device));
+    RQ_CUDA(cudaStreamSynchronize(b->stream));
+    b->graph.drop();
+    b->graph.key.clear();
+    b->graph.enabled = enable != 0;
+    return RQ_OK;
+}
+
+int rq_vqe_batch_last_graph(const rq_vqe_batch* b, int32_t* replayed, uint64_t* kernels) {
+    if (!b || !replayed || !kernels) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    *replayed = b->graph.replayed ? 1 : 0;
+    *kernels = b->graph.nodes;
     return RQ_OK;
 }
 
@@ -2556,6 +2672,7 @@ int rq_vqe_batch_destroy(rq_vqe_batch* b) {
     void* ptrs[] = {b->prog,     b->d_groups, b->d_terms, b->d_gofs,  b->d_part, b->d_params, b->d_rot,
                     b->d_states, b->d_energy, b->aprog,   b->d_hterms, b->d_lam,  b->d_gpart,  b->d_grad};
     for (void* q : ptrs) if (q) cudaFree(q);
+    b->graph.drop();
     b->prof.release();
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);

@@ -145,3 +145,37 @@ def test_batch_best_cut_of_every_wave_matches_oracle_sampler():
         probs = a.real * a.real + a.imag * a.imag
         assert _best_from_oracle(probs, n, e, 7 + (k << 32), 1024) == (int(out["best_bits"][k]),
                                                                          int(out["best_cut"][k])), (k, n)
+
+
+def test_repeated_runs_replay_one_graph_with_identical_results():
+    """rq_qaoa_batch_run / _gradient as CUDA graphs: the first run of a shape is plain, the
+    second captures and launches the graph, later ones replay it; energies, shots and
+    gradients equal those of a batch that never uses graphs, for new angles every run, and
+    a new shape (other shot count) runs plainly again."""
+    graphs = _graphs([10, 12, 12, 14, 16], 21)
+    r = np.random.default_rng(4)
+    a = QaoaBatch(graphs, 3, "f32")
+    plain = QaoaBatch(graphs, 3, "f32")
+    plain.set_graphs(False)
+    flags = []
+    for it in range(4):
+        gam = r.uniform(0, math.pi, size=(len(graphs), 2, 3))
+        bet = r.uniform(0, math.pi / 2, size=(len(graphs), 2, 3))
+        x = a.run(gam, bet, shots=256, seed=77)
+        flags.append(a.last_graph()["replayed"])
+        y = plain.run(gam, bet, shots=256, seed=77)
+        assert not plain.last_graph()["replayed"]
+        for k in ("energies", "best_bits", "best_cut"):
+            assert np.array_equal(x[k], y[k]), (it, k)
+    assert flags == [False, True, True, True]
+    assert a.last_graph()["kernels"] > 5
+    x = a.run(gam, bet, shots=128, seed=77)
+    assert not a.last_graph()["replayed"]
+    assert np.array_equal(x["energies"], plain.run(gam, bet, shots=128, seed=77)["energies"])
+    for it in range(3):
+        g1 = r.uniform(0, math.pi, size=(len(graphs), 3))
+        b1 = r.uniform(0, math.pi / 2, size=(len(graphs), 3))
+        ea, ga = a.gradient(g1, b1)
+        eb, gb = plain.gradient(g1, b1)
+        assert np.array_equal(ea, eb) and np.array_equal(ga, gb)
+        assert a.last_graph()["replayed"] == (it > 0)

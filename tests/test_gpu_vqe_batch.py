@@ -75,3 +75,28 @@ def test_vqe_batch_f64_two_energy_tiles():
     for s in range(2):
         want = _energy(n, depth, params[s], coeffs, strings)
         assert abs(e[s] - want) < 1e-10, (e[s], want)
+
+
+@pytest.mark.parametrize("gradient", [False, "shift", "adjoint"])
+def test_vqe_runs_replay_one_graph_with_identical_results(gradient):
+    """rq_vqe_batch_run as a CUDA graph: results equal a batch
+    that never uses graphs, for new parameters every run; the first run of a shape is plain,
+    later ones launch the captured graph."""
+    n, depth = 12, 3
+    coeffs, strings = workloads.pauli_hamiltonian(n, 40, 7)
+    P = n * depth
+    r = np.random.default_rng(8)
+    a = VqeBatch(n, depth, coeffs, strings, "f32")
+    b = VqeBatch(n, depth, coeffs, strings, "f32")
+    b.set_graphs(False)
+    flags = []
+    for it in range(3):
+        params = r.uniform(-math.pi, math.pi, size=(5, P))
+        x = a.run(params, gradient=gradient)
+        flags.append(a.last_graph()["replayed"])
+        y = b.run(params, gradient=gradient)
+        if gradient:
+            assert np.array_equal(x[0], y[0]) and np.array_equal(x[1], y[1])
+        else:
+            assert np.array_equal(x, y)
+    assert flags == [False, True, True]
