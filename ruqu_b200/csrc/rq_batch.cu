@@ -50,6 +50,9 @@ __device__ __forceinline__ uint32_t swzb(uint32_t e) {
     return e ^ (f & ((1u << CB) - 1));
 }
 
+// index of the lowest set bit of 1 <= g < 32 (the Gray-code bit that flips at step g)
+__host__ __device__ constexpr int gray_bit(int g) { return (g & 1) ? 0 : (g & 2) ? 1 : (g & 4) ? 2 : (g & 8) ? 3 : 4; }
+
 // Per-class launch arguments.
 template <typename T>
 struct QArgs {
@@ -244,6 +247,14 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
     const uint32_t stid = swzb<T>(tid * EPV);   // swz(e) = stid ^ sgj[j] (the swizzle is XOR-linear)
     const uint64_t nwork = a.ncirc * a.ntiles;
     const uint64_t nstate = 1ull << d.n;
+    // the sweep's phase descriptors in shared memory, after the tile
+    PhaseDesc* sph = reinterpret_cast<PhaseDesc*>(smem_raw + ((size_t)1 << d.m) * sizeof(V));
+    {
+        const uint32_t nw = (d.phase_end - d.phase_begin) * (uint32_t)(sizeof(PhaseDesc) / 16);
+        const uint4* src = reinterpret_cast<const uint4*>(phases + d.phase_begin);
+        for (uint32_t k = tid; k < nw; k += T_) reinterpret_cast<uint4*>(sph)[k] = src[k];
+    }
+    __syncthreads();
 
     for (uint64_t w = blockIdx.x; w < nwork; w += gridDim.x) {
         const uint64_t circ = w / a.ntiles, tile = w - circ * a.ntiles;
@@ -281,7 +292,7 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
 
         double energy = 0.0;
         for (uint32_t p = d.phase_begin; p < d.phase_end; ++p) {
-            const PhaseDesc& ph = phases[p];
+            const PhaseDesc& ph = sph[p - d.phase_begin];
             uint32_t ebase = 0;
             uint64_t U = base;
             for (uint32_t b = 0; b < ph.nt; ++b)
@@ -293,6 +304,11 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
             uint64_t slotmask = 0;
 #pragma unroll
             for (int s = 0; s < RB; ++s) slotmask |= 1ull << ph.slot_global[s];
+            // register i sits at sb ^ (XOR of S[k] over the set bits k of i): visited in
+            // Gray-code order, each address is one XOR from the previous one
+            uint32_t S[RB];
+#pragma unroll
+            for (int k = 0; k < RB; ++k) S[k] = ph.slut[1 << k];
             V reg[NR];
             if (init && p == d.phase_begin) {
                 if (d.flags & SWEEP_INIT_UNIFORM) {
@@ -303,8 +319,12 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
                     for (int i = 0; i < NR; ++i) { reg[i].x = (i == 0 && U == 0) ? (T)1 : (T)0; reg[i].y = (T)0; }
                 }
             } else {
+                uint32_t ad = sb;
 #pragma unroll
-                for (int i = 0; i < NR; ++i) reg[i] = sm[sb ^ ph.slut[i]];
+                for (int g = 0; g < NR; ++g) {
+                    if (g) ad ^= S[gray_bit(g)];
+                    reg[g ^ (g >> 1)] = sm[ad];
+                }
             }
             for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
                 const SwOp op = ops[o];
@@ -343,8 +363,14 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
                     energy += (re * re + im * im) * (double)cut_of<RB>(cp, i);
                 }
             }
+            {
+                uint32_t ad = sb;
 #pragma unroll
-            for (int i = 0; i < NR; ++i) sm[sb ^ ph.slut[i]] = reg[i];
+                for (int g = 0; g < NR; ++g) {
+                    if (g) ad ^= S[gray_bit(g)];
+                    sm[ad] = reg[g ^ (g >> 1)];
+                }
+            }
             __syncthreads();
         }
 
@@ -1287,6 +1313,13 @@ namespace {
 
 size_t elem_size(int32_t prec) { return prec == RQ_F32 ? 8 : 16; }
 
+// the most phases of one sweep (k_batch_sweep keeps a sweep's phase descriptors in shared memory)
+size_t max_phases(const std::vector<SweepDesc>& descs) {
+    size_t m = 0;
+    for (const auto& d : descs) m = std::max<size_t>(m, d.phase_end - d.phase_begin);
+    return m;
+}
+
 template <typename P>
 int grow(P** ptr, size_t* cap, size_t need_elems) {
     if (*cap >= need_elems) return RQ_OK;
@@ -1524,6 +1557,7 @@ int rq_qaoa_batch_create(uint32_t ninst, const uint32_t* num_nodes, const uint32
         std::vector<SwOp> ops;
         std::vector<double> mats;
         build_program(sweeps, K.n, K.m, K.c, rb, precision == RQ_F32 ? 2 : 1, K.descs, phases, ops, mats);
+        K.smem += max_phases(K.descs) * sizeof(PhaseDesc);   // the phase descriptors after the tile
         K.descs.front().flags |= SWEEP_INIT_UNIFORM;
         K.descs.back().flags |= SWEEP_ENERGY;
         K.off_ops = (phases.size() * sizeof(PhaseDesc) + 255) & ~size_t(255);
@@ -2523,6 +2557,7 @@ int rq_vqe_batch_create(uint32_t num_qubits, uint32_t depth, const double* coeff
     std::vector<SwOp> opsv;
     std::vector<double> mats;
     build_program(sweeps, num_qubits, b->m, c, rb, precision == RQ_F32 ? 2 : 1, b->descs, phases, opsv, mats);
+    b->smem += max_phases(b->descs) * sizeof(PhaseDesc);   // the phase descriptors after the tile
     b->descs.front().flags |= SWEEP_INIT_ZERO;
     b->off_ops = (phases.size() * sizeof(PhaseDesc) + 255) & ~size_t(255);
     const size_t total = b->off_ops + opsv.size() * sizeof(SwOp);
