@@ -64,6 +64,7 @@ struct QArgs {
     const uint8_t* edges;          // (u, v) byte pairs of all instances
     const uint32_t* eoff;          // instance -> first edge
     const uint32_t* ne;            // instance -> edge count
+    const uint64_t* nbr;           // instance -> NBR_STRIDE neighbour masks (bit w of entry v: edge (v, w))
     const T* rot;                  // [global circuit][nparam] (cos, sin) of Rx(2 beta) / Ry(theta) half-angles
     uint32_t nparam;
     const T* ph;                   // [global circuit][p][phs] (re, im) of exp(-i gamma (|E| - 2k))
@@ -135,6 +136,51 @@ __device__ __forceinline__ int cut_of(const CutPlan<RB>& cp, int i) {
         const int s = (int)(ss & 7), t = (int)((ss >> 3) & 7);
         c += ((i >> s) ^ (i >> t)) & 1;
     }
+    return c;
+}
+
+// The same cut counts from neighbour masks N(v), for U with every slot bit 0:
+//   cut(U)             = sum over vertices v with U_v = 1 of popc(N(v) & ~U)
+//   flipping slot s    : delta_s = deg(s) - 2 popc(N(s) & U)   (slot neighbours count as 0)
+//   slots s, t both 1  : their shared edge was counted twice by delta_s + delta_t, -2 each
+// so cut(U | deposit(i)) = c0 + sum_{s in i} delta_s - 2 #(adjacent slot pairs in i).
+constexpr uint32_t NBR_STRIDE = 32;   // batched graphs have at most 30 vertices
+
+template <int RB>
+struct CutNb {
+    int c0;
+    int delta[RB];
+    uint32_t adj;      // bit s * RB + t (s < t): slots s and t adjacent
+};
+
+template <int RB>
+__device__ __forceinline__ void cut_plan_nb(CutNb<RB>& cp, const uint64_t* __restrict__ nb, uint64_t U,
+                                            const uint8_t* slot_global) {
+    int c0 = 0;
+    for (uint64_t m = U; m; m &= m - 1) c0 += __popcll(nb[__ffsll((long long)m) - 1] & ~U);
+    cp.c0 = c0;
+    cp.adj = 0;
+#pragma unroll
+    for (int s = 0; s < RB; ++s) {
+        const uint64_t ns = nb[slot_global[s]];
+        cp.delta[s] = __popcll(ns) - 2 * __popcll(ns & U);
+#pragma unroll
+        for (int t = s + 1; t < RB; ++t)
+            if ((ns >> slot_global[t]) & 1ull) cp.adj |= 1u << (s * RB + t);
+    }
+}
+
+template <int RB>
+__device__ __forceinline__ int cut_nb(const CutNb<RB>& cp, int i) {   // i: a compile-time register index
+    int c = cp.c0;
+#pragma unroll
+    for (int s = 0; s < RB; ++s)
+        if ((i >> s) & 1) c += cp.delta[s];
+#pragma unroll
+    for (int s = 0; s < RB; ++s)
+#pragma unroll
+        for (int t = s + 1; t < RB; ++t)
+            if (((i >> s) & 1) && ((i >> t) & 1)) c -= 2 * (int)((cp.adj >> (s * RB + t)) & 1u);
     return c;
 }
 
@@ -260,13 +306,8 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
         const uint64_t circ = w / a.ntiles, tile = w - circ * a.ntiles;
         const uint64_t gcirc = a.circ0 + circ;
         V* amps = a.amps + circ * nstate;
-        const uint8_t* edges = nullptr;
-        uint32_t ne = 0;
-        if (a.circ_inst) {
-            const uint32_t inst = a.circ_inst[gcirc];
-            edges = a.edges + 2 * (size_t)a.eoff[inst];
-            ne = a.ne[inst];
-        }
+        const uint64_t* nb = nullptr;   // the instance's neighbour masks (cost phase and energy)
+        if (a.circ_inst) nb = a.nbr + (size_t)a.circ_inst[gcirc] * NBR_STRIDE;
         uint64_t base = 0;
         for (uint32_t b = 0; b < d.nonlocal_count; ++b)
             if ((tile >> b) & 1ull) base |= 1ull << d.nonlocal[b];
@@ -344,23 +385,23 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
                         if (b0 & b1) { reg[i].x = -reg[i].x; reg[i].y = -reg[i].y; }
                     }
                 } else if (op.type == OP_CPH) {
-                    CutPlan<RB> cp;
-                    cut_plan<RB>(cp, edges, ne, U, slotmask);
+                    CutNb<RB> cp;
+                    cut_plan_nb<RB>(cp, nb, U, ph.slot_global);
                     const T* tab = a.ph + ((size_t)gcirc * a.p + op.param) * a.phs * 2;
 #pragma unroll
                     for (int i = 0; i < NR; ++i) {
-                        const int c = cut_of<RB>(cp, i);
+                        const int c = cut_nb<RB>(cp, i);
                         reg[i] = cmulv(reg[i], tab[2 * c], tab[2 * c + 1]);
                     }
                 }
             }
             if ((d.flags & SWEEP_ENERGY) && p + 1 == d.phase_end) {
-                CutPlan<RB> cp;
-                cut_plan<RB>(cp, edges, ne, U, slotmask);
+                CutNb<RB> cp;
+                cut_plan_nb<RB>(cp, nb, U, ph.slot_global);
 #pragma unroll
                 for (int i = 0; i < NR; ++i) {
                     const double re = (double)reg[i].x, im = (double)reg[i].y;
-                    energy += (re * re + im * im) * (double)cut_of<RB>(cp, i);
+                    energy += (re * re + im * im) * (double)cut_nb<RB>(cp, i);
                 }
             }
             {
@@ -1275,6 +1316,7 @@ struct rq_qaoa_batch {
     uint8_t* d_edges = nullptr;
     uint32_t* d_eoff = nullptr;
     uint32_t* d_ne = nullptr;
+    uint64_t* d_nbr = nullptr;             // [instance][NBR_STRIDE] neighbour masks
     // per-run buffers
     uint32_t* d_circ_inst = nullptr;       // global circuit -> instance (class-major order)
     uint64_t* d_user = nullptr;            // run position -> caller's circuit index
@@ -1374,6 +1416,7 @@ int launch_class(rq_qaoa_batch* b, QClass& K, uint64_t ncirc, uint64_t circ0, vo
     a.edges = b->d_edges;
     a.eoff = b->d_eoff;
     a.ne = b->d_ne;
+    a.nbr = b->d_nbr;
     a.rot = (const T*)b->d_rx;
     a.nparam = b->p;
     a.ph = (const T*)b->d_ph;
@@ -1418,6 +1461,7 @@ int adjoint_class(rq_qaoa_batch* b, QClass& K, uint64_t ncirc, uint64_t circ0, v
     a.edges = b->d_edges;
     a.eoff = b->d_eoff;
     a.ne = b->d_ne;
+    a.nbr = b->d_nbr;
     a.rot = (const T*)b->d_rx;
     a.nparam = b->p;
     a.ph = (const T*)b->d_ph;
@@ -1614,6 +1658,15 @@ int rq_qaoa_batch_create(uint32_t ninst, const uint32_t* num_nodes, const uint32
     RQ_CUDA(cudaMemcpy(b->d_eoff, eoff.data(), (ninst + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice));
     RQ_CUDA(cudaMalloc((void**)&b->d_ne, std::max<uint32_t>(1, ninst) * sizeof(uint32_t)));
     if (ninst) RQ_CUDA(cudaMemcpy(b->d_ne, b->ne_of.data(), ninst * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    std::vector<uint64_t> nbr((size_t)std::max<uint32_t>(1, ninst) * NBR_STRIDE, 0);
+    for (uint32_t k = 0; k < ninst; ++k)
+        for (uint32_t e = eoff[k]; e < eoff[k + 1]; ++e) {
+            const uint32_t u = ed[2 * (size_t)e], v = ed[2 * (size_t)e + 1];
+            nbr[(size_t)k * NBR_STRIDE + u] |= 1ull << v;
+            nbr[(size_t)k * NBR_STRIDE + v] |= 1ull << u;
+        }
+    RQ_CUDA(cudaMalloc((void**)&b->d_nbr, nbr.size() * sizeof(uint64_t)));
+    RQ_CUDA(cudaMemcpy(b->d_nbr, nbr.data(), nbr.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
     // the copies above (from pageable memory) may return before their DMA lands, and the
     // batch's stream is not ordered after them: wait here, once, before any run
     RQ_CUDA(cudaDeviceSynchronize());
@@ -1629,7 +1682,7 @@ int rq_qaoa_batch_destroy(rq_qaoa_batch* b) {
         if (K.prog) cudaFree(K.prog);
         if (K.aprog) cudaFree(K.aprog);
     }
-    void* ptrs[] = {b->d_edges, b->d_eoff, b->d_ne, b->d_circ_inst, b->d_user, b->d_ang, b->d_rx, b->d_ph, b->d_energy,
+    void* ptrs[] = {b->d_edges, b->d_eoff, b->d_ne, b->d_nbr, b->d_circ_inst, b->d_user, b->d_ang, b->d_rx, b->d_ph, b->d_energy,
                     b->d_best_bits, b->d_best_cut, b->d_states, b->d_epart, b->d_tree, b->d_lam, b->d_gpart,
                     b->d_grad};
     for (void* q : ptrs) if (q) cudaFree(q);

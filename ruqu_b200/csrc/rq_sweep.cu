@@ -1791,17 +1791,11 @@ static int launch_tc16(rq_state* s, const rq_plan* P, const PhaseDesc* ph, const
     const int by_regs = 65536 / (128 * (int)threads);
     const int by_smem = (int)((228u * 1024u) / (smem_max + 1024u + 128u));
     const int by_tmem = (int)(512u / (128u * (threads / 128u)));
-    // RUQU_TC16_ONE_CTA=1: one CTA per SM (the shared-memory request padded so that a second
-    // cannot fit), for measuring how much the second CTA of an SM hides
-    static const bool one_cta = [] {
-        const char* e = std::getenv("RUQU_TC16_ONE_CTA");
-        return e && e[0] == '1';
-    }();
-    const int per_sm = one_cta ? 1 : std::min(by_regs, std::min(by_smem, by_tmem));
+    const int per_sm = std::min(by_regs, std::min(by_smem, by_tmem));
     if (per_sm < 1) return fail(RQ_ERR_CUDA, "FP16 tensor-core sweep kernel does not fit on an SM");
     const unsigned grid = (unsigned)std::min<uint64_t>(P->ntiles, (uint64_t)per_sm * rq::num_sms(s->device));
     for (const auto& d : P->descs) {
-        const size_t smem = one_cta ? std::max<size_t>(smem_of(d), 120u * 1024u) : smem_of(d);
+        const size_t smem = smem_of(d);
         RQ_CUDA(cudaFuncSetAttribute(k_sweep_tc16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_sweep_tc16<<<grid, threads, smem, s->stream>>>((float2*)s->amps, d, ph, op, img, P->ntiles);
         RQ_CUDA(cudaGetLastError());
