@@ -12,9 +12,9 @@
 //  * H^n|0> is synthesised by the first sweep (uniform amplitude 2^(-n/2));
 //  * the product of all Rzz of a layer is one diagonal phase
 //    exp(-i*gamma*(|E| - 2 cut(x))) (unit weights): each thread derives
-//    cut(x) for its 2^RB register amplitudes from the graph's edge list
-//    (edges between non-register bits are constant per thread, edges touching
-//    a register slot add per-slot counts) and looks the phase up in a table;
+//    cut(x) for its 2^RB register amplitudes from the graph's neighbour masks
+//    (the cut of its fixed bits, one count change per register slot, and the
+//    edges between slots) and looks the phase up in a table;
 //  * the last sweep reduces <C> = sum_x |a_x|^2 cut(x) in FP64 (the same
 //    quantity as the per-edge sum of qaoa.rs:194-200) into per-tile partials;
 //  * optional shots: FP64 prefix trees per circuit, then every shot walks its
@@ -76,70 +76,8 @@ struct QArgs {
     uint32_t gwidth;               // adjoint sweeps: gradient entries per circuit (2p for QAOA, P for VQE)
 };
 
-// cut(x) for the register amplitudes of one thread: x = U | deposit(i).
-// Edges with no endpoint on a register slot contribute a per-thread constant;
-// an edge from slot s to a non-slot vertex w contributes bit_s(i) xor bit_w(U),
-// i.e. a0[s] edges count when bit_s(i) = 1 and a1[s] edges when it is 0;
-// edges between two slots (at most 10 in a simple graph) are listed.
-template <int RB>
-struct CutPlan {
-    int base;          // cut of the register index 0 (all slot bits 0)
-    int delta[RB];     // change of the cut when slot s flips to 1 (slot-slot edges excluded)
-    uint64_t ss;       // 6 bits per slot-slot edge: s | t << 3
-    int nss;
-};
-
-template <int RB>
-__device__ __forceinline__ void cut_plan(CutPlan<RB>& cp, const uint8_t* __restrict__ e, uint32_t ne, uint64_t U,
-                                         uint64_t slotmask) {
-    int cu = 0;
-    uint64_t pk = 0;   // 6-bit counters, field 2s+b: edges from slot s to a non-slot vertex whose bit is b
-    cp.ss = 0;
-    cp.nss = 0;
-    for (uint32_t k = 0; k < ne; ++k) {
-        const uint32_t u = e[2 * k], v = e[2 * k + 1];
-        const bool su = (slotmask >> u) & 1ull, sv = (slotmask >> v) & 1ull;
-        const int bu = (int)((U >> u) & 1ull), bv = (int)((U >> v) & 1ull);
-        if (!su && !sv) {
-            cu += bu ^ bv;
-        } else if (su && !sv) {
-            const int s = __popcll(slotmask & ((1ull << u) - 1));
-            pk += 1ull << (6 * (2 * s + bv));
-        } else if (!su && sv) {
-            const int s = __popcll(slotmask & ((1ull << v) - 1));
-            pk += 1ull << (6 * (2 * s + bu));
-        } else if (cp.nss < 10) {
-            const uint64_t s = (uint64_t)__popcll(slotmask & ((1ull << u) - 1));
-            const uint64_t t = (uint64_t)__popcll(slotmask & ((1ull << v) - 1));
-            cp.ss |= (s | (t << 3)) << (6 * cp.nss);
-            cp.nss++;
-        }
-    }
-    // slot bit 0: an edge to a non-slot vertex w counts iff bit_w = 1; slot bit 1: iff bit_w = 0
-    cp.base = cu;
-#pragma unroll
-    for (int s = 0; s < RB; ++s) {
-        const int n0 = (int)((pk >> (12 * s)) & 63), n1 = (int)((pk >> (12 * s + 6)) & 63);
-        cp.base += n1;
-        cp.delta[s] = n0 - n1;
-    }
-}
-
-template <int RB>
-__device__ __forceinline__ int cut_of(const CutPlan<RB>& cp, int i) {
-    int c = cp.base;
-#pragma unroll
-    for (int s = 0; s < RB; ++s)
-        if ((i >> s) & 1) c += cp.delta[s];
-    uint64_t ss = cp.ss;
-    for (int k = 0; k < cp.nss; ++k, ss >>= 6) {
-        const int s = (int)(ss & 7), t = (int)((ss >> 3) & 7);
-        c += ((i >> s) ^ (i >> t)) & 1;
-    }
-    return c;
-}
-
-// The same cut counts from neighbour masks N(v), for U with every slot bit 0:
+// cut(x) for the register amplitudes of one thread, x = U | deposit(i), from the graph's
+// neighbour masks N(v), for U with every slot bit 0:
 //   cut(U)             = sum over vertices v with U_v = 1 of popc(N(v) & ~U)
 //   flipping slot s    : delta_s = deg(s) - 2 popc(N(s) & U)   (slot neighbours count as 0)
 //   slots s, t both 1  : their shared edge was counted twice by delta_s + delta_t, -2 each
@@ -342,9 +280,6 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
                     U |= 1ull << ph.tbit_global[b];
                 }
             const uint32_t sb = swzb<T>(ebase);
-            uint64_t slotmask = 0;
-#pragma unroll
-            for (int s = 0; s < RB; ++s) slotmask |= 1ull << ph.slot_global[s];
             // register i sits at sb ^ (XOR of S[k] over the set bits k of i): visited in
             // Gray-code order, each address is one XOR from the previous one
             uint32_t S[RB];
@@ -571,11 +506,11 @@ __global__ void __launch_bounds__(512, 1) k_batch_adjoint(const SweepDesc d, con
         const uint64_t gcirc = a.circ0 + circ;
         V* psi = a.amps + circ * nstate;
         V* lam = a.lam + circ * nstate;
-        const uint8_t* edges = nullptr;
+        const uint64_t* nb = nullptr;   // the instance's neighbour masks
         uint32_t ne = 0;
         if (a.circ_inst) {
             const uint32_t inst = a.circ_inst[gcirc];
-            edges = a.edges + 2 * (size_t)a.eoff[inst];
+            nb = a.nbr + (size_t)inst * NBR_STRIDE;
             ne = a.ne[inst];
         }
         uint64_t base = 0;
@@ -620,24 +555,35 @@ __global__ void __launch_bounds__(512, 1) k_batch_adjoint(const SweepDesc d, con
                     U |= 1ull << ph.tbit_global[b];
                 }
             const uint32_t sb = swzb<T>(ebase);
-            uint64_t slotmask = 0;
+            // register i sits at sb ^ (XOR of S[k] over the set bits k of i): Gray-code order
+            uint32_t S[RB];
 #pragma unroll
-            for (int s = 0; s < RB; ++s) slotmask |= 1ull << ph.slot_global[s];
+            for (int k = 0; k < RB; ++k) S[k] = ph.slut[1 << k];
             V rp[NR], rl[NR];
+            {
+                uint32_t ad = sb;
 #pragma unroll
-            for (int i = 0; i < NR; ++i) rp[i] = smp[sb ^ ph.slut[i]];
+                for (int g = 0; g < NR; ++g) {
+                    if (g) ad ^= S[gray_bit(g)];
+                    rp[g ^ (g >> 1)] = smp[ad];
+                }
+            }
             if (initl && p == d.phase_begin) {
-                CutPlan<RB> cp;
-                cut_plan<RB>(cp, edges, ne, U, slotmask);
+                CutNb<RB> cp;
+                cut_plan_nb<RB>(cp, nb, U, ph.slot_global);
 #pragma unroll
                 for (int i = 0; i < NR; ++i) {
-                    const T c = (T)cut_of<RB>(cp, i);
+                    const T c = (T)cut_nb<RB>(cp, i);
                     rl[i].x = c * rp[i].x;
                     rl[i].y = c * rp[i].y;
                 }
             } else {
+                uint32_t ad = sb;
 #pragma unroll
-                for (int i = 0; i < NR; ++i) rl[i] = sml[sb ^ ph.slut[i]];
+                for (int g = 0; g < NR; ++g) {
+                    if (g) ad ^= S[gray_bit(g)];
+                    rl[g ^ (g >> 1)] = sml[ad];
+                }
             }
             for (uint32_t o = ph.op_begin; o < ph.op_end; ++o) {
                 const SwOp op = ops[o];
@@ -647,13 +593,13 @@ __global__ void __launch_bounds__(512, 1) k_batch_adjoint(const SweepDesc d, con
                     dispatch_rx<NR>(op.k0, rp, r[0], -r[1]);
                     dispatch_rx<NR>(op.k0, rl, r[0], -r[1]);
                 } else if (op.type == OP_CPH) {
-                    CutPlan<RB> cp;
-                    cut_plan<RB>(cp, edges, ne, U, slotmask);
+                    CutNb<RB> cp;
+                    cut_plan_nb<RB>(cp, nb, U, ph.slot_global);
                     const T* tab = a.ph + ((size_t)gcirc * a.p + op.param) * a.phs * 2;
                     double acc = 0.0;
 #pragma unroll
                     for (int i = 0; i < NR; ++i) {
-                        const int c = cut_of<RB>(cp, i);
+                        const int c = cut_nb<RB>(cp, i);
                         const T gdiag = (T)((int)ne - 2 * c);
                         acc += (double)(gdiag * (rl[i].x * rp[i].y - rl[i].y * rp[i].x));
                         rp[i] = cmulv(rp[i], tab[2 * c], -tab[2 * c + 1]);
@@ -682,10 +628,14 @@ __global__ void __launch_bounds__(512, 1) k_batch_adjoint(const SweepDesc d, con
                     }
                 }
             }
+            {
+                uint32_t ad = sb;
 #pragma unroll
-            for (int i = 0; i < NR; ++i) {
-                smp[sb ^ ph.slut[i]] = rp[i];
-                sml[sb ^ ph.slut[i]] = rl[i];
+                for (int g = 0; g < NR; ++g) {
+                    if (g) ad ^= S[gray_bit(g)];
+                    smp[ad] = rp[g ^ (g >> 1)];
+                    sml[ad] = rl[g ^ (g >> 1)];
+                }
             }
             __syncthreads();
         }
