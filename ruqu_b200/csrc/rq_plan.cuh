@@ -478,17 +478,21 @@ inline Sweep take_sweep(const std::vector<PGate>& gates, std::vector<char>& take
     return sw;
 }
 
-// Tensor-core sweep cost model: a launch costs about SWEEP_COST + PHASE_COST x its phases
-// (least-squares fit of the per-launch times of a 30-qubit f32 circuit's 14 sweeps with
-// 1-14 phases: 1.79 ms + 1.91 ms per phase, residuals < 0.8 ms; both terms scale with
-// the state size, so only their ratio matters here).
-constexpr double SWEEP_COST = 1.79, PHASE_COST = 1.91;
+// Tensor-core sweep cost model: a launch costs about sweep + phase x its phases.  Least-
+// squares fits of the per-launch times of the 30-qubit f32 benchmark circuit (launch lists
+// of one step; both terms scale with the state size, so only their ratio matters here):
+//   3xTF32 sweeps (two MMA round trips per phase): 1.79 ms + 1.91 ms per phase;
+//   FP16-split sweeps (one round trip):             3.15 ms + 1.05 ms per phase.
+struct SweepCost {
+    double sweep, phase;
+};
+constexpr SweepCost COST_TF32{1.79, 1.91}, COST_F16{3.15, 1.05};
 
-inline double plan_cost(std::vector<Sweep> sweeps, uint32_t n, uint32_t m, uint32_t rb) {
+inline double plan_cost(std::vector<Sweep> sweeps, uint32_t n, uint32_t m, uint32_t rb, SweepCost k = COST_TF32) {
     double c = 0.0;
     for (auto& sw : sweeps) {
         for (uint32_t q = 0; q < n && (uint32_t)__builtin_popcountll(sw.L) < m; ++q) sw.L |= 1ull << q;
-        c += SWEEP_COST + PHASE_COST * (double)plan_phases(sw, rb, true).size();
+        c += k.sweep + k.phase * (double)plan_phases(sw, rb, true).size();
     }
     return c;
 }
@@ -498,7 +502,7 @@ inline double plan_cost(std::vector<Sweep> sweeps, uint32_t n, uint32_t m, uint3
 // reference plan, so a set that runs many gates but needs many phases can lose to one
 // that runs slightly fewer in fewer phases.
 inline std::vector<Sweep> plan_sweeps_costed(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c,
-                                             uint32_t rb, double rate) {
+                                             uint32_t rb, double rate, SweepCost k = COST_TF32) {
     std::vector<Sweep> out;
     std::vector<char> taken(gates.size(), 0);
     size_t first = 0;
@@ -512,7 +516,7 @@ inline std::vector<Sweep> plan_sweeps_costed(const std::vector<PGate>& gates, ui
             if (sw.ops.empty()) continue;
             int got = 0;
             for (size_t k = first; k < gates.size(); ++k) got += (t2[k] && !taken[k]) ? 1 : 0;
-            const double score = rate * got - (SWEEP_COST + PHASE_COST * (double)plan_phases(sw, rb, true).size());
+            const double score = rate * got - (k.sweep + k.phase * (double)plan_phases(sw, rb, true).size());
             if (score > best) {
                 best = score;
                 bestL = L;
@@ -534,15 +538,15 @@ inline std::vector<Sweep> plan_sweeps_costed(const std::vector<PGate>& gates, ui
 // keeping the plan of least modelled cost.  A gate qubit that stays outside a sweep's
 // local set is uniform over each tile, for CUDA-core and tensor-core plans alike.
 inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c,
-                                      bool all_slots = false) {
+                                      bool all_slots = false, SweepCost k = COST_TF32) {
     auto a = plan_sweeps_first_come(gates, n, m, c);
     auto b = plan_sweeps_lookahead(gates, n, m, c);
     auto best = b.size() < a.size() ? b : a;
     if (!all_slots || gates.empty()) return best;
     const uint32_t rb = 5;
-    const double cost_best = plan_cost(best, n, m, rb);
-    auto d = plan_sweeps_costed(gates, n, m, c, rb, cost_best / (double)gates.size());
-    if (!d.empty() && plan_cost(d, n, m, rb) < cost_best) return d;
+    const double cost_best = plan_cost(best, n, m, rb, k);
+    auto d = plan_sweeps_costed(gates, n, m, c, rb, cost_best / (double)gates.size(), k);
+    if (!d.empty() && plan_cost(d, n, m, rb, k) < cost_best) return d;
     return best;
 }
 

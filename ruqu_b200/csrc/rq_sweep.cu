@@ -1476,7 +1476,7 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
         return fail(RQ_ERR_CIRCUIT, "circuit error: only unitary gates can be planned");
     }
     const bool tcp = tc_passes > 0;
-    auto sweeps = plan_sweeps(pg, nq, m, c, tcp);
+    auto sweeps = plan_sweeps(pg, nq, m, c, tcp, tc_passes == TC_F16 ? COST_F16 : COST_TF32);
     for (const auto& sw : sweeps) {   // the structure, before build_program pads the local sets
         P->sweep_L.push_back(sw.L);
         P->sig.push_back(sweep_signature(sw));

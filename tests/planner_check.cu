@@ -107,11 +107,12 @@ int main() {
         for (auto& v : want) v = Cx(nd(r), nd(r));
         const std::vector<Cx> start = want;
         for (const auto& g : pg) apply(want, g);
-        for (int sp = 0; sp < 5; ++sp) {
+        for (int sp = 0; sp < 6; ++sp) {
             std::vector<Sweep> sweeps = sp == 0 ? plan_sweeps_first_come(pg, n, m, c)
                                       : sp == 1 ? plan_sweeps_lookahead(pg, n, m, c)
                                       : sp == 2 ? plan_sweeps(pg, n, m, c)
                                       : sp == 3 ? plan_sweeps(pg, n, m, c, true)
+                                      : sp == 4 ? plan_sweeps(pg, n, m, c, true, COST_F16)
                                                 : plan_sweeps_costed(pg, n, m, c, 5, 0.05);
             if (sweeps.empty() && !pg.empty()) return fail("no sweep plan", trial);
             for (int pp = 0; pp < 3; ++pp)
