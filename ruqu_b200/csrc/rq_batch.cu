@@ -228,7 +228,10 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
         for (uint32_t b = d.c; b < d.m; ++b)
             if ((x >> b) & 1ull) dep_tid |= 1ull << d.local_global[b];
     }
-    const uint32_t stid = swzb<T>(tid * EPV);   // swz(e) = stid ^ sgj[j] (the swizzle is XOR-linear)
+    // complex f32 programs use the layout of swz16 (retable_f16: every local bit has its own
+    // bank pattern, warp lanes span the banks); complex f64 programs the row swizzle swzb
+    constexpr bool F16L = std::is_same<T, float>::value;
+    const uint32_t stid = F16L ? swz16(tid * EPV) : swzb<T>(tid * EPV);   // swz(e) = stid ^ sgj[j] (XOR-linear)
     const uint64_t nwork = a.ncirc * a.ntiles;
     const uint64_t nstate = 1ull << d.n;
     // the sweep's phase descriptors in shared memory, after the tile
@@ -279,7 +282,7 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
                     ebase |= 1u << ph.tbit_local[b];
                     U |= 1ull << ph.tbit_global[b];
                 }
-            const uint32_t sb = swzb<T>(ebase);
+            const uint32_t sb = F16L ? swz16(ebase) : swzb<T>(ebase);
             // register i sits at sb ^ (XOR of S[k] over the set bits k of i): visited in
             // Gray-code order, each address is one XOR from the previous one
             uint32_t S[RB];
@@ -1551,6 +1554,7 @@ int rq_qaoa_batch_create(uint32_t ninst, const uint32_t* num_nodes, const uint32
         std::vector<SwOp> ops;
         std::vector<double> mats;
         build_program(sweeps, K.n, K.m, K.c, rb, precision == RQ_F32 ? 2 : 1, K.descs, phases, ops, mats);
+        if (precision == RQ_F32) retable_f16(K.descs, phases, rb);   // the conflict-free layout (k_batch_sweep<float>)
         K.smem += max_phases(K.descs) * sizeof(PhaseDesc);   // the phase descriptors after the tile
         K.descs.front().flags |= SWEEP_INIT_UNIFORM;
         K.descs.back().flags |= SWEEP_ENERGY;
@@ -2560,6 +2564,7 @@ int rq_vqe_batch_create(uint32_t num_qubits, uint32_t depth, const double* coeff
     std::vector<SwOp> opsv;
     std::vector<double> mats;
     build_program(sweeps, num_qubits, b->m, c, rb, precision == RQ_F32 ? 2 : 1, b->descs, phases, opsv, mats);
+    if (precision == RQ_F32) retable_f16(b->descs, phases, rb);   // the conflict-free layout (k_batch_sweep<float>)
     b->smem += max_phases(b->descs) * sizeof(PhaseDesc);   // the phase descriptors after the tile
     b->descs.front().flags |= SWEEP_INIT_ZERO;
     b->off_ops = (phases.size() * sizeof(PhaseDesc) + 255) & ~size_t(255);
