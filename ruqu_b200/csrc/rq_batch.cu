@@ -1013,7 +1013,6 @@ __global__ void __launch_bounds__(512, 1) k_vqe_energy_tiles(const typename C2<T
                 __syncthreads();
                 src = par;
             }
-            const bool r_is_lo = r < rp;
             for (uint32_t g = gofs[t] + warp; g < gofs[t + 1]; g += nw) {
                 const VGroup G = groups[g];
                 switch (G.nt) {

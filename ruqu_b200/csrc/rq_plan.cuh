@@ -502,7 +502,7 @@ inline double plan_cost(std::vector<Sweep> sweeps, uint32_t n, uint32_t m, uint3
 // reference plan, so a set that runs many gates but needs many phases can lose to one
 // that runs slightly fewer in fewer phases.
 inline std::vector<Sweep> plan_sweeps_costed(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c,
-                                             uint32_t rb, double rate, SweepCost k = COST_TF32) {
+                                             uint32_t rb, double rate, SweepCost cost = COST_TF32) {
     std::vector<Sweep> out;
     std::vector<char> taken(gates.size(), 0);
     size_t first = 0;
@@ -516,7 +516,7 @@ inline std::vector<Sweep> plan_sweeps_costed(const std::vector<PGate>& gates, ui
             if (sw.ops.empty()) continue;
             int got = 0;
             for (size_t k = first; k < gates.size(); ++k) got += (t2[k] && !taken[k]) ? 1 : 0;
-            const double score = rate * got - (k.sweep + k.phase * (double)plan_phases(sw, rb, true).size());
+            const double score = rate * got - (cost.sweep + cost.phase * (double)plan_phases(sw, rb, true).size());
             if (score > best) {
                 best = score;
                 bestL = L;
