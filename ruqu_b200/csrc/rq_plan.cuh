@@ -617,20 +617,21 @@ inline uint32_t swz_host(uint32_t e, uint32_t cb) {
     return e ^ (f & ((1u << cb) - 1));
 }
 
-// Shared-memory layout of the FP16 tensor-core sweeps (complex f32, at most 13 local bits):
+// Shared-memory layout of the FP16 tensor-core sweeps (complex f32, at most 14 local bits):
 // element e is stored at swz16(e) = e ^ g(e), where local bits 0..3 address the 16 8-byte
 // units of a 128-byte row and every higher local bit b flips the unit index by its own
-// 4-bit pattern SWZ16_ROW[b - 4].  All 13 patterns (with 1, 2, 4, 8 for bits 0..3) are
-// distinct and non-zero, so any 8 local bits span all 16 units: a phase can always give its
+// 4-bit pattern SWZ16_ROW[b - 4].  All 14 patterns (with 1, 2, 4, 8 for bits 0..3) are
+// distinct and non-zero, so any 8 local bits span all 16 units (8 distinct non-zero vectors
+// cannot lie in a 3-dimensional subspace, which holds only 7): a phase can always give its
 // warp lanes 5 thread bits whose patterns span the units, and then the 32 8-byte accesses of
 // a warp fall on every bank exactly twice (two wavefronts, no conflict), whichever 5 local
 // bits the phase keeps in registers.
-// SWZ16_ROW nibble k = the pattern of local bit 4 + k: 3, 5, 6, 9, 10, 12, 7, 11, 13
-constexpr uint64_t SWZ16_ROW = 0xDB7CA9653ull;
+// SWZ16_ROW nibble k = the pattern of local bit 4 + k: 3, 5, 6, 9, 10, 12, 7, 11, 13, 14
+constexpr uint64_t SWZ16_ROW = 0xEDB7CA9653ull;
 
 __host__ __device__ inline uint32_t swz16(uint32_t e) {
     uint32_t g = 0;
-    for (int b = 0; b < 9; ++b)
+    for (int b = 0; b < 10; ++b)
         if ((e >> (4 + b)) & 1u) g ^= (uint32_t)(SWZ16_ROW >> (4 * b)) & 15u;
     return e ^ g;
 }

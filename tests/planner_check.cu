@@ -169,12 +169,15 @@ int main() {
     // tile exactly once, and the five lane bits of every phase span all 16 bank units (the
     // 32 8-byte accesses of a warp hit each bank exactly twice).
     {
-        std::vector<int> hit(1u << 13, 0);
-        for (uint32_t e = 0; e < (1u << 13); ++e) ++hit[swz16(e)];
+        std::vector<int> hit(1u << 14, 0);
+        for (uint32_t e = 0; e < (1u << 14); ++e) ++hit[swz16(e)];
         for (int h : hit)
             if (h != 1) return fail("swz16 is not a bijection", -1);
-        for (int t2 = 0; t2 < 40; ++t2) {
-            const uint32_t n = 16 + (uint32_t)(t2 % 5), m = 13, c = 5, rb = 5;
+        for (int t2 = 0; t2 < 60; ++t2) {
+            // 13 local bits (256-thread tiles) and 14 (512 threads, the ninth thread bit's
+            // offset computed from tbit_local[8] as the kernel does)
+            const uint32_t m = t2 % 3 == 2 ? 14 : 13, n = 16 + (uint32_t)(t2 % 5), c = 5, rb = 5;
+            const uint32_t tb = m - rb;
             const auto circ = random_circuit(n, r, t2 % 2 == 0);
             std::vector<PGate> pg;
             if (!to_pgates(circ.data(), circ.size(), pg)) return fail("to_pgates", t2);
@@ -193,7 +196,7 @@ int main() {
                     set_a |= 1ull << ph.tbit_local[b];
                     set_b |= 1ull << before[pi].tbit_local[b];
                 }
-                if (set_a != set_b || ph.nt != 8) return fail("retable changed the thread bits", t2);
+                if (set_a != set_b || ph.nt != tb) return fail("retable changed the thread bits", t2);
                 uint32_t basis[4] = {0, 0, 0, 0};
                 int rank = 0;
                 for (uint32_t b = 0; b < 5; ++b) {
@@ -206,10 +209,11 @@ int main() {
                 }
                 if (rank != 4) return fail("lane bits do not span the banks", t2);
                 std::vector<int> cover(1u << m, 0);
-                for (uint32_t tid = 0; tid < 256; ++tid) {
+                for (uint32_t tid = 0; tid < (1u << tb); ++tid) {
                     uint32_t sb = 0;
                     for (uint32_t b = 0; b < 8; ++b)
                         if ((tid >> b) & 1u) sb ^= ph.tsw[b];
+                    if (tb > 8 && ((tid >> 8) & 1u)) sb ^= swz16(1u << ph.tbit_local[8]);
                     for (uint32_t i = 0; i < 32; ++i) ++cover[sb ^ ph.slut[i]];
                 }
                 for (int v : cover)
@@ -217,7 +221,7 @@ int main() {
             }
             for (const auto& d : descs)
                 for (uint32_t j = 0; j < 16; ++j)
-                    if (d.sgj[j] != swz16(j * (1u << 8) * 2u)) return fail("sgj not under swz16", t2);
+                    if (d.sgj[j] != swz16(j * (1u << tb) * 2u)) return fail("sgj not under swz16", t2);
         }
     }
     std::printf("ok %d plans\n", trials);
