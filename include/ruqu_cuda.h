@@ -262,6 +262,14 @@ RQ_API int rq_plan_create(const rq_state* s, const rq_gate* gates, uint64_t n,
                           int32_t mode, rq_plan** out);
 RQ_API int rq_plan_execute(rq_state* s, const rq_plan* p);
 
+/* As rq_plan_create with the tile size of a tensor-core sweep chosen by the caller (the
+ * autotuner of RQ_EXEC_AUTO picks among these itself): local_qubits 12 or 13 for
+ * RQ_EXEC_SWEEP_TC / _TC_FAST, 12, 13 or 14 for RQ_EXEC_SWEEP_TC16 (14: one 512-thread CTA
+ * per SM, fewer sweeps), complex f32 states only; 0 = the default.  No counterpart in the
+ * reference. */
+RQ_API int rq_plan_create_tiled(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode,
+                                uint32_t local_qubits, rq_plan** out);
+
 /* New gate values for a prepared plan: `gates` must have the plan's gate kinds and
  * qubits (barriers aside) and may change any angle or matrix.  No counterpart in the
  * reference (whose drivers rebuild the circuit for every evaluation, qaoa.rs:232 and

@@ -54,6 +54,7 @@ SIGNATURES = {
     "rq_device_set": (C.c_int, [_i32]),
     "rq_device_count": (C.c_int, [_P(_i32)]),
     "rq_plan_create": (C.c_int, [_vp, _P(RqGate), _u64, _i32, _P(_vp)]),
+    "rq_plan_create_tiled": (C.c_int, [_vp, C.c_void_p, _u64, _i32, _u32, _P(_vp)]),
     "rq_plan_execute": (C.c_int, [_vp, _vp]),
     "rq_plan_update": (C.c_int, [_vp, _vp, _P(RqGate), _u64]),
     "rq_plan_get_stats": (C.c_int, [_vp, _P(RqPlanStats)]),

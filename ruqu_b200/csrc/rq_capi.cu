@@ -368,6 +368,24 @@ int rq_plan_create(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t 
     return rq::plan_build(s, gates, n, use_sweep ? RQ_EXEC_SWEEP : RQ_EXEC_PER_GATE, out, passes, 2, m);
 }
 
+int rq_plan_create_tiled(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode, uint32_t local_qubits,
+                         rq_plan** out) {
+    if (local_qubits == 0) return rq_plan_create(s, gates, n, mode, out);
+    if (!s || !out || (!gates && n)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");
+    const uint32_t hi = mode == RQ_EXEC_SWEEP_TC16 ? 14u : 13u;
+    if ((mode != RQ_EXEC_SWEEP_TC && mode != RQ_EXEC_SWEEP_TC_FAST && mode != RQ_EXEC_SWEEP_TC16) ||
+        s->prec != RQ_F32 || local_qubits < 12 || local_qubits > hi || s->nq < local_qubits)
+        return rq::fail(RQ_ERR_INVALID_ARGUMENT, "tile sizes: 12-13 local qubits for the tensor-core sweeps, 12-14 for "
+                                                 "RQ_EXEC_SWEEP_TC16, complex f32 states of at least that many qubits");
+    for (uint64_t k = 0; k < n; ++k) {
+        RQ_TRY(validate_gate(s, gates[k]));
+        if (gates[k].kind == RQ_GATE_MEASURE || gates[k].kind == RQ_GATE_RESET)
+            return rq::fail(RQ_ERR_CIRCUIT, "circuit error: a plan holds unitary gates only");
+    }
+    RQ_TRY(set_device(s));
+    return rq::plan_build(s, gates, n, RQ_EXEC_SWEEP, out, rq::tc_passes_of(mode), 2, local_qubits);
+}
+
 int rq_state_apply_kraus(rq_state* s, uint32_t q, const double* kraus, uint32_t nk, int32_t* chosen,
                          double* probability) {
     if (!s || (!kraus && nk)) return rq::fail(RQ_ERR_INVALID_ARGUMENT, "null pointer");

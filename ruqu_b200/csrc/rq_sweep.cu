@@ -958,7 +958,10 @@ __device__ __forceinline__ bool wait_sleep(uint64_t* bar, uint32_t parity, uint3
 
 }  // namespace tc16
 
-__global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps, const SweepDesc d,
+// NTHR = 256: tiles of up to 13 local qubits, two CTAs per SM; NTHR = 512: 14 local qubits,
+// one CTA (four 128-row halves, all 512 tensor-memory columns) per SM.
+template <int NTHR>
+__global__ void __launch_bounds__(NTHR, 512 / NTHR) k_sweep_tc16(float2* __restrict__ amps, const SweepDesc d,
                                                      const PhaseDesc* __restrict__ phases,
                                                      const SwOp* __restrict__ ops,
                                                      const uint32_t* __restrict__ images, uint64_t ntiles) {
@@ -972,10 +975,10 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
     const uint32_t nph = d.phase_end - d.phase_begin;
     const uint32_t op0 = phases[d.phase_begin].op_begin, nops = phases[d.phase_end - 1].op_end - op0;
     SwOp* sop = reinterpret_cast<SwOp*>(sph + nph);
-    __shared__ __align__(8) uint64_t mbar[2], ibar[2];
+    __shared__ __align__(8) uint64_t mbar[NTHR / 128], ibar[2];
     __shared__ uint32_t tmem_base;
-    __shared__ float wmax[8], wsum[8], wsum2[8];
-    __shared__ int half_failed[2];
+    __shared__ float wmax[NTHR / 32], wsum[NTHR / 32], wsum2[NTHR / 32];
+    __shared__ int half_failed[NTHR / 128];
 
     const uint32_t tid = threadIdx.x;
     const uint32_t T_ = blockDim.x;
@@ -991,11 +994,12 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     if (tid == 0) {
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < NTHR / 128; ++k) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc::smem_u32(&mbar[k])), "r"(1u) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc::smem_u32(&ibar[k])), "r"(1u) : "memory");
             half_failed[k] = 0;
         }
+        for (int k = 0; k < 2; ++k)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc::smem_u32(&ibar[k])), "r"(1u) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1087,6 +1091,7 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc16(float2* __restrict__ amps
 #pragma unroll
                 for (uint32_t b = 0; b < 8; ++b)
                     if ((tid >> b) & 1u) sb ^= (tw[b >> 1] >> (16 * (b & 1u))) & 0xFFFFu;
+                if (NTHR > 256 && ((tid >> 8) & 1u)) sb ^= swz16(1u << ph.tbit_local[8]);   // a ninth thread bit
             }
             // register i sits at sb ^ (XOR of S[k] over the set bits k of i); visiting the
             // registers in Gray-code order makes each address one XOR from the previous one
@@ -1463,9 +1468,12 @@ int plan_build(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode
         return RQ_OK;
     }
     P->mode = RQ_EXEC_SWEEP;
-    const uint32_t m = m_override ? std::min(nq, m_override) : sweep_local_qubits(nq, s->prec);
-    if (s->prec != RQ_F32 || (m != 12 && m != 13)) tc_passes = 0;   // the tensor-core sweep's tile shapes
+    uint32_t m = m_override ? std::min(nq, m_override) : sweep_local_qubits(nq, s->prec);
     if (tc_passes == TC_F16 && !all_unitary(gates, n)) tc_passes = 3;
+    // the tensor-core sweeps' tile shapes: 12 or 13 local qubits, and 14 for the FP16 sweep only
+    // (other 14-qubit requests take 13)
+    if (m == 14 && tc_passes != TC_F16) m = 13;
+    if (s->prec != RQ_F32 || (m != 12 && m != 13 && !(m == 14 && tc_passes == TC_F16))) tc_passes = 0;
     const uint32_t c = std::min<uint32_t>(m, 5);
     std::vector<PGate> pg;
     std::vector<rq_gate> filtered;
@@ -1723,8 +1731,9 @@ int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes
             return RQ_OK;
         }
     }
-    // candidates: CUDA-core sweep; 3xTF32 tensor-core sweep with the default tile and with one
-    // local qubit fewer (twice the CTAs per SM, more sweeps)
+    // candidates: CUDA-core sweep; 3xTF32 and FP16-split tensor-core sweeps with the default
+    // tile and with one local qubit fewer (twice the CTAs per SM, more sweeps); the FP16 sweep
+    // also with one local qubit more (one 512-thread CTA per SM, fewer sweeps)
     struct Cand {
         int passes;
         uint32_t m;
@@ -1735,6 +1744,7 @@ int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes
     if (m == 13 && s->nq > 13) {
         cands.push_back({3, 12, nullptr, 0.f});
         cands.push_back({TC_F16, 12, nullptr, 0.f});
+        if (s->nq > 14) cands.push_back({TC_F16, 14, nullptr, 0.f});
     }
     for (auto& c : cands)
         if (plan_build(s, gates, n, RQ_EXEC_SWEEP, &c.plan, c.passes, 2, c.m) != RQ_OK) {
@@ -1796,8 +1806,9 @@ static int launch_tc16(rq_state* s, const rq_plan* P, const PhaseDesc* ph, const
     const unsigned grid = (unsigned)std::min<uint64_t>(P->ntiles, (uint64_t)per_sm * rq::num_sms(s->device));
     for (const auto& d : P->descs) {
         const size_t smem = smem_of(d);
-        RQ_CUDA(cudaFuncSetAttribute(k_sweep_tc16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_sweep_tc16<<<grid, threads, smem, s->stream>>>((float2*)s->amps, d, ph, op, img, P->ntiles);
+        auto kern = threads > 256 ? k_sweep_tc16<512> : k_sweep_tc16<256>;
+        RQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        kern<<<grid, threads, smem, s->stream>>>((float2*)s->amps, d, ph, op, img, P->ntiles);
         RQ_CUDA(cudaGetLastError());
     }
     return RQ_OK;

@@ -305,10 +305,15 @@ class Plan:
     planning and the upload of the gate tables happen here, once.
     """
 
-    def __init__(self, state: QuantumState, gates, mode: int = _capi.RQ_EXEC_AUTO):
+    def __init__(self, state: QuantumState, gates, mode: int = _capi.RQ_EXEC_AUTO, local_qubits: int = 0):
+        """local_qubits (tensor-core modes, complex f32): the sweep tile size, 12-13, or 12-14
+        for RQ_EXEC_SWEEP_TC16 (rq_plan_create_tiled); 0 = the default."""
         arr = gates if isinstance(gates, C.Array) else gates_to_array(gates)
         h = C.c_void_p()
-        check(lib.rq_plan_create(state.handle, arr, len(gates), int(mode), C.byref(h)))
+        if local_qubits:
+            check(lib.rq_plan_create_tiled(state.handle, arr, len(gates), int(mode), int(local_qubits), C.byref(h)))
+        else:
+            check(lib.rq_plan_create(state.handle, arr, len(gates), int(mode), C.byref(h)))
         self._h = h
 
     def execute(self, state: QuantumState) -> None:

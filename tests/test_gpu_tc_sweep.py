@@ -251,3 +251,38 @@ def test_tc16_non_unitary_matrices_run_on_the_tf32_split():
         g.reset()
         g.apply_gates(gates, rq.RQ_EXEC_SWEEP_TC16)
         assert err(g, gates) < 1e-5
+
+
+@pytest.mark.parametrize("n,layers", [(14, 6), (17, 8), (20, 10)])
+def test_tc16_14_qubit_tiles_match_oracle(n, layers):
+    """FP16-split sweeps on 14-qubit tiles (one 512-thread CTA per SM, four 128-row halves,
+    a ninth thread bit in the shared-memory layout): amplitudes within 1e-5 of the f64
+    oracle, fewer sweeps than 13-qubit tiles, and a rebind to new angles equals a fresh plan."""
+    gates = workloads.random_layer_circuit(n, layers, 30 + n)
+    g = QuantumState(n, 0, "f32")
+    plan = rq.Plan(g, gates, rq.RQ_EXEC_SWEEP_TC16, local_qubits=14)
+    st = plan.stats()
+    assert st["local_qubits"] == 14 and st["exec_mode"] == rq.RQ_EXEC_SWEEP_TC16
+    plan.execute(g)
+    assert float(np.max(np.abs(g.state_vector() - _oracle_f64(n, gates)))) < 1e-5
+    if n >= 17:
+        p13 = rq.Plan(QuantumState(n, 0, "f32"), gates, rq.RQ_EXEC_SWEEP_TC16, local_qubits=13)
+        assert st["sweeps"] <= p13.stats()["sweeps"]
+    new = workloads.random_layer_circuit(n, layers, 31 + n)
+    plan.update(g, new)
+    g.reset()
+    plan.execute(g)
+    f = QuantumState(n, 0, "f32")
+    rq.Plan(f, new, rq.RQ_EXEC_SWEEP_TC16, local_qubits=14).execute(f)
+    assert np.array_equal(g.state_vector(), f.state_vector())
+
+
+def test_tiled_plan_rejects_bad_tile_sizes():
+    g = QuantumState(16, 0, "f32")
+    gates = workloads.random_layer_circuit(16, 2, 1)
+    for mode, lq in ((rq.RQ_EXEC_SWEEP_TC, 14), (rq.RQ_EXEC_SWEEP_TC16, 15), (rq.RQ_EXEC_SWEEP_TC16, 11),
+                     (rq.RQ_EXEC_SWEEP, 13)):
+        with pytest.raises(rq.InvalidArgument):
+            rq.Plan(g, gates, mode, local_qubits=lq)
+    with pytest.raises(rq.InvalidArgument):
+        rq.Plan(QuantumState(16, 0, "f64"), gates, rq.RQ_EXEC_SWEEP_TC16, local_qubits=13)
