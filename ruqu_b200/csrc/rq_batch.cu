@@ -894,11 +894,15 @@ __global__ void k_vqe_energy(const typename C2<T>::t* __restrict__ states, uint3
 // into wsum.  Products of amplitudes in the state's precision, every product
 // added to an FP64 accumulator; indices fit 32 bits (at most 30 qubits).
 // need: 1 = only Re of conj(a_j) a_i is used, 2 = only Im, 3 = both.
+// a group's pairs are split into this many work units, so that the warps of a CTA finish a
+// partner tile together (groups alone are too few and too coarse to balance 16 warps)
+constexpr uint32_t VQE_CHUNKS = 4;
+
 template <typename T, int NT>
 __device__ __forceinline__ void tile_group(const VGroup& G, const VTerm* __restrict__ terms,
                                            const typename C2<T>::t* own, const typename C2<T>::t* src, uint32_t r,
                                            uint32_t rp, uint32_t t, uint32_t M, double* wsum, uint32_t nterms,
-                                           uint32_t lane, uint32_t warp) {
+                                           uint32_t lane, uint32_t warp, uint32_t chunk, uint32_t nchunk) {
     using V = typename C2<T>::t;
     const uint32_t L = 1u << M;
     uint32_t pm[NT];
@@ -915,19 +919,21 @@ __device__ __forceinline__ void tile_group(const VGroup& G, const VTerm* __restr
     const uint32_t x = (uint32_t)G.x;
     const uint32_t xl = x & (L - 1);
     const uint32_t count = x == 0 ? L : L >> 1;
+    // this call's share of the group's pairs: chunk `chunk` of `nchunk` equal parts
+    const uint32_t qlo = (uint32_t)(((uint64_t)count * chunk) / nchunk), qhi = (uint32_t)(((uint64_t)count * (chunk + 1)) / nchunk);
     const uint32_t sel = r < rp ? 0u : (1u ^ ((xl >> (M - 1)) & 1u));
     const uint32_t rbase = r << M, pbase = rp << M;
     // one warp owns the group: its lanes walk all pairs, one warp reduction per group.  The
     // products are summed in T over 16 pairs of a lane, then added into the FP64 accumulators
     // (16 terms in f32 keep the partial within ~1e-6 relative).
-    for (uint32_t q0 = lane; q0 < count; q0 += 32 * 16) {
+    for (uint32_t q0 = qlo + lane; q0 < qhi; q0 += 32 * 16) {
         T part[NT];
 #pragma unroll
         for (int k = 0; k < NT; ++k) part[k] = (T)0;
 #pragma unroll 4
         for (uint32_t u = 0; u < 16; ++u) {
             const uint32_t q = q0 + 32 * u;
-            if (q >= count) break;
+            if (q >= qhi) break;
             T re = 0, im = 0;
             uint32_t i;
             if (x == 0) {
@@ -966,7 +972,7 @@ __device__ __forceinline__ void tile_group(const VGroup& G, const VTerm* __restr
 #pragma unroll
     for (int k = 0; k < NT; ++k) {
         const double v = warp_sum_d(acc[k]);
-        if (lane == 0 && k < (int)G.nt) wsum[warp * nterms + G.t0 + k] = v;
+        if (lane == 0 && k < (int)G.nt) wsum[warp * nterms + G.t0 + k] += v;
     }
 }
 
@@ -1013,14 +1019,18 @@ __global__ void __launch_bounds__(512, 1) k_vqe_energy_tiles(const typename C2<T
                 __syncthreads();
                 src = par;
             }
-            for (uint32_t g = gofs[t] + warp; g < gofs[t + 1]; g += nw) {
-                const VGroup G = groups[g];
+            // work units: each group's pairs in VQE_CHUNKS equal parts, dealt to the warps in turn
+            // (a warp's partial sums of a term add up in its own row of wsum)
+            const uint32_t nunits = (gofs[t + 1] - gofs[t]) * VQE_CHUNKS;
+            for (uint32_t u = warp; u < nunits; u += nw) {
+                const VGroup G = groups[gofs[t] + u / VQE_CHUNKS];
+                const uint32_t ch = u % VQE_CHUNKS;
                 switch (G.nt) {
-                    case 1: tile_group<T, 1>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp); break;
-                    case 2: tile_group<T, 2>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp); break;
-                    case 3: tile_group<T, 3>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp); break;
-                    case 4: tile_group<T, 4>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp); break;
-                    default: tile_group<T, 8>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp); break;
+                    case 1: tile_group<T, 1>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp, ch, VQE_CHUNKS); break;
+                    case 2: tile_group<T, 2>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp, ch, VQE_CHUNKS); break;
+                    case 3: tile_group<T, 3>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp, ch, VQE_CHUNKS); break;
+                    case 4: tile_group<T, 4>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp, ch, VQE_CHUNKS); break;
+                    default: tile_group<T, 8>(G, terms, own, src, r, rp, t, M, wsum, nterms, lane, warp, ch, VQE_CHUNKS); break;
                 }
             }
             __syncthreads();
