@@ -160,6 +160,22 @@ __device__ __forceinline__ void dispatch_rx(int k, V* reg, T c, T s) {
     }
 }
 
+// packed FP32x2 arithmetic: one instruction for both parts of a complex f32 value
+__device__ __forceinline__ float2 pk_mul(float2 a, float2 b) {
+    float2 r;
+    asm("{.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 pk_fma(float2 a, float2 b, float2 c) {
+    float2 r;
+    asm("{.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
+        "mov.b64 rc, {%6, %7};\n\tfma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;}"
+        : "=f"(r.x), "=f"(r.y) : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return r;
+}
+
 // Ry(theta) on slot K: [[c, -s], [s, c]] with c = cos(theta/2), s = sin(theta/2)
 template <int K, int NR, typename V, typename T>
 __device__ __forceinline__ void op_ry(V* reg, T c, T s) {
@@ -169,10 +185,16 @@ __device__ __forceinline__ void op_ry(V* reg, T c, T s) {
         const int j = i | (1 << K);
         V x = reg[i], y = reg[j];
         V o0, o1;
-        o0.x = c * x.x - s * y.x;
-        o0.y = c * x.y - s * y.y;
-        o1.x = s * x.x + c * y.x;
-        o1.y = s * x.y + c * y.y;
+        if constexpr (std::is_same<T, float>::value) {   // c x - s y and s x + c y, both parts at once
+            const float2 c2 = make_float2(c, c), s2 = make_float2(s, s), ms2 = make_float2(-s, -s);
+            o0 = pk_fma(c2, x, pk_mul(ms2, y));
+            o1 = pk_fma(s2, x, pk_mul(c2, y));
+        } else {
+            o0.x = c * x.x - s * y.x;
+            o0.y = c * x.y - s * y.y;
+            o1.x = s * x.x + c * y.x;
+            o1.y = s * x.y + c * y.y;
+        }
         reg[i] = o0;
         reg[j] = o1;
     }
