@@ -155,3 +155,14 @@ def test_pauli_hamiltonian():
 def test_rng_box_muller_moments():
     z = rng.Stream(9, 4).normal(20000)
     assert abs(z.mean()) < 0.03 and abs(z.std() - 1) < 0.03
+
+
+def test_uniforms_keys_equal_the_per_key_stream():
+    """rng.uniforms_keys (draw k of many keys at once, the shots of a distributed sample)
+    equals draw k of each key's own stream."""
+    import numpy as np
+    from ruqu_b200.rng import uniforms, uniforms_keys
+    keys = np.array([0, 1, 42, 2**63 + 5, 2**64 - 1], dtype=np.uint64)
+    for k in (0, 1, 2, 7, 1000001):
+        want = np.array([uniforms(int(s), 0, k, 1)[0] for s in keys])
+        assert np.array_equal(uniforms_keys(keys, 0, k), want)
