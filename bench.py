@@ -445,6 +445,16 @@ def warmstart_leg(a, ws, rank, with_cpu=False):
         _, _, e, st = hb.optimize_precond(pg, pb, P, 200, 0.8, target=target, rtol=1e-5)
         arm("learned_pipeline_convergence_rule", hb.last_ms() + infer_ms, e, st)
         hb.set_convergence(0.0)
+        # the network on label-free cycle statistics instead of the padded adjacency
+        wc = WarmStart(p, encoding="cycles")
+        hist_c = wc.fit(train, g, b)
+        wc.precond = warm.precond
+        cg, cb = wc.predict(held)
+        _, _, e, st = hb.optimize_precond(cg, cb, P, 200, 0.8, target=target, rtol=1e-5)
+        arm("cycles_pipeline", hb.last_ms(), e, st)
+        arms["cycles_pipeline"]["mlp_val_error_vs_trend"] = min(hist_c) if hist_c else None
+        arms["cycles_pipeline"]["median_start_distance"] = float(np.median(np.linalg.norm(
+            np.concatenate([cg, cb], axis=1) - np.concatenate([opt_g, opt_b], axis=1), axis=1)))
     # start-point quality: distance of each start from the graph's own optimum (the plain run's)
     ng = np.array([n for n, _ in held])
     opt = np.concatenate([opt_g, opt_b], axis=1)
