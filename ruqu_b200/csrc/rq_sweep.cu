@@ -303,7 +303,6 @@ __global__ void __launch_bounds__(256, 2) k_sweep(typename C2<T>::t* __restrict_
     V* sm = reinterpret_cast<V*>(smem_raw);
 
     const uint32_t tid = threadIdx.x;
-    const uint32_t T_ = blockDim.x;
     const uint64_t cmask = (1ull << d.c) - 1;
 
     // deposit of this thread's vector offset (local bits of EPV*tid) into global positions
@@ -877,11 +876,6 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
 }
 
 __device__ __forceinline__ float pow2f(int k) { return __int_as_float((k + 127) << 23); }   // |k| <= 126
-
-__device__ __forceinline__ uint32_t pack_f16x2(float lo_elem, float hi_elem) {
-    const __half2 h = __floats2half2_rn(lo_elem, hi_elem);
-    return *reinterpret_cast<const uint32_t*>(&h);
-}
 
 __device__ __forceinline__ void st16u(uint32_t taddr, const uint32_t* v) {
     asm volatile(
