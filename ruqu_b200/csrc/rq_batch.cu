@@ -431,15 +431,15 @@ __global__ void k_energy_finalize(const double* __restrict__ epart, uint64_t nci
 // gpart -- deterministic for a given launch shape.
 template <int K, int NR, typename V>
 __device__ __forceinline__ double im_x_overlap(const V* p, const V* l) {
-    double acc = 0.0;
+    decltype(p[0].x) acc = 0;   // at most 16 products of one thread, in the state's type
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
         if (i & (1 << K)) continue;
         const int j = i | (1 << K);
         // Im(conj(l_i) p_j + conj(l_j) p_i)
-        acc += (double)(l[i].x * p[j].y - l[i].y * p[j].x) + (double)(l[j].x * p[i].y - l[j].y * p[i].x);
+        acc += (l[i].x * p[j].y - l[i].y * p[j].x) + (l[j].x * p[i].y - l[j].y * p[i].x);
     }
-    return acc;
+    return (double)acc;
 }
 
 template <int NR, typename V>
@@ -460,14 +460,14 @@ __device__ __forceinline__ double dispatch_im_x(int k, const V* p, const V* l) {
 // part is Re(conj(l_j) p_i) - Re(conj(l_i) p_j).
 template <int K, int NR, typename V>
 __device__ __forceinline__ double im_y_overlap(const V* p, const V* l) {
-    double acc = 0.0;
+    decltype(p[0].x) acc = 0;   // at most 16 products of one thread, in the state's type
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
         if (i & (1 << K)) continue;
         const int j = i | (1 << K);
-        acc += (double)(l[j].x * p[i].x + l[j].y * p[i].y) - (double)(l[i].x * p[j].x + l[i].y * p[j].y);
+        acc += (l[j].x * p[i].x + l[j].y * p[i].y) - (l[i].x * p[j].x + l[i].y * p[j].y);
     }
-    return acc;
+    return (double)acc;
 }
 
 template <int NR, typename V>
