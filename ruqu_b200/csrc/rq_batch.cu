@@ -426,9 +426,10 @@ __global__ void k_energy_finalize(const double* __restrict__ epart, uint64_t nci
 // taken when Rx_q is undone), then dE/dgamma_l = 2 Im <lambda|G|psi> with
 // G = diag(|E| - 2 cut(x)) (the product of the layer's Rzz(2 gamma) is
 // exp(-i gamma G)).  Each thread holds the same 2^RB indices of psi and
-// lambda; the per-op partial sums are FP64, reduced per warp by shuffles
-// (fixed order) into per-warp rows of shared memory, and per tile into
-// gpart -- deterministic for a given launch shape.
+// lambda; a thread sums its (at most 16) products of one op in the state's type,
+// the per-op partials are FP64, reduced per warp by shuffles (fixed order) into
+// per-warp rows of shared memory, and per tile into gpart -- deterministic for a
+// given launch shape.
 template <int K, int NR, typename V>
 __device__ __forceinline__ double im_x_overlap(const V* p, const V* l) {
     decltype(p[0].x) acc = 0;   // at most 16 products of one thread, in the state's type
