@@ -358,11 +358,11 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
             if ((d.flags & SWEEP_ENERGY) && p + 1 == d.phase_end) {
                 CutNb<RB> cp;
                 cut_plan_nb<RB>(cp, nb, U, ph.slot_global);
+                T e = 0;   // this thread's 2^RB terms in the state's type, then FP64 across threads
 #pragma unroll
-                for (int i = 0; i < NR; ++i) {
-                    const double re = (double)reg[i].x, im = (double)reg[i].y;
-                    energy += (re * re + im * im) * (double)cut_nb<RB>(cp, i);
-                }
+                for (int i = 0; i < NR; ++i)
+                    e += (reg[i].x * reg[i].x + reg[i].y * reg[i].y) * (T)cut_nb<RB>(cp, i);
+                energy += (double)e;
             }
             {
                 uint32_t ad = sb;
@@ -622,16 +622,16 @@ __global__ void __launch_bounds__(512, 1) k_batch_adjoint(const SweepDesc d, con
                     CutNb<RB> cp;
                     cut_plan_nb<RB>(cp, nb, U, ph.slot_global);
                     const T* tab = a.ph + ((size_t)gcirc * a.p + op.param) * a.phs * 2;
-                    double acc = 0.0;
+                    T acc = 0;   // this thread's 2^RB terms in the state's type
 #pragma unroll
                     for (int i = 0; i < NR; ++i) {
                         const int c = cut_nb<RB>(cp, i);
                         const T gdiag = (T)((int)ne - 2 * c);
-                        acc += (double)(gdiag * (rl[i].x * rp[i].y - rl[i].y * rp[i].x));
+                        acc += gdiag * (rl[i].x * rp[i].y - rl[i].y * rp[i].x);
                         rp[i] = cmulv(rp[i], tab[2 * c], -tab[2 * c + 1]);
                         rl[i] = cmulv(rl[i], tab[2 * c], -tab[2 * c + 1]);
                     }
-                    flush(2.0 * acc, op.param);
+                    flush(2.0 * (double)acc, op.param);
                 } else if (op.type == OP_RYP) {
                     // Ry(theta) = exp(-i theta Y / 2): dE/dtheta = Im <lambda|Y|psi>
                     const T* r = a.rot + ((size_t)gcirc * a.nparam + op.param) * 2;
