@@ -122,6 +122,19 @@ __device__ __forceinline__ int cut_nb(const CutNb<RB>& cp, int i) {   // i: a co
     return c;
 }
 
+// v * i^k (exact: a swap and sign changes)
+template <typename V>
+__device__ __forceinline__ V mul_ipow(V v, int k) {
+    V r;
+    switch (k & 3) {
+        case 0: r = v; break;
+        case 1: r.x = -v.y; r.y = v.x; break;
+        case 2: r.x = -v.x; r.y = -v.y; break;
+        default: r.x = v.y; r.y = -v.x; break;
+    }
+    return r;
+}
+
 template <typename V, typename T>
 __device__ __forceinline__ V cmulv(V a, T br, T bi) {
     V r;
@@ -315,6 +328,11 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
                 if (d.flags & SWEEP_INIT_UNIFORM) {
 #pragma unroll
                     for (int i = 0; i < NR; ++i) { reg[i].x = a.amp0; reg[i].y = (T)0; }
+                    if (d.flags & SWEEP_PHASE_IN) {   // S^n H^n |0>: amplitude i^popc(x)
+                        const int pu = __popcll(U);
+#pragma unroll
+                        for (int i = 0; i < NR; ++i) reg[i] = mul_ipow(reg[i], pu + __popc(i));
+                    }
                 } else {   // |0...0>
 #pragma unroll
                     for (int i = 0; i < NR; ++i) { reg[i].x = (i == 0 && U == 0) ? (T)1 : (T)0; reg[i].y = (T)0; }
@@ -354,6 +372,11 @@ __global__ void __launch_bounds__(256, 2) k_batch_sweep(const SweepDesc d, const
                         reg[i] = cmulv(reg[i], tab[2 * c], tab[2 * c + 1]);
                     }
                 }
+            }
+            if ((d.flags & SWEEP_PHASE_OUT) && p + 1 == d.phase_end) {   // S^dag on every qubit
+                const int pu = __popcll(U);
+#pragma unroll
+                for (int i = 0; i < NR; ++i) reg[i] = mul_ipow(reg[i], -(pu + __popc(i)));
             }
             if ((d.flags & SWEEP_ENERGY) && p + 1 == d.phase_end) {
                 CutNb<RB> cp;
@@ -1563,7 +1586,9 @@ int rq_qaoa_batch_create(uint32_t ninst, const uint32_t* num_nodes, const uint32
         K.c = std::min<uint32_t>(K.m, 5);
         K.ntiles = 1ull << (K.n - K.m);
         K.smem = ((size_t)1 << K.m) * elem_size(precision);
-        // the circuit of qaoa.rs:125-153 after H^n: per layer the cost phase, then Rx on every qubit
+        // the circuit of qaoa.rs:125-153 after H^n: per layer the cost phase, then Rx on every
+        // qubit, run as Ry between the phases S^n H^n |0> and a final S^dag n (SWEEP_PHASE_IN /
+        // _OUT): a real rotation costs half the arithmetic of Rx
         std::vector<PGate> g;
         for (uint32_t l = 0; l < p; ++l) {
             PGate ph{};
@@ -1575,7 +1600,7 @@ int rq_qaoa_batch_create(uint32_t ninst, const uint32_t* num_nodes, const uint32
             g.push_back(ph);
             for (uint32_t q = 0; q < K.n; ++q) {
                 PGate rx{};
-                rx.type = OP_RXP;
+                rx.type = OP_RYP;
                 rx.q0 = q;
                 rx.param = (uint16_t)l;
                 g.push_back(rx);
@@ -1588,8 +1613,8 @@ int rq_qaoa_batch_create(uint32_t ninst, const uint32_t* num_nodes, const uint32
         build_program(sweeps, K.n, K.m, K.c, rb, precision == RQ_F32 ? 2 : 1, K.descs, phases, ops, mats);
         if (precision == RQ_F32) retable_f16(K.descs, phases, rb);   // the conflict-free layout (k_batch_sweep<float>)
         K.smem += max_phases(K.descs) * sizeof(PhaseDesc);   // the phase descriptors after the tile
-        K.descs.front().flags |= SWEEP_INIT_UNIFORM;
-        K.descs.back().flags |= SWEEP_ENERGY;
+        K.descs.front().flags |= SWEEP_INIT_UNIFORM | SWEEP_PHASE_IN;
+        K.descs.back().flags |= SWEEP_ENERGY | SWEEP_PHASE_OUT;
         K.off_ops = (phases.size() * sizeof(PhaseDesc) + 255) & ~size_t(255);
         size_t total = K.off_ops + ops.size() * sizeof(SwOp);
         std::vector<unsigned char> host(total);

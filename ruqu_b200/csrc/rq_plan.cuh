@@ -71,6 +71,12 @@ constexpr uint32_t SWEEP_INIT_UNIFORM = 1u;   // synthesise |+>^n instead of loa
 constexpr uint32_t SWEEP_ENERGY = 2u;         // reduce sum |a|^2 cut(x) after the last phase
 constexpr uint32_t SWEEP_INIT_ZERO = 4u;      // synthesise |0...0> instead of loading the tile
 constexpr uint32_t SWEEP_INIT_LAMBDA = 8u;    // adjoint sweeps: build lambda = C psi instead of loading it
+// batched QAOA: Rx(t) = S^dag Ry(t) S, and the S of one layer cancels the S^dag of the next
+// across the diagonal cost phase, so the forward program runs Ry and carries the phases
+// i^popc(x) from the start (PHASE_IN, with INIT_UNIFORM) to the end (PHASE_OUT: (-i)^popc(x)
+// after the last phase)
+constexpr uint32_t SWEEP_PHASE_IN = 16u;
+constexpr uint32_t SWEEP_PHASE_OUT = 32u;
 
 
 struct PGate {
