@@ -449,9 +449,27 @@ def warmstart_leg(a, ws, rank, with_cpu=False):
         wc = WarmStart(p, encoding="cycles")
         hist_c = wc.fit(train, g, b)
         wc.precond = warm.precond
+        t2 = time.perf_counter()
         cg, cb = wc.predict(held)
+        infer_c = (time.perf_counter() - t2) * 1e3
         _, _, e, st = hb.optimize_precond(cg, cb, P, 200, 0.8, target=target, rtol=1e-5)
-        arm("cycles_pipeline", hb.last_ms(), e, st)
+        arm("cycles_pipeline", hb.last_ms() + infer_c, e, st)
+        # the same start with a safeguard: instances not at their target after K steps start
+        # again from the size trend (the remaining budget, on a batch of those instances only)
+        K = 12
+        g1, b1, e1, st1 = hb.optimize_precond(cg, cb, P, K, 0.8, target=target, rtol=1e-5)
+        ms = hb.last_ms() + infer_c
+        left = np.flatnonzero(~reached(e1, target))
+        e_all, st_all = e1.copy(), st1.astype(np.int64)
+        if len(left):
+            sb = QaoaBatch([held[i] for i in left], p, "f32")
+            _, _, e2, st2 = sb.optimize_precond(mg[left], mb[left], P[left], 200 - K, 0.8, target=target[left],
+                                                rtol=1e-5)
+            ms += sb.last_ms()
+            e_all[left] = e2
+            st_all[left] = K + st2
+        arm("cycles_then_trend", ms, e_all, st_all)
+        arms["cycles_then_trend"]["restarted"] = int(len(left))
         arms["cycles_pipeline"]["mlp_val_error_vs_trend"] = min(hist_c) if hist_c else None
         arms["cycles_pipeline"]["median_start_distance"] = float(np.median(np.linalg.norm(
             np.concatenate([cg, cb], axis=1) - np.concatenate([opt_g, opt_b], axis=1), axis=1)))
