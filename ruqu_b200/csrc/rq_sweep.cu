@@ -952,8 +952,12 @@ __device__ __forceinline__ bool wait_sleep(uint64_t* bar, uint32_t parity, uint3
 
 }  // namespace tc16
 
-// NTHR = 256: tiles of up to 13 local qubits, two CTAs per SM; NTHR = 512: 14 local qubits,
-// one CTA (four 128-row halves, all 512 tensor-memory columns) per SM.
+// NTHR = 128: tiles of 12 local qubits, four CTAs per SM, one operand-image buffer (the next
+// image is copied in once the CTA's only half has finished its MMAs: a second buffer would
+// leave room for three CTAs only, and a fourth independent phase chain per SM hides more of
+// the chain's latency than the earlier image copy does); NTHR = 256: 13 local qubits, two
+// CTAs per SM; NTHR = 512: 14 local qubits, one CTA (four 128-row halves, all 512
+// tensor-memory columns) per SM.  NTHR = 256 and 512 double-buffer the images.
 template <int NTHR>
 __global__ void __launch_bounds__(NTHR, 512 / NTHR) k_sweep_tc16(float2* __restrict__ amps, const SweepDesc d,
                                                      const PhaseDesc* __restrict__ phases,
@@ -961,11 +965,12 @@ __global__ void __launch_bounds__(NTHR, 512 / NTHR) k_sweep_tc16(float2* __restr
                                                      const uint32_t* __restrict__ images, uint64_t ntiles) {
     using VV = float4;
     constexpr int NR = 32;
+    constexpr bool ONE_BUF = NTHR == 128;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t tile_elems = 1u << d.m;
     float2* sm = reinterpret_cast<float2*>(smem_raw);
-    unsigned char* img = reinterpret_cast<unsigned char*>(sm + tile_elems);   // two image buffers
-    PhaseDesc* sph = reinterpret_cast<PhaseDesc*>(img + 2 * tc16::IMG_BYTES);
+    unsigned char* img = reinterpret_cast<unsigned char*>(sm + tile_elems);   // one or two image buffers
+    PhaseDesc* sph = reinterpret_cast<PhaseDesc*>(img + (ONE_BUF ? 1u : 2u) * tc16::IMG_BYTES);
     const uint32_t nph = d.phase_end - d.phase_begin;
     const uint32_t op0 = phases[d.phase_begin].op_begin, nops = phases[d.phase_end - 1].op_end - op0;
     SwOp* sop = reinterpret_cast<SwOp*>(sph + nph);
@@ -1066,7 +1071,7 @@ __global__ void __launch_bounds__(NTHR, 512 / NTHR) k_sweep_tc16(float2* __restr
             const uint32_t buf = step & 1u;
             const PhaseDesc& ph = lph[p];
             // the next step's image into the other buffer (its previous MMAs finished last step)
-            if (tid == 0) {
+            if (!ONE_BUF && tid == 0) {
                 const bool more = p + 1 < d.phase_end;
                 if (more || next < ntiles) {
                     tc16::start_copy(tc::smem_u32(img + (buf ^ 1u) * tc16::IMG_BYTES),
@@ -1155,8 +1160,13 @@ __global__ void __launch_bounds__(NTHR, 512 / NTHR) k_sweep_tc16(float2* __restr
             const uint32_t mpar = step & 1u;
             if ((tid & 127u) == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                if (tc16::wait_sleep(&ibar[buf], (step >> 1) & 1u, hpolls)) {
-                    const uint32_t bh = tc::smem_u32(img + buf * tc16::IMG_BYTES), bl = bh + tc16::PART_BYTES;
+                // with one buffer the n-th copy completes phase n of ibar[0]; with two, copies
+                // alternate between the buffers
+                const bool landed = ONE_BUF ? tc16::wait_sleep(&ibar[0], step & 1u, hpolls)
+                                            : tc16::wait_sleep(&ibar[buf], (step >> 1) & 1u, hpolls);
+                if (landed) {
+                    const uint32_t bh = tc::smem_u32(img + (ONE_BUF ? 0u : buf) * tc16::IMG_BYTES);
+                    const uint32_t bl = bh + tc16::PART_BYTES;
                     const uint32_t dt = tmem + col_h, ah = tmem + col_h + 64u, al = tmem + col_h + 96u;
                     // the small correction products first, then the large one on top of them:
                     // fewer additions into a large running sum, where the accumulator rounds
@@ -1177,6 +1187,15 @@ __global__ void __launch_bounds__(NTHR, 512 / NTHR) k_sweep_tc16(float2* __restr
                 }
             }
             if (!tc16::wait_sleep(&mbar[half], mpar, hpolls)) failed = true;
+            if (ONE_BUF && tid == 0 && !failed && !half_failed[0]) {
+                // the only half's MMAs have read the image: copy in the next step's
+                const bool more = p + 1 < d.phase_end;
+                if (more || next < ntiles) {
+                    tc16::start_copy(tc::smem_u32(img), more ? image_of(base, p + 1) : image_of(nbase, d.phase_begin),
+                                     &ibar[0]);
+                    ++issued[0];
+                }
+            }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (half_failed[half]) failed = true;
             {
@@ -1788,7 +1807,8 @@ static int launch_tc16(rq_state* s, const rq_plan* P, const PhaseDesc* ph, const
     auto smem_of = [&](const SweepDesc& d) {
         const size_t nph = d.phase_end - d.phase_begin;
         const size_t nops = hph[d.phase_end - 1].op_end - hph[d.phase_begin].op_begin;
-        return P->smem + 2 * (size_t)tc16::IMG_BYTES + nph * sizeof(PhaseDesc) + nops * sizeof(SwOp);
+        return P->smem + (threads == 128 ? 1u : 2u) * (size_t)tc16::IMG_BYTES + nph * sizeof(PhaseDesc) +
+               nops * sizeof(SwOp);
     };
     size_t smem_max = 0;
     for (const auto& d : P->descs) smem_max = std::max(smem_max, smem_of(d));
@@ -1800,7 +1820,7 @@ static int launch_tc16(rq_state* s, const rq_plan* P, const PhaseDesc* ph, const
     const unsigned grid = (unsigned)std::min<uint64_t>(P->ntiles, (uint64_t)per_sm * rq::num_sms(s->device));
     for (const auto& d : P->descs) {
         const size_t smem = smem_of(d);
-        auto kern = threads > 256 ? k_sweep_tc16<512> : k_sweep_tc16<256>;
+        auto kern = threads > 256 ? k_sweep_tc16<512> : threads > 128 ? k_sweep_tc16<256> : k_sweep_tc16<128>;
         RQ_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kern<<<grid, threads, smem, s->stream>>>((float2*)s->amps, d, ph, op, img, P->ntiles);
         RQ_CUDA(cudaGetLastError());
