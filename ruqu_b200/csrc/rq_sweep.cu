@@ -855,8 +855,10 @@ __global__ void __launch_bounds__(256, 2) k_sweep_tc(float2* __restrict__ amps, 
 // * each half is issued by its own thread (warp 4h, lane 0) with its own
 //   completion mbarrier, so one half's MMAs overlap the other half's
 //   conversion; the CTA meets once per phase (the shared-memory exchange);
-// * operand images are double-buffered: while a phase's MMAs run, the next
-//   phase's image (or the next tile's first image) is already being copied.
+// * operand images are double-buffered on 13- and 14-qubit tiles: while a
+//   phase's MMAs run, the next phase's image (or the next tile's first image)
+//   is already being copied; 12-qubit tiles keep one buffer, so that four CTAs
+//   fit on an SM, and copy the next image in once their MMAs are done.
 namespace tc16 {
 
 constexpr uint32_t IMG_BYTES = DENSE_F16_WORDS * 4u;   // 16 KB: high + low part
