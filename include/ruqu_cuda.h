@@ -264,9 +264,9 @@ RQ_API int rq_plan_execute(rq_state* s, const rq_plan* p);
 
 /* As rq_plan_create with the tile size of a tensor-core sweep chosen by the caller (the
  * autotuner of RQ_EXEC_AUTO picks among these itself): local_qubits 12 or 13 for
- * RQ_EXEC_SWEEP_TC / _TC_FAST, 12, 13 or 14 for RQ_EXEC_SWEEP_TC16 (14: one 512-thread CTA
- * per SM, fewer sweeps), complex f32 states only; 0 = the default.  No counterpart in the
- * reference. */
+ * RQ_EXEC_SWEEP_TC / _TC_FAST, 12, 13 or 14 for RQ_EXEC_SWEEP_TC16 (12: four 128-thread CTAs
+ * per SM, more sweeps; 13: two 256-thread CTAs per SM; 14: one 512-thread CTA per SM, fewer
+ * sweeps), complex f32 states only; 0 = the default.  No counterpart in the reference. */
 RQ_API int rq_plan_create_tiled(const rq_state* s, const rq_gate* gates, uint64_t n, int32_t mode,
                                 uint32_t local_qubits, rq_plan** out);
 

@@ -494,6 +494,17 @@ struct SweepCost {
 };
 constexpr SweepCost COST_TF32{1.79, 1.91}, COST_F16{3.15, 1.05};
 
+// The autotuner's choice among timed candidates: candidate 0 is the reference point, and a
+// later eligible candidate replaces the best so far only when it is faster by more than the
+// relative margin, so near-equal plans keep the earlier one (the candidates are listed with
+// fewer sweeps first) instead of following timing noise.
+inline size_t pick_fastest(const float* ms, const bool* eligible, size_t n, float margin = 0.02f) {
+    size_t best = 0;
+    for (size_t k = 1; k < n; ++k)
+        if (eligible[k] && ms[k] < (1.f - margin) * ms[best]) best = k;
+    return best;
+}
+
 inline double plan_cost(std::vector<Sweep> sweeps, uint32_t n, uint32_t m, uint32_t rb, SweepCost k = COST_TF32) {
     double c = 0.0;
     for (auto& sw : sweeps) {

@@ -1790,9 +1790,16 @@ int autotune_tc(const rq_state* s, const rq_gate* gates, uint64_t n, int* passes
         // a later candidate must be more than 2 % faster than the best so far: near-equal plans
         // (the 12- and 13-qubit FP16 plans of a 30-qubit random-layer circuit are within 1 %)
         // then keep the earlier one, which has fewer sweeps, instead of following timing noise
-        for (size_t k = 1; k < cands.size() && rc == RQ_OK; ++k)
-            if (cands[k].plan && cands[k].plan->stats.dense_ops > 0 && cands[k].ms < 0.98f * cands[best].ms)
-                best = (int)k;
+        if (rc == RQ_OK) {
+            float ms[8];
+            bool ok[8];
+            const size_t nc = std::min<size_t>(cands.size(), 8);   // at most six candidates
+            for (size_t k = 0; k < nc; ++k) {
+                ms[k] = cands[k].ms;
+                ok[k] = cands[k].plan && cands[k].plan->stats.dense_ops > 0;
+            }
+            best = (int)pick_fastest(ms, ok, nc);
+        }
         cudaFree(scratch);
     } else {
         cudaGetLastError();   // no room for a scratch state (or nothing to compare): CUDA-core sweep

@@ -224,6 +224,17 @@ int main() {
                     if (d.sgj[j] != swz16(j * (1u << tb) * 2u)) return fail("sgj not under swz16", t2);
         }
     }
+    {   // the autotuner's pick: a later candidate must win by more than 2 %
+        const float ms1[4] = {400.f, 130.f, 100.f, 99.f};   // CUDA cores, 3xTF32, FP16 13, FP16 12
+        const bool all[4] = {true, true, true, true};
+        if (pick_fastest(ms1, all, 4) != 2) return fail("a 1 % faster later candidate was taken", -1);
+        const float ms2[4] = {400.f, 130.f, 100.f, 97.f};
+        if (pick_fastest(ms2, all, 4) != 3) return fail("a 3 % faster later candidate was not taken", -1);
+        const bool no_tc[4] = {true, false, false, false};
+        if (pick_fastest(ms2, no_tc, 4) != 0) return fail("an ineligible candidate was taken", -1);
+        const float ms3[3] = {10.f, 10.f, 10.f};
+        if (pick_fastest(ms3, all, 3) != 0) return fail("a tie did not keep the first candidate", -1);
+    }
     std::printf("ok %d plans\n", trials);
     return 0;
 }
