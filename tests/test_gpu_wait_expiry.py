@@ -23,13 +23,18 @@ pytestmark = pytest.mark.gpu
 DEFAULT = 0xFFFFFFFF
 
 
-@pytest.mark.parametrize("mode", [rq.RQ_EXEC_SWEEP_TC, rq.RQ_EXEC_SWEEP_TC16])
-def test_sweep_wait_expiry_reports_timeout_and_state_recovers(mode):
+@pytest.mark.parametrize("mode,lq", [(rq.RQ_EXEC_SWEEP_TC, 0), (rq.RQ_EXEC_SWEEP_TC16, 0),
+                                     (rq.RQ_EXEC_SWEEP_TC16, 12)])
+def test_sweep_wait_expiry_reports_timeout_and_state_recovers(mode, lq):
+    """lq 0 = the default tile (13 local qubits here); 12 = the FP16 kernel's one-buffer,
+    four-CTAs-per-SM instantiation, whose next image copy is issued after the MMAs."""
     n = 15
     gates = workloads.random_layer_circuit(n, 4, 7)
     st = rq.QuantumState(n, 0, "f32")
-    plan = rq.Plan(st, gates, mode)
+    plan = rq.Plan(st, gates, mode, local_qubits=lq) if lq else rq.Plan(st, gates, mode)
     assert plan.stats()["dense_ops"] > 0
+    if lq:
+        assert plan.stats()["local_qubits"] == lq
     st.synchronize()
     assert _capi.lib.rq_debug_set_wait_limit(0) == 0
     try:
