@@ -22,7 +22,6 @@ def _free_port():
 def _rank_main(rank, ws, port, out):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(ws), RANK=str(rank),
                       LOCAL_RANK=str(rank))
-    import torch
     import torch.distributed as tdist
 
     from ruqu_b200 import dist, workloads
