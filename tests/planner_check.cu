@@ -1,8 +1,8 @@
 // Host check of the sweep and phase planners of rq_plan.cuh (no GPU needed).
 //
 // Random circuits are planned with every planner combination (first-come,
-// lookahead and cost-aware sweeps, first-come and lookahead phases, CUDA-core and tensor-core
-// slot rules); the planned ops are applied in plan order (sweep, phase, op) to a
+// lookahead and cost-aware sweeps, first-come, lookahead and beam-search phases, CUDA-core and
+// tensor-core slot rules); the planned ops are applied in plan order (sweep, phase, op) to a
 // state vector in double precision, which must equal the gates applied in list
 // order.  The planners' own rules are checked on the way: every op's required
 // qubits are local and on slots, slot sets fit the register count, tensor-core
@@ -115,7 +115,7 @@ int main() {
                                       : sp == 4 ? plan_sweeps(pg, n, m, c, true, COST_F16)
                                                 : plan_sweeps_costed(pg, n, m, c, 5, 0.05);
             if (sweeps.empty() && !pg.empty()) return fail("no sweep plan", trial);
-            for (int pp = 0; pp < 3; ++pp)
+            for (int pp = 0; pp < 4; ++pp)
                 for (int tc = 0; tc < 2; ++tc) {
                     const uint32_t rb = tc ? 5 : (trial % 2 ? 5 : 4);
                     std::vector<Cx> a = start;
@@ -127,14 +127,17 @@ int main() {
                             if (needs(g, false) & ~sw.L) return fail("op needs a qubit outside its sweep", trial);
                         const auto phases = pp == 0 ? plan_phases_first_come(sw, rb, tc)
                                             : pp == 1 ? plan_phases_lookahead(sw, rb, tc)
+                                            : pp == 2 ? plan_phases_beam(sw, rb, tc)
                                                       : plan_phases(sw, rb, tc);
                         if (phases.empty() && !sw.ops.empty()) {
-                            if (pp == 1) {   // the lookahead may give up; plan_phases then falls back
+                            if (pp == 1 || pp == 2) {   // the lookahead and the beam may give up; plan_phases falls back
                                 gave_up = true;
                                 break;
                             }
                             return fail("no phase plan", trial);
                         }
+                        if (pp == 3 && phases.size() > plan_phases_first_come(sw, rb, tc).size())
+                            return fail("plan_phases has more phases than the first-come plan", trial);
                         std::vector<int> seen(sw.ops.size(), 0);
                         for (const auto& ph : phases) {
                             if ((uint32_t)__builtin_popcountll(ph.R) > rb) return fail("too many slots", trial);
