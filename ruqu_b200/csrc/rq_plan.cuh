@@ -628,10 +628,78 @@ inline std::vector<Sweep> plan_sweeps_costed(const std::vector<PGate>& gates, ui
     return out;
 }
 
+// Beam search over sweep plans for tensor-core sweeps: breadth-first by sweep, each partial
+// plan extended by every candidate local set of sweep_candidates (its phases planned with
+// plan_phases), the `width` extensions of highest (gates run) x rate - (modelled cost) kept
+// (distinct sets of gates run), extensions that already cost more than the cheapest complete
+// plan dropped; returns the cheapest complete plan seen.  rate = the cost per gate of a
+// reference plan, as in plan_sweeps_costed.
+inline std::vector<Sweep> plan_sweeps_beam(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c,
+                                           uint32_t rb, double rate, SweepCost cost, size_t width = 16) {
+    struct Partial {
+        std::vector<char> taken;
+        size_t first;
+        double cost;
+        int done;
+        std::vector<uint64_t> sets;
+    };
+    if (gates.empty()) return {};
+    std::vector<Partial> beam(1);
+    beam[0].taken.assign(gates.size(), 0);
+    beam[0].first = 0;
+    beam[0].cost = 0.0;
+    beam[0].done = 0;
+    double best_cost = 1e300;
+    std::vector<uint64_t> best_sets;
+    while (!beam.empty()) {
+        std::vector<Partial> next;
+        std::vector<std::vector<char>> seen;
+        for (const Partial& p : beam)
+            for (uint64_t L : sweep_candidates(gates, p.taken, p.first, n, m, c)) {
+                Partial t{p.taken, p.first, p.cost, p.done, p.sets};
+                const Sweep sw = take_sweep(gates, t.taken, p.first, L, n, m);
+                if (sw.ops.empty()) continue;
+                int got = 0;
+                for (size_t k = p.first; k < gates.size(); ++k) got += (t.taken[k] && !p.taken[k]) ? 1 : 0;
+                t.cost += cost.sweep + cost.phase * (double)plan_phases(sw, rb, true).size();
+                t.done += got;
+                t.sets.push_back(L);
+                while (t.first < gates.size() && t.taken[t.first]) ++t.first;
+                if (t.cost >= best_cost) continue;
+                if (t.first >= gates.size()) {
+                    best_cost = t.cost;
+                    best_sets = t.sets;
+                    continue;
+                }
+                if (std::find(seen.begin(), seen.end(), t.taken) != seen.end()) continue;
+                seen.push_back(t.taken);
+                next.push_back(std::move(t));
+            }
+        std::stable_sort(next.begin(), next.end(), [rate](const Partial& a, const Partial& b) {
+            return a.done * rate - a.cost > b.done * rate - b.cost;
+        });
+        if (next.size() > width) next.resize(width);
+        beam = std::move(next);
+    }
+    // replay the chosen local sets into sweeps (as plan_sweeps_costed builds them)
+    std::vector<Sweep> out;
+    std::vector<char> taken(gates.size(), 0);
+    size_t first = 0;
+    for (uint64_t L : best_sets) {
+        Sweep sw = take_sweep(gates, taken, first, L, n, m);
+        sw.L = L;
+        out.push_back(std::move(sw));
+        while (first < gates.size() && taken[first]) ++first;
+    }
+    if (first < gates.size()) return {};   // cannot happen: the chosen plan ran every gate
+    return out;
+}
+
 // The sweep plan.  CUDA-core plans: the first-come and lookahead plans, keeping the one
 // with fewer sweeps (each sweep is a full read and write of the state; first-come on a
-// tie).  Tensor-core plans (all_slots, five register slots): also the cost-aware plan,
-// keeping the plan of least modelled cost.  A gate qubit that stays outside a sweep's
+// tie).  Tensor-core plans (all_slots, five register slots): also the cost-aware and the
+// beam-search plans, keeping the plan of least modelled cost (the fewest-sweeps plan on a
+// tie, then the cost-aware one).  A gate qubit that stays outside a sweep's
 // local set is uniform over each tile, for CUDA-core and tensor-core plans alike.
 inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t n, uint32_t m, uint32_t c,
                                       bool all_slots = false, SweepCost k = COST_TF32) {
@@ -641,8 +709,13 @@ inline std::vector<Sweep> plan_sweeps(const std::vector<PGate>& gates, uint32_t 
     if (!all_slots || gates.empty()) return best;
     const uint32_t rb = 5;
     const double cost_best = plan_cost(best, n, m, rb, k);
-    auto d = plan_sweeps_costed(gates, n, m, c, rb, cost_best / (double)gates.size(), k);
-    if (!d.empty() && plan_cost(d, n, m, rb, k) < cost_best) return d;
+    const double rate = cost_best / (double)gates.size();
+    auto d = plan_sweeps_costed(gates, n, m, c, rb, rate, k);
+    double cost_d = d.empty() ? 1e300 : plan_cost(d, n, m, rb, k);
+    auto e = plan_sweeps_beam(gates, n, m, c, rb, rate, k);
+    const double cost_e = e.empty() ? 1e300 : plan_cost(e, n, m, rb, k);
+    if (cost_e < cost_best && cost_e < cost_d) return e;
+    if (cost_d < cost_best) return d;
     return best;
 }
 

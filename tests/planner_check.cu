@@ -1,7 +1,7 @@
 // Host check of the sweep and phase planners of rq_plan.cuh (no GPU needed).
 //
 // Random circuits are planned with every planner combination (first-come,
-// lookahead and cost-aware sweeps, first-come, lookahead and beam-search phases, CUDA-core and
+// lookahead, cost-aware and beam-search sweeps, first-come, lookahead and beam-search phases, CUDA-core and
 // tensor-core slot rules); the planned ops are applied in plan order (sweep, phase, op) to a
 // state vector in double precision, which must equal the gates applied in list
 // order.  The planners' own rules are checked on the way: every op's required
@@ -107,13 +107,20 @@ int main() {
         for (auto& v : want) v = Cx(nd(r), nd(r));
         const std::vector<Cx> start = want;
         for (const auto& g : pg) apply(want, g);
-        for (int sp = 0; sp < 6; ++sp) {
+        for (int sp = 0; sp < 7; ++sp) {
             std::vector<Sweep> sweeps = sp == 0 ? plan_sweeps_first_come(pg, n, m, c)
                                       : sp == 1 ? plan_sweeps_lookahead(pg, n, m, c)
                                       : sp == 2 ? plan_sweeps(pg, n, m, c)
                                       : sp == 3 ? plan_sweeps(pg, n, m, c, true)
                                       : sp == 4 ? plan_sweeps(pg, n, m, c, true, COST_F16)
-                                                : plan_sweeps_costed(pg, n, m, c, 5, 0.05);
+                                      : sp == 5 ? plan_sweeps_costed(pg, n, m, c, 5, 0.05)
+                                                : plan_sweeps_beam(pg, n, m, c, 5, 0.05, COST_F16);
+            if (sp >= 3 && sp != 5 && !pg.empty()) {   // tensor-core plans: never above the fewest-sweeps plan's cost
+                auto a = plan_sweeps_first_come(pg, n, m, c), b = plan_sweeps_lookahead(pg, n, m, c);
+                const double ref = plan_cost(b.size() < a.size() ? b : a, n, m, 5, COST_F16);
+                if (sp == 4 && plan_cost(sweeps, n, m, 5, COST_F16) > ref + 1e-9)
+                    return fail("plan_sweeps costs more than the fewest-sweeps plan", trial);
+            }
             if (sweeps.empty() && !pg.empty()) return fail("no sweep plan", trial);
             for (int pp = 0; pp < 4; ++pp)
                 for (int tc = 0; tc < 2; ++tc) {
